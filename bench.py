@@ -1,0 +1,295 @@
+#!/usr/bin/env python
+"""Benchmark of the TRiSK shallow-water RK4 step on B200.
+
+Workload (one "step" = one classical RK4 step = 4 tendencies): create_hexagon_mesh(7;
+centroidal=true) (163842 cells, 491520 edges, 327680 vertices), Gassmann PV flux, vertex
+kinetic energy, FP64, dt = 75 s, a seeded synthetic height/wind state on the Earth.
+
+  value  device-resident throughput in cell-steps/s (state and tables in HBM, one
+         trisk_rk4_step_async call of K steps, CUDA events on the model's stream).
+  e2e    the same metric through the public C ABI (trisk_rk4_step) with the state in
+         pinned host memory: every step copies the state in and reads it back.
+  roofline  the dominant kernel (k_tend: PV flux + gradient + continuity + RK4 update),
+         its algorithmic bytes per launch over its CUDA-event duration, against the
+         measured HBM copy bandwidth.
+  cpu_baseline  the CPU oracle (a C restatement of the reference kernels, not Julia) on
+         all host cores, over a bounded sample of the same workload.
+
+--impl reference times that CPU restatement alone (the reference itself is Julia, which
+is not installed). With N > 1 GPUs (torchrun) every rank runs an independent replica.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-steps/s on 1 B200: plain FP64 vs batched+closure at equal h L2 error"
+LEVEL, PV, KE, DT = 7, "gassmann", "vertex", 75.0
+WORKLOAD = "hexagon7-gassmann-vertex-fp64-rk4"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=1000)
+    p.add_argument("--warmup", type=int, default=10)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--cpu-seconds", type=float, default=15.0, help="bounded CPU-baseline sample")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--level", type=int, default=LEVEL, help="mesh level (7 is the benchmark workload)")
+    args = p.parse_args()
+    return args
+
+
+def build_workload(seed, level=LEVEL):
+    import dmplex_b200 as d
+    from dmplex_b200 import workloads as w
+    g = d.TRiSKGrid(d.create_hexagon_mesh(level, centroidal=True))
+    y = w.synthetic_state(g, seed=seed)
+    return g, y
+
+
+def config_dict(g, n, level=LEVEL):
+    workload = WORKLOAD if level == LEVEL else WORKLOAD.replace(f"hexagon{LEVEL}", f"hexagon{level}")
+    return {"workload": workload, "mesh": f"create_hexagon_mesh({level}; centroidal=true)", "cells": int(g.nc),
+            "edges": int(g.ne), "vertices": int(g.nv), "pv_flux": PV, "kinetic_energy": KE, "dt_s": DT,
+            "state": "seeded spherical harmonics deg<=8, 100 m rms, geostrophic u max 40 m/s",
+            "l2": "inputs larger than L2: the scheme's tables are 181 MB (L2 126 MB)",
+            "parallelism": "replicas" if n > 1 else "single"}
+
+
+def oracle_baseline(g, y, seconds, threads):
+    """CPU restatement of the reference kernels on `threads` host threads: bounded sample."""
+    import dmplex_b200 as d
+    from dmplex_b200 import workloads as w
+    from oracle.oracle import Oracle
+    o = Oracle(d.model_tables(g, pv_flux=PV, kinetic_energy=KE, **w.si_parameters()), threads=threads)
+    z = y.copy()
+    o.rk4_step(z, DT, 1)  # warm-up
+    steps, t0 = 0, time.perf_counter()
+    while True:
+        o.rk4_step(z, DT, 1)
+        steps += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or steps >= 1000:
+            break
+    return g.nc * steps / el, steps, el
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        self.file.flush()
+        rows = []
+        with open(self.file.name) as f:
+            for line in f:
+                parts = [s.strip() for s in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.file.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        loaded = sorted(sm)[len(sm) // 4:] if sm else []
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel):
+    """Per-launch DRAM bytes of `kernel` from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "traffic.txt")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        for line in f:
+            parts = line.split()
+            if len(parts) >= 2 and parts[0] == kernel:
+                return float(parts[1])
+    return None
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    g, y = build_workload(seed=0, level=args.level)
+    threads = os.cpu_count() or 1
+    budget = max(5.0, min(args.cpu_seconds * 4, 150.0))
+    value, steps, el = oracle_baseline(g, y, budget, threads)
+    kind = "port"
+    line = {"metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * el / steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config_dict(g, 1, args.level), "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": "cell-steps/s", "cores": threads, "kind": kind,
+                             "sample": f"{steps} RK4 steps of the workload ({el:.1f} s); CPU restatement of "
+                                       f"the reference kernels in C (Julia is not installed)"},
+            "e2e": {"value": value, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_b200(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    import dmplex_b200 as d
+    from dmplex_b200 import workloads as w
+
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        os.environ.setdefault("OMP_NUM_THREADS", str(max(1, (os.cpu_count() or 8) // world)))
+    g, y_host = build_workload(seed=rank, level=args.level)
+    m = d.TRiSKShallowWater(g, pv_flux=PV, kinetic_energy=KE, device=local_rank, **w.si_parameters())
+    stream = torch.cuda.ExternalStream(m.stream(), device=local_rank)
+    yd = torch.from_numpy(y_host).to(f"cuda:{local_rank}")
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local_rank}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # warm-up (also captures the CUDA graph)
+    m.rk4_async(yd, DT, max(args.warmup, 3))
+    m.synchronize()
+    barrier()
+    launches0 = m.launch_count()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clocks:
+        barrier()
+        start.record(stream)
+        m.rk4_async(yd, DT, args.steps)
+        end.record(stream)
+        m.synchronize()
+        barrier()
+    ms = start.elapsed_time(end)
+    launches = m.launch_count() - launches0
+    ms = max_over_ranks(ms)
+    value = world * g.nc * args.steps / (ms * 1e-3)
+
+    # e2e: the public synchronous call with a pinned host state, one step per call
+    pinned = torch.from_numpy(y_host.copy()).pin_memory()
+    ya = pinned.numpy()
+    nbytes = ya.nbytes
+    d.rk4_step(ya, DT, d.tendency, d.RK4Cache(ya), m)
+    barrier()
+    e_steps = max(1, min(args.steps, 200))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    cache = d.RK4Cache(ya)
+    for _ in range(e_steps):
+        d.rk4_step(ya, DT, d.tendency, cache, m)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e_ms = max_over_ranks(e0.elapsed_time(e1))
+    e2e = {"value": world * g.nc * e_steps / (e_ms * 1e-3), "unit": "cell-steps/s", "h2d_bytes_per_step": nbytes,
+           "d2h_bytes_per_step": nbytes, "steps": e_steps}
+
+    # roofline of the dominant kernel: a second, instrumented pass with events around
+    # every launch of the same workload
+    prof_steps = max(1, min(args.steps, 50))
+    phases = m.profile_phases(yd, DT, prof_steps)
+    nbytes_phase = m.algorithmic_bytes()
+    peak, peak_kind = measured_peak()
+    achieved = nbytes_phase["tend"] / (phases["tend"] * 1e-3) / 1e9
+    step_gbs = nbytes_phase["rk4_step"] / (ms / args.steps * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": "k_tend<gassmann,stage>", "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                "traffic": ncu_traffic("k_tend"), "algorithmic_bytes_per_launch": nbytes_phase["tend"],
+                "launch_ms": phases["tend"], "phase_ms": phases,
+                "phase_bytes": {k: nbytes_phase[k] for k in ("vertex", "flux", "tend")},
+                "step_bytes": nbytes_phase["rk4_step"], "step_gbs": step_gbs, "step_frac": step_gbs / peak}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        v, steps, el = oracle_baseline(g, y_host, args.cpu_seconds, threads)
+        cpu = {"value": v, "unit": "cell-steps/s", "cores": threads, "kind": "port",
+               "sample": f"{steps} RK4 steps of the workload ({el:.1f} s); CPU restatement of the reference "
+                         f"kernels in C with OpenMP (not Julia)"}
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": config_dict(g, world, args.level), "clocks": clocks.summary(), "e2e": e2e,
+                "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu}
+        print(json.dumps(line), flush=True)
+    del m
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        run_b200(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

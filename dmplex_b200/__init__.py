@@ -1,0 +1,17 @@
+"""dmplex_b200: the TRiSK C-grid shallow-water hot path of dmplex.jl on NVIDIA B200.
+
+The package is a thin host layer over libtrisk_b200.so (C ABI in include/trisk_b200.h):
+mesh generation and table construction in C++, the tendency and the RK4 step as
+hand-written sm_100a kernels. Names follow the reference (dmplex.jl); Julia's
+mutating ``f!`` functions are ``f`` here.
+"""
+from ._lib import TriskError
+from .mesh import HexMesh, Plex, TRiSKGrid, create_hexagon_mesh, icosahedral_mesh, lloyd
+from .model import (RK4Cache, TRiSKShallowWater, height_dofs, initial_state, model_tables, potential_enstrophy,
+                    relative_vorticity, rk4_step, tendency, total_energy, total_mass, velocity_dofs)
+
+__all__ = [
+    "TriskError", "HexMesh", "Plex", "TRiSKGrid", "create_hexagon_mesh", "icosahedral_mesh", "lloyd", "RK4Cache", "TRiSKShallowWater",
+    "height_dofs", "initial_state", "model_tables", "potential_enstrophy", "relative_vorticity", "rk4_step", "tendency",
+    "total_energy", "total_mass", "velocity_dofs",
+]

@@ -1,0 +1,356 @@
+// sm_100a kernels of the TRiSK shallow-water tendency and the RK4 stage updates.
+//
+// The reference runs 6-8 one-entity-per-thread KernelAbstractions gathers per tendency
+// (src/FiniteVolumes/TRiSKShallowWater.jl:202-305) plus 4 broadcast passes per RK4 step
+// (src/TimeSteppers/RungeKutta.jl:18-29). Here a tendency is three launches, one per
+// grid-wide dependency level:
+//
+//   k_vertex : zeta_v, h_v, q_v (TRiSK only), K_v (alpha != 1)        (:212-219, :246-259)
+//   k_flux   : edges -> F_e = h_e u_e and q_e;  cells -> B_i = K_i + g h_i
+//                                                          (:202-210, :222-244, :261-273)
+//   k_tend   : edges -> du_e (TRiSK or Gassmann PV flux - grad B);  cells -> dh_i = -div F
+//              followed by the fused RK4 stage update of that state element
+//                                                          (:275-305, RungeKutta.jl:21-27)
+//
+// Every per-entity sum keeps the reference's table-row order and association, and the
+// library is compiled with --fmad=false, so results are bitwise those of the same
+// arithmetic done serially (the CPU oracle), whatever the entity numbering.
+//
+// Memory layout in HBM: neighbour tables are int32 / FP64 "structure of arrays"
+// [k][entity] with the entity dimension padded to a multiple of 32, so a warp reads each
+// table row with one 128 B (int32) or 256 B (FP64) coalesced transaction. Tables are read
+// with evict-first (streaming) loads: they are touched once per tendency and should not
+// push the small state and work vectors (a few MB, reused across the three phases) out of
+// L2. The state and work vectors are [entity][member] so that in an ensemble one gathered
+// index serves the contiguous member values of that entity.
+//
+// Programmatic dependent launch: every kernel loads its (read-only) tables first, then
+// executes griddepcontrol.wait, and only then touches data written by the previous phase.
+// Launched with the programmatic-serialization attribute, the next phase's table stream
+// overlaps the previous phase's tail.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace trisk {
+
+constexpr int CW = 6;   // cell table width (hexagons; pentagons padded)
+constexpr int VW = 3;   // vertex table width (Voronoi vertices have three edges)
+constexpr int TWD = 10; // TRiSK table width (5 + 5 edges of the two hexagons)
+constexpr int GW = 12;  // Gassmann stencil width
+
+enum PvMode { PVM_TRISK = 0, PVM_GASSMANN = 1, PVM_GASSMANN_MEAN = 2 };
+enum KeMode { KE_CELL = 0, KE_VERTEX = 1, KE_MIXED = 2 };
+enum Epilogue { EPI_TENDENCY = 0, EPI_STAGE1 = 1, EPI_STAGE2 = 2, EPI_STAGE3 = 3, EPI_STAGE4 = 4 };
+
+struct DevTables {
+  int32_t nc, ne, nv;
+  int32_t ldc, lde, ldv;  // padded entity counts of the [k][entity] tables
+  double gravity;
+  const int32_t* cell_edges;     // CW x ldc
+  const double* divergence;      // CW x ldc
+  const double* kinetic;         // CW x ldc (alpha != 0)
+  const int32_t* cell_vertices;  // CW x ldc (alpha != 1)
+  const double* vk_kites;        // CW x ldc (alpha != 1)
+  const int32_t* edge_cells;     // 2 x lde
+  const double* edge_height;     // 2 x lde (alpha != 0)
+  const int32_t* edge_vertices;  // 2 x lde
+  const double* inverse_dual;    // lde
+  const double* vk_height;       // 2 x lde (alpha != 1)
+  const double* rhombus;         // 2 x lde (Gassmann)
+  const double* g_coriolis;      // lde (Gassmann)
+  const int32_t* trisk_edges;    // TWD x lde (TRiSK)
+  const double* trisk;           // TWD x lde (TRiSK)
+  const int32_t* g_edges;        // GW x lde (Gassmann)
+  const int32_t* g_pv_edges;     // GW x lde (Gassmann, not for the mean variant)
+  const double* g_weights;       // GW x lde (Gassmann)
+  const int32_t* vertex_edges;   // VW x ldv
+  const double* curl;            // VW x ldv
+  const int32_t* vertex_cells;   // VW x ldv
+  const double* vertex_height;   // VW x ldv
+  const double* coriolis;        // ldv
+  const double* vk_weights;      // VW x ldv (alpha != 1)
+};
+
+// Work vectors of one member group, [entity][member].
+struct DevWork {
+  double *K, *B, *F, *qe, *zv, *hv, *qv, *Kv;
+};
+
+// State pointers of one stage. y = [u (ne x M); h (nc x M)].
+struct DevStage {
+  const double* u;  // stage state read by the phases
+  const double* h;
+  double* y;    // base state (RK4) / unused for a plain tendency
+  double* acc;  // k1 + 2 k2 + 2 k3 accumulator
+  double* st;   // next stage state
+  double* dy;   // plain tendency output
+  double c;     // dt/2 (stages 1, 2) or dt (stage 3)
+  double sixth; // dt/6
+  int* flag;    // set to 1 when a non-finite state appears
+};
+
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+template <typename T>
+__device__ __forceinline__ T ldt(const T* p) {  // streaming (evict-first) table load
+  return __ldcs(p);
+}
+
+template <bool ENS>
+__device__ __forceinline__ void split(int t, int M, int& ent, int& mem) {
+  if (ENS) {
+    ent = t / M;
+    mem = t - ent * M;
+  } else {
+    ent = t;
+    mem = 0;
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// phase 1: vertices
+template <int PV, int KE, bool ENS>
+__global__ void __launch_bounds__(256) k_vertex(DevTables T, DevWork W, const double* u, const double* h, int M,
+                                                int want_qv) {
+  pdl_trigger();
+  int v, mm;
+  split<ENS>(blockIdx.x * blockDim.x + threadIdx.x, M, v, mm);
+  if (v >= T.nv) return;
+  int ve[VW], vc[VW];
+  double cu[VW], vh[VW], vkw[VW];
+  double cor = 0.0;
+#pragma unroll
+  for (int k = 0; k < VW; ++k) {
+    ve[k] = ldt(T.vertex_edges + k * T.ldv + v);
+    cu[k] = ldt(T.curl + k * T.ldv + v);
+    vc[k] = ldt(T.vertex_cells + k * T.ldv + v);
+    vh[k] = ldt(T.vertex_height + k * T.ldv + v);
+    if (KE != KE_CELL) vkw[k] = ldt(T.vk_weights + k * T.ldv + v);
+  }
+  const bool qv = PV == PVM_TRISK || want_qv;
+  if (qv) cor = ldt(T.coriolis + v);
+  pdl_wait();
+  double uu[VW], hh[VW];
+#pragma unroll
+  for (int k = 0; k < VW; ++k) {
+    uu[k] = u[(size_t)ve[k] * M + mm];
+    hh[k] = h[(size_t)vc[k] * M + mm];
+  }
+  double z = 0.0, eta = 0.0;
+#pragma unroll
+  for (int k = 0; k < VW; ++k) z += cu[k] * uu[k];
+#pragma unroll
+  for (int k = 0; k < VW; ++k) eta += vh[k] * hh[k];
+  const size_t o = (size_t)v * M + mm;
+  W.zv[o] = z;
+  W.hv[o] = eta;
+  if (qv) W.qv[o] = (z + cor) / eta;
+  if (KE != KE_CELL) {
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < VW; ++k) s += vkw[k] * (uu[k] * uu[k]);
+    W.Kv[o] = s;
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// phase 2: edges (mass flux, edge PV) and cells (Bernoulli function)
+template <int PV, int KE, bool ENS>
+__global__ void __launch_bounds__(256) k_flux(DevTables T, DevWork W, const double* u, const double* h, int M,
+                                              int nbE, int want_K) {
+  pdl_trigger();
+  if ((int)blockIdx.x < nbE) {
+    int e, mm;
+    split<ENS>(blockIdx.x * blockDim.x + threadIdx.x, M, e, mm);
+    if (e >= T.ne) return;
+    const int ev0 = ldt(T.edge_vertices + e), ev1 = ldt(T.edge_vertices + T.lde + e);
+    int ec0 = 0, ec1 = 0;
+    double eh0 = 0, eh1 = 0, vk0 = 0, vk1 = 0, r0 = 0, r1 = 0, gc = 0;
+    if (KE != KE_VERTEX) {
+      ec0 = ldt(T.edge_cells + e);
+      ec1 = ldt(T.edge_cells + T.lde + e);
+      eh0 = ldt(T.edge_height + e);
+      eh1 = ldt(T.edge_height + T.lde + e);
+    }
+    if (KE != KE_CELL) {
+      vk0 = ldt(T.vk_height + e);
+      vk1 = ldt(T.vk_height + T.lde + e);
+    }
+    if (PV != PVM_TRISK) {
+      r0 = ldt(T.rhombus + e);
+      r1 = ldt(T.rhombus + T.lde + e);
+      gc = ldt(T.g_coriolis + e);
+    }
+    pdl_wait();
+    const size_t o = (size_t)e * M + mm;
+    const size_t o0 = (size_t)ev0 * M + mm, o1 = (size_t)ev1 * M + mm;
+    const double ue = u[o];
+    double hv0 = 0, hv1 = 0;
+    if (KE != KE_CELL || PV != PVM_TRISK) {
+      hv0 = W.hv[o0];
+      hv1 = W.hv[o1];
+    }
+    double he;
+    if (KE == KE_CELL) {
+      he = eh0 * h[(size_t)ec0 * M + mm] + eh1 * h[(size_t)ec1 * M + mm];
+    } else if (KE == KE_VERTEX) {
+      he = vk0 * hv0 + vk1 * hv1;  // the reference's zero cell part adds exactly 0
+    } else {
+      he = eh0 * h[(size_t)ec0 * M + mm] + eh1 * h[(size_t)ec1 * M + mm] + vk0 * hv0 + vk1 * hv1;
+    }
+    W.F[o] = he * ue;
+    if (PV == PVM_TRISK) {
+      W.qe[o] = (W.qv[o0] + W.qv[o1]) / 2;
+    } else {
+      const double z = r0 * W.zv[o0] + r1 * W.zv[o1];
+      const double eta = r0 * hv0 + r1 * hv1;
+      W.qe[o] = (z + gc) / eta;
+    }
+  } else {
+    int i, mm;
+    split<ENS>((blockIdx.x - nbE) * blockDim.x + threadIdx.x, M, i, mm);
+    if (i >= T.nc) return;
+    int ce[CW], cv[CW];
+    double kin[CW], kk[CW];
+#pragma unroll
+    for (int k = 0; k < CW; ++k) {
+      if (KE != KE_VERTEX) {
+        ce[k] = ldt(T.cell_edges + k * T.ldc + i);
+        kin[k] = ldt(T.kinetic + k * T.ldc + i);
+      }
+      if (KE != KE_CELL) {
+        cv[k] = ldt(T.cell_vertices + k * T.ldc + i);
+        kk[k] = ldt(T.vk_kites + k * T.ldc + i);
+      }
+    }
+    pdl_wait();
+    const size_t o = (size_t)i * M + mm;
+    const double hi = h[o];
+    double K = 0.0, B;
+    if (KE != KE_VERTEX) {
+      double uk[CW];
+#pragma unroll
+      for (int k = 0; k < CW; ++k) uk[k] = u[(size_t)ce[k] * M + mm];
+#pragma unroll
+      for (int k = 0; k < CW; ++k) K += kin[k] * (uk[k] * uk[k]);
+      B = K + T.gravity * hi;
+    } else {
+      B = T.gravity * hi;  // the reference's zero cell part adds exactly 0
+    }
+    if (KE != KE_CELL) {
+      double kv[CW];
+#pragma unroll
+      for (int k = 0; k < CW; ++k) kv[k] = W.Kv[(size_t)cv[k] * M + mm];
+      double s = 0.0;
+#pragma unroll
+      for (int k = 0; k < CW; ++k) s += kk[k] * kv[k];
+      K += s;
+      B += s;
+    }
+    W.B[o] = B;
+    if (want_K) W.K[o] = K;
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// phase 3: tendencies and the RK4 stage update
+template <int EPI>
+__device__ __forceinline__ void epilogue(const DevStage& S, size_t j, double kv) {
+  if (EPI == EPI_TENDENCY) {
+    S.dy[j] = kv;
+  } else if (EPI == EPI_STAGE1) {
+    S.acc[j] = kv;
+    S.st[j] = S.y[j] + S.c * kv;
+  } else if (EPI == EPI_STAGE2 || EPI == EPI_STAGE3) {
+    S.acc[j] = S.acc[j] + 2 * kv;
+    S.st[j] = S.y[j] + S.c * kv;
+  } else {
+    const double yn = S.y[j] + S.sixth * (S.acc[j] + kv);
+    S.y[j] = yn;
+    if (!isfinite(yn)) atomicOr(S.flag, 1);
+  }
+}
+
+template <int PV, int EPI, bool ENS>
+__global__ void __launch_bounds__(256) k_tend(DevTables T, DevWork W, DevStage S, int M, int nbE) {
+  pdl_trigger();
+  if ((int)blockIdx.x < nbE) {
+    int e, mm;
+    split<ENS>(blockIdx.x * blockDim.x + threadIdx.x, M, e, mm);
+    if (e >= T.ne) return;
+    const int ec0 = ldt(T.edge_cells + e), ec1 = ldt(T.edge_cells + T.lde + e);
+    const double invd = ldt(T.inverse_dual + e);
+    const size_t o = (size_t)e * M + mm;
+    double du;
+    if (PV == PVM_TRISK) {
+      int te[TWD];
+      double tr[TWD];
+#pragma unroll
+      for (int k = 0; k < TWD; ++k) {
+        te[k] = ldt(T.trisk_edges + k * T.lde + e);
+        tr[k] = ldt(T.trisk + k * T.lde + e);
+      }
+      pdl_wait();
+      const double qself = W.qe[o];
+      double f[TWD], q[TWD];
+#pragma unroll
+      for (int k = 0; k < TWD; ++k) {
+        f[k] = W.F[(size_t)te[k] * M + mm];
+        q[k] = W.qe[(size_t)te[k] * M + mm];
+      }
+      double s = 0.0;
+#pragma unroll
+      for (int k = 0; k < TWD; ++k) s += tr[k] * f[k] * (qself + q[k]);
+      du = s / 2 - (W.B[(size_t)ec1 * M + mm] - W.B[(size_t)ec0 * M + mm]) * invd;
+    } else {
+      int ge[GW], gp[GW];
+      double gw[GW];
+#pragma unroll
+      for (int k = 0; k < GW; ++k) {
+        ge[k] = ldt(T.g_edges + k * T.lde + e);
+        if (PV == PVM_GASSMANN) gp[k] = ldt(T.g_pv_edges + k * T.lde + e);
+        gw[k] = ldt(T.g_weights + k * T.lde + e);
+      }
+      pdl_wait();
+      double f[GW], q[GW];
+      const double qself = PV == PVM_GASSMANN_MEAN ? W.qe[o] : 0.0;
+#pragma unroll
+      for (int k = 0; k < GW; ++k) {
+        f[k] = W.F[(size_t)ge[k] * M + mm];
+        if (PV == PVM_GASSMANN)
+          q[k] = W.qe[(size_t)gp[k] * M + mm];
+        else
+          q[k] = (qself + W.qe[(size_t)ge[k] * M + mm]) / 2;
+      }
+      double s = 0.0;
+#pragma unroll
+      for (int k = 0; k < GW; ++k) s += gw[k] * f[k] * q[k];
+      du = s - (W.B[(size_t)ec1 * M + mm] - W.B[(size_t)ec0 * M + mm]) * invd;
+    }
+    epilogue<EPI>(S, o, du);
+  } else {
+    int i, mm;
+    split<ENS>((blockIdx.x - nbE) * blockDim.x + threadIdx.x, M, i, mm);
+    if (i >= T.nc) return;
+    int ce[CW];
+    double dv[CW];
+#pragma unroll
+    for (int k = 0; k < CW; ++k) {
+      ce[k] = ldt(T.cell_edges + k * T.ldc + i);
+      dv[k] = ldt(T.divergence + k * T.ldc + i);
+    }
+    pdl_wait();
+    double f[CW];
+#pragma unroll
+    for (int k = 0; k < CW; ++k) f[k] = W.F[(size_t)ce[k] * M + mm];
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < CW; ++k) s += dv[k] * f[k];
+    const size_t o = (size_t)i * M + mm;
+    epilogue<EPI>(S, (size_t)T.ne * M + o, -s);
+  }
+}
+
+}  // namespace trisk

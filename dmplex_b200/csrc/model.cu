@@ -1,0 +1,1041 @@
+// TRiSK shallow-water model on one B200: table upload, the internal (Hilbert) numbering,
+// the phase launches, the CUDA-graph RK4 step and the diagnostics, behind the C ABI of
+// include/trisk_b200.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <type_traits>
+#include <vector>
+
+#include "common.hpp"
+#include "kernels.cuh"
+
+using trisk::Error;
+
+#define CUDA_CHECK(x)                                                                                   \
+  do {                                                                                                  \
+    cudaError_t err__ = (x);                                                                            \
+    if (err__ != cudaSuccess)                                                                           \
+      throw trisk::Error(TRISK_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(err__));          \
+  } while (0)
+
+namespace trisk {
+
+// ---------------------------------------------------------------------------------------
+// small kernels: state permutation, reductions, vorticity
+
+__global__ void k_gather(double* __restrict__ dst, const double* __restrict__ src, const int32_t* __restrict__ idx,
+                         int64_t n) {
+  const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (j < n) dst[j] = src[idx[j]];
+}
+
+constexpr int RED_BLOCK = 256, RED_PER_THREAD = 8;
+
+// MODE 0: a b   MODE 1: (a b)(c + g b / 2)   MODE 2: (a b)(c c)
+template <int MODE>
+__global__ void k_reduce_partial(const double* a, const double* b, const double* c, double g, int64_t n,
+                                 double* partials) {
+  __shared__ double sm[RED_BLOCK];
+  const int64_t base = (int64_t)blockIdx.x * RED_BLOCK * RED_PER_THREAD;
+  double s = 0.0;
+  for (int r = 0; r < RED_PER_THREAD; ++r) {
+    const int64_t i = base + (int64_t)r * RED_BLOCK + threadIdx.x;
+    if (i < n) {
+      double t;
+      if (MODE == 0)
+        t = a[i] * b[i];
+      else if (MODE == 1)
+        t = a[i] * b[i] * (c[i] + g * b[i] / 2);
+      else
+        t = a[i] * b[i] * (c[i] * c[i]);
+      s += t;
+    }
+  }
+  sm[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = RED_BLOCK / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) sm[threadIdx.x] += sm[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partials[blockIdx.x] = sm[0];
+}
+
+__global__ void k_reduce_final(const double* partials, int n, double* out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    double s = 0.0;
+    for (int i = 0; i < n; ++i) s += partials[i];
+    *out = s;
+  }
+}
+
+__global__ void k_vertex_curl(DevTables T, const double* u, double* zeta) {  // edge_sum_kernel! as curl
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= T.nv) return;
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < VW; ++k) s += T.curl[k * T.ldv + v] * u[T.vertex_edges[k * T.ldv + v]];
+  zeta[v] = s;
+}
+
+static inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
+static inline int64_t round_up(int64_t a, int64_t b) { return cdiv(a, b) * b; }
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) CUDA_CHECK(cudaSetDevice(dev));
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+// Host staging of all tables in one allocation (256-byte aligned pieces).
+struct Packer {
+  std::vector<char> host;
+  size_t add(size_t bytes) {
+    size_t off = (size_t)round_up((int64_t)host.size(), 256);
+    host.resize(off + bytes, 0);
+    return off;
+  }
+  template <class T>
+  T* at(size_t off) {
+    return reinterpret_cast<T*>(host.data() + off);
+  }
+};
+
+}  // namespace trisk
+
+using namespace trisk;
+
+// 1-based copies of the index tables handed out through TriskCoefficients views.
+struct CoefficientExport {
+  std::vector<int64_t> t[9];
+};
+
+// Host-side premultiplied tables (the reference constructor's output), no device.
+struct TriskTables {
+  Coefficients C;
+  CoefficientExport exported;
+};
+
+struct TriskModel {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int pv = 0, ke = 0;
+  double alpha = 1.0, gravity = 1.0;
+  int64_t nc = 0, ne = 0, nv = 0, N = 0;
+  int block = 256;
+  bool use_graph = true, use_pdl = true, identity = true;
+  Coefficients C;  // file numbering, 0-based (kept for export)
+  CoefficientExport exported;
+  std::vector<int32_t> cell_n2o, edge_n2o, vert_n2o, cell_o2n, edge_o2n, vert_o2n;
+  std::vector<void*> allocations;
+  DevTables T{};
+  DevWork W{};
+  double *y = nullptr, *acc = nullptr, *st = nullptr, *stage = nullptr, *dy = nullptr;
+  int32_t *state_n2o = nullptr, *state_o2n = nullptr, *vertex_o2n = nullptr;
+  double *area_c = nullptr, *area_v = nullptr, *partials = nullptr, *scalars = nullptr;
+  int* flag = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  double graph_dt = NAN;
+  int64_t launches = 0;
+  double table_bytes_unique = 0;
+  double phase_bytes[3] = {0, 0, 0};
+
+  ~TriskModel() {
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(device);
+    if (graph) cudaGraphExecDestroy(graph);
+    if (stream) {
+      cudaStreamSynchronize(stream);
+      cudaStreamDestroy(stream);
+    }
+    for (void* p : allocations) cudaFree(p);
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+
+  template <class T>
+  T* alloc(size_t count) {
+    void* p = nullptr;
+    CUDA_CHECK(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
+    allocations.push_back(p);
+    return static_cast<T*>(p);
+  }
+};
+
+namespace {
+
+// ---------------------------------------------------------------------------------------
+// launch helpers
+
+template <typename... KArgs, typename... Args>
+void launch(TriskModel& m, void (*kernel)(KArgs...), int64_t grid, cudaEvent_t ev0, cudaEvent_t ev1,
+            Args&&... args) {
+  if (grid <= 0) return;
+  if (ev0) CUDA_CHECK(cudaEventRecord(ev0, m.stream));
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)m.block);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = m.stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = (m.use_pdl && !ev0) ? 1 : 0;
+  CUDA_CHECK(cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...));
+  if (ev1) CUDA_CHECK(cudaEventRecord(ev1, m.stream));
+  m.launches++;
+}
+
+template <class F>
+void with_modes(int pv, int ke, F&& f) {
+  using std::integral_constant;
+  switch (pv * 3 + ke) {
+    case 0: f(integral_constant<int, 0>{}, integral_constant<int, 0>{}); break;
+    case 1: f(integral_constant<int, 0>{}, integral_constant<int, 1>{}); break;
+    case 2: f(integral_constant<int, 0>{}, integral_constant<int, 2>{}); break;
+    case 3: f(integral_constant<int, 1>{}, integral_constant<int, 0>{}); break;
+    case 4: f(integral_constant<int, 1>{}, integral_constant<int, 1>{}); break;
+    case 5: f(integral_constant<int, 1>{}, integral_constant<int, 2>{}); break;
+    case 6: f(integral_constant<int, 2>{}, integral_constant<int, 0>{}); break;
+    case 7: f(integral_constant<int, 2>{}, integral_constant<int, 1>{}); break;
+    case 8: f(integral_constant<int, 2>{}, integral_constant<int, 2>{}); break;
+    default: throw Error(TRISK_ERR_ARGUMENT, "bad scheme");
+  }
+}
+
+// One tendency: three phase launches. ev: optional 6 events (pairs around each launch).
+void enqueue_tendency(TriskModel& m, const DevStage& S, int epi, cudaEvent_t* ev = nullptr) {
+  const int64_t B = m.block;
+  const int64_t nbV = cdiv(m.nv, B), nbE = cdiv(m.ne, B), nbC = cdiv(m.nc, B);
+  with_modes(m.pv, m.ke, [&](auto pvc, auto kec) {
+    constexpr int PV = decltype(pvc)::value, KE = decltype(kec)::value;
+    launch(m, k_vertex<PV, KE, false>, nbV, ev ? ev[0] : nullptr, ev ? ev[1] : nullptr, m.T, m.W, S.u, S.h, 1, 0);
+    launch(m, k_flux<PV, KE, false>, nbE + nbC, ev ? ev[2] : nullptr, ev ? ev[3] : nullptr, m.T, m.W, S.u, S.h, 1,
+           (int)nbE, 0);
+    cudaEvent_t e0 = ev ? ev[4] : nullptr, e1 = ev ? ev[5] : nullptr;
+    switch (epi) {
+      case EPI_TENDENCY: launch(m, k_tend<PV, EPI_TENDENCY, false>, nbE + nbC, e0, e1, m.T, m.W, S, 1, (int)nbE); break;
+      case EPI_STAGE1: launch(m, k_tend<PV, EPI_STAGE1, false>, nbE + nbC, e0, e1, m.T, m.W, S, 1, (int)nbE); break;
+      case EPI_STAGE2: launch(m, k_tend<PV, EPI_STAGE2, false>, nbE + nbC, e0, e1, m.T, m.W, S, 1, (int)nbE); break;
+      case EPI_STAGE3: launch(m, k_tend<PV, EPI_STAGE3, false>, nbE + nbC, e0, e1, m.T, m.W, S, 1, (int)nbE); break;
+      default: launch(m, k_tend<PV, EPI_STAGE4, false>, nbE + nbC, e0, e1, m.T, m.W, S, 1, (int)nbE); break;
+    }
+  });
+}
+
+// One RK4 step on the internal state m.y (RungeKutta.jl:18-29). ev: optional 24 events.
+void enqueue_step(TriskModel& m, double dt, cudaEvent_t* ev = nullptr) {
+  DevStage S{};
+  S.y = m.y;
+  S.acc = m.acc;
+  S.st = m.st;
+  S.flag = m.flag;
+  S.sixth = dt / 6;
+  S.u = m.y;
+  S.h = m.y + m.ne;
+  S.c = dt / 2;
+  enqueue_tendency(m, S, EPI_STAGE1, ev);
+  S.u = m.st;
+  S.h = m.st + m.ne;
+  enqueue_tendency(m, S, EPI_STAGE2, ev ? ev + 6 : nullptr);
+  S.c = dt;
+  enqueue_tendency(m, S, EPI_STAGE3, ev ? ev + 12 : nullptr);
+  enqueue_tendency(m, S, EPI_STAGE4, ev ? ev + 18 : nullptr);
+}
+
+void ensure_graph(TriskModel& m, double dt) {
+  if (m.graph && m.graph_dt == dt) return;
+  if (m.graph) {
+    cudaGraphExecDestroy(m.graph);
+    m.graph = nullptr;
+  }
+  const int64_t before = m.launches;
+  cudaGraph_t g = nullptr;
+  CUDA_CHECK(cudaStreamBeginCapture(m.stream, cudaStreamCaptureModeThreadLocal));
+  try {
+    enqueue_step(m, dt);
+  } catch (...) {
+    cudaStreamEndCapture(m.stream, &g);
+    if (g) cudaGraphDestroy(g);
+    m.launches = before;
+    throw;
+  }
+  CUDA_CHECK(cudaStreamEndCapture(m.stream, &g));
+  m.launches = before;  // captured launches are counted when the graph is replayed
+  cudaError_t e = cudaGraphInstantiate(&m.graph, g, 0);
+  cudaGraphDestroy(g);
+  CUDA_CHECK(e);
+  m.graph_dt = dt;
+}
+
+void run_steps(TriskModel& m, double dt, int64_t nsteps) {
+  if (m.use_graph) {
+    ensure_graph(m, dt);
+    for (int64_t s = 0; s < nsteps; ++s) {
+      CUDA_CHECK(cudaGraphLaunch(m.graph, m.stream));
+      m.launches += 12;
+    }
+  } else {
+    for (int64_t s = 0; s < nsteps; ++s) enqueue_step(m, dt);
+  }
+}
+
+bool is_device_pointer(const void* p) {
+  cudaPointerAttributes a;
+  cudaError_t e = cudaPointerGetAttributes(&a, p);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+void gather(TriskModel& m, double* dst, const double* src, const int32_t* idx, int64_t n) {
+  k_gather<<<(unsigned)cdiv(n, 256), 256, 0, m.stream>>>(dst, src, idx, n);
+  CUDA_CHECK(cudaGetLastError());
+  m.launches++;
+}
+
+// file-numbered user state -> internal m.y
+void state_in(TriskModel& m, const double* y_user, double* dst) {
+  const size_t bytes = (size_t)m.N * sizeof(double);
+  if (is_device_pointer(y_user)) {
+    if (m.identity)
+      CUDA_CHECK(cudaMemcpyAsync(dst, y_user, bytes, cudaMemcpyDeviceToDevice, m.stream));
+    else
+      gather(m, dst, y_user, m.state_n2o, m.N);
+  } else {
+    if (m.identity) {
+      CUDA_CHECK(cudaMemcpyAsync(dst, y_user, bytes, cudaMemcpyHostToDevice, m.stream));
+    } else {
+      CUDA_CHECK(cudaMemcpyAsync(m.stage, y_user, bytes, cudaMemcpyHostToDevice, m.stream));
+      gather(m, dst, m.stage, m.state_n2o, m.N);
+    }
+  }
+}
+
+// internal src -> file-numbered user state
+void state_out(TriskModel& m, double* y_user, const double* src) {
+  const size_t bytes = (size_t)m.N * sizeof(double);
+  if (is_device_pointer(y_user)) {
+    if (m.identity)
+      CUDA_CHECK(cudaMemcpyAsync(y_user, src, bytes, cudaMemcpyDeviceToDevice, m.stream));
+    else
+      gather(m, y_user, src, m.state_o2n, m.N);
+  } else {
+    if (m.identity) {
+      CUDA_CHECK(cudaMemcpyAsync(y_user, src, bytes, cudaMemcpyDeviceToHost, m.stream));
+    } else {
+      gather(m, m.stage, src, m.state_o2n, m.N);
+      CUDA_CHECK(cudaMemcpyAsync(y_user, m.stage, bytes, cudaMemcpyDeviceToHost, m.stream));
+    }
+  }
+}
+
+void check_flag(TriskModel& m) {
+  int flag = 0;
+  CUDA_CHECK(cudaMemcpyAsync(&flag, m.flag, sizeof(int), cudaMemcpyDeviceToHost, m.stream));
+  CUDA_CHECK(cudaStreamSynchronize(m.stream));
+  if (flag) {
+    CUDA_CHECK(cudaMemsetAsync(m.flag, 0, sizeof(int), m.stream));
+    throw Error(TRISK_ERR_NONFINITE, "the state became non-finite");
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// model construction
+
+Coefficients coefficients_from_abi(const TriskCoefficients* c) {
+  if (!c) throw Error(TRISK_ERR_ARGUMENT, "coefficients is NULL");
+  Coefficients C;
+  C.nc = c->nc;
+  C.ne = c->ne;
+  C.nv = c->nv;
+  C.cw = c->cw;
+  C.vw = c->vw;
+  C.tw = c->tw;
+  C.pv_flux = c->pv_flux;
+  C.alpha = c->alpha;
+  C.gravity = c->gravity;
+  if (C.nc <= 0 || C.ne <= 0 || C.nv <= 0) throw Error(TRISK_ERR_ARGUMENT, "empty mesh");
+  if (C.pv_flux < 0 || C.pv_flux > 2) throw Error(TRISK_ERR_ARGUMENT, "pv_flux must be :trisk, :gassmann or :gassmann_mean");
+  auto idx = [](const int64_t* p, size_t n, int64_t bound, const char* name) {
+    if (!p) throw Error(TRISK_ERR_ARGUMENT, std::string(name) + " is NULL");
+    std::vector<int64_t> out(n);
+    for (size_t i = 0; i < n; ++i) {
+      if (p[i] < 1 || p[i] > bound)
+        throw Error(TRISK_ERR_TABLE, std::string(name) + "[" + std::to_string(i) + "] = " + std::to_string(p[i]) +
+                                         " is outside 1.." + std::to_string(bound));
+      out[i] = p[i] - 1;
+    }
+    return out;
+  };
+  auto val = [](const double* p, size_t n, const char* name) {
+    if (!p) throw Error(TRISK_ERR_ARGUMENT, std::string(name) + " is NULL");
+    return std::vector<double>(p, p + n);
+  };
+  const size_t nc = C.nc, ne = C.ne, nv = C.nv;
+  C.cell_edges = idx(c->cell_edges, C.cw * nc, C.ne, "cell_edges");
+  C.divergence = val(c->divergence, C.cw * nc, "divergence");
+  C.kinetic = val(c->kinetic, C.cw * nc, "kinetic");
+  C.edge_cells = idx(c->edge_cells, 2 * ne, C.nc, "edge_cells");
+  C.edge_height = val(c->edge_height, 2 * ne, "edge_height");
+  C.edge_vertices = idx(c->edge_vertices, 2 * ne, C.nv, "edge_vertices");
+  C.inverse_dual = val(c->inverse_dual, ne, "inverse_dual");
+  C.vertex_edges = idx(c->vertex_edges, C.vw * nv, C.ne, "vertex_edges");
+  C.curl = val(c->curl, C.vw * nv, "curl");
+  C.vertex_cells = idx(c->vertex_cells, C.vw * nv, C.nc, "vertex_cells");
+  C.vertex_height = val(c->vertex_height, C.vw * nv, "vertex_height");
+  C.coriolis = val(c->coriolis, nv, "coriolis");
+  if (C.pv_flux == PV_TRISK) {
+    C.trisk_edges = idx(c->trisk_edges, C.tw * ne, C.ne, "trisk_edges");
+    C.trisk = val(c->trisk, C.tw * ne, "trisk");
+  }
+  C.cell_areas = val(c->cell_areas, nc, "cell_areas");
+  C.vertex_areas = val(c->vertex_areas, nv, "vertex_areas");
+  if (C.pv_flux != PV_TRISK) {
+    C.g_edges = idx(c->g_edges, 12 * ne, C.ne, "g_edges");
+    C.g_pv_edges = idx(c->g_pv_edges, 12 * ne, C.ne, "g_pv_edges");
+    C.g_weights = val(c->g_weights, 12 * ne, "g_weights");
+    C.rhombus = val(c->rhombus, 2 * ne, "rhombus");
+    C.g_coriolis = val(c->g_coriolis, ne, "g_coriolis");
+  }
+  if (C.alpha != 1.0) {
+    C.vk_cell_vertices = idx(c->vk_cell_vertices, C.cw * nc, C.nv, "vk_cell_vertices");
+    C.vk_kites = val(c->vk_kites, C.cw * nc, "vk_kites");
+    C.vk_weights = val(c->vk_weights, C.vw * nv, "vk_weights");
+    C.vk_height = val(c->vk_height, 2 * ne, "vk_height");
+  }
+  return C;
+}
+
+Grid grid_from_abi(const TriskGrid* g) {
+  if (!g) throw Error(TRISK_ERR_ARGUMENT, "grid is NULL");
+  Grid G;
+  G.nc = g->nc;
+  G.ne = g->ne;
+  G.nv = g->nv;
+  G.cw = g->cw;
+  G.vw = g->vw;
+  G.tw = g->tw;
+  if (G.nc <= 0 || G.ne <= 0 || G.nv <= 0 || G.cw <= 0 || G.vw <= 0 || G.tw <= 0)
+    throw Error(TRISK_ERR_ARGUMENT, "empty grid");
+  auto v3 = [](const double* p, int64_t n, const char* name) {
+    if (!p) throw Error(TRISK_ERR_ARGUMENT, std::string(name) + " is NULL");
+    std::vector<V3> out(n);
+    std::memcpy(out.data(), p, n * sizeof(V3));
+    return out;
+  };
+  auto val = [](const double* p, size_t n, const char* name) {
+    if (!p) throw Error(TRISK_ERR_ARGUMENT, std::string(name) + " is NULL");
+    return std::vector<double>(p, p + n);
+  };
+  auto idx = [](const int64_t* p, size_t n, int64_t bound, const char* name) {
+    if (!p) throw Error(TRISK_ERR_ARGUMENT, std::string(name) + " is NULL");
+    std::vector<int64_t> out(n);
+    for (size_t i = 0; i < n; ++i) {
+      if (p[i] < 1 || p[i] > bound)
+        throw Error(TRISK_ERR_TABLE, std::string(name) + "[" + std::to_string(i) + "] is outside 1.." +
+                                         std::to_string(bound));
+      out[i] = p[i] - 1;
+    }
+    return out;
+  };
+  const size_t nc = G.nc, ne = G.ne, nv = G.nv;
+  G.centers = v3(g->centers, G.nc, "centers");
+  G.vertices = v3(g->vertices, G.nv, "vertices");
+  G.edge_points = v3(g->edge_points, G.ne, "edge_points");
+  G.edge_normals = v3(g->edge_normals, G.ne, "edge_normals");
+  G.primal_lengths = val(g->primal_lengths, ne, "primal_lengths");
+  G.dual_lengths = val(g->dual_lengths, ne, "dual_lengths");
+  G.edge_cells = idx(g->edge_cells, 2 * ne, G.nc, "edge_cells");
+  G.edge_vertices = idx(g->edge_vertices, 2 * ne, G.nv, "edge_vertices");
+  G.cell_distances = val(g->cell_distances, 2 * ne, "cell_distances");
+  G.cell_areas = val(g->cell_areas, nc, "cell_areas");
+  G.vertex_areas = val(g->vertex_areas, nv, "vertex_areas");
+  G.cell_edges = idx(g->cell_edges, G.cw * nc, G.ne, "cell_edges");
+  G.cell_signs = val(g->cell_signs, G.cw * nc, "cell_signs");
+  G.cell_vertices = idx(g->cell_vertices, G.cw * nc, G.nv, "cell_vertices");
+  G.cell_kites = val(g->cell_kites, G.cw * nc, "cell_kites");
+  G.vertex_edges = idx(g->vertex_edges, G.vw * nv, G.ne, "vertex_edges");
+  G.vertex_signs = val(g->vertex_signs, G.vw * nv, "vertex_signs");
+  G.vertex_cells = idx(g->vertex_cells, G.vw * nv, G.nc, "vertex_cells");
+  G.vertex_kites = val(g->vertex_kites, G.vw * nv, "vertex_kites");
+  G.trisk_edges = idx(g->trisk_edges, G.tw * ne, G.ne, "trisk_edges");
+  G.trisk_weights = val(g->trisk_weights, G.tw * ne, "trisk_weights");
+  return G;
+}
+
+// Internal numbering: cells along the Hilbert curve, edges by first appearance in the
+// cells' edge lists, vertices by first appearance in the edges' vertex pairs (the same
+// rule as hilbert_order, src/Topology/Ordering.jl:54-82). The permutation is integer and
+// exact; every table row keeps its order, so per-entity sums are unchanged bit for bit.
+void build_numbering(TriskModel& m, const Coefficients& C, const std::vector<V3>* centroids) {
+  const int64_t nc = C.nc, ne = C.ne, nv = C.nv;
+  std::vector<int64_t> cperm(nc);
+  for (int64_t i = 0; i < nc; ++i) cperm[i] = i;
+  if (centroids) cperm = hilbert_sort(*centroids, 16);
+  m.cell_n2o.assign(nc, 0);
+  m.cell_o2n.assign(nc, -1);
+  for (int64_t j = 0; j < nc; ++j) {
+    m.cell_n2o[j] = (int32_t)cperm[j];
+    m.cell_o2n[cperm[j]] = (int32_t)j;
+  }
+  m.edge_o2n.assign(ne, -1);
+  int32_t next = 0;
+  if (centroids) {
+    for (int64_t j = 0; j < nc; ++j) {
+      const int64_t i = cperm[j];
+      for (int k = 0; k < C.cw; ++k) {
+        if (C.divergence[i * C.cw + k] == 0.0) continue;
+        const int64_t e = C.cell_edges[i * C.cw + k];
+        if (m.edge_o2n[e] < 0) m.edge_o2n[e] = next++;
+      }
+    }
+  }
+  for (int64_t e = 0; e < ne; ++e)
+    if (m.edge_o2n[e] < 0) m.edge_o2n[e] = next++;
+  m.edge_n2o.assign(ne, 0);
+  for (int64_t e = 0; e < ne; ++e) m.edge_n2o[m.edge_o2n[e]] = (int32_t)e;
+  m.vert_o2n.assign(nv, -1);
+  next = 0;
+  if (centroids) {
+    for (int64_t j = 0; j < ne; ++j) {
+      const int64_t e = m.edge_n2o[j];
+      for (int s = 0; s < 2; ++s) {
+        const int64_t v = C.edge_vertices[2 * e + s];
+        if (m.vert_o2n[v] < 0) m.vert_o2n[v] = next++;
+      }
+    }
+  }
+  for (int64_t v = 0; v < nv; ++v)
+    if (m.vert_o2n[v] < 0) m.vert_o2n[v] = next++;
+  m.vert_n2o.assign(nv, 0);
+  for (int64_t v = 0; v < nv; ++v) m.vert_n2o[m.vert_o2n[v]] = (int32_t)v;
+  m.identity = true;
+  for (int64_t i = 0; i < nc && m.identity; ++i) m.identity = m.cell_n2o[i] == i;
+  for (int64_t e = 0; e < ne && m.identity; ++e) m.identity = m.edge_n2o[e] == e;
+}
+
+// [k][ld] int32 table in internal numbering from a [k + w*entity] file-numbered table.
+size_t pack_index(Packer& P, const std::vector<int64_t>& tab, int w, int wpad, int64_t n, int64_t ld,
+                  const std::vector<int32_t>& n2o, const std::vector<int32_t>& target_o2n) {
+  if (w > wpad) throw Error(TRISK_ERR_UNSUPPORTED, "neighbour table wider than this build supports");
+  const size_t off = P.add((size_t)wpad * ld * sizeof(int32_t));
+  int32_t* out = P.at<int32_t>(off);
+  for (int64_t j = 0; j < n; ++j) {
+    const int64_t old = n2o[j];
+    for (int k = 0; k < w; ++k) out[k * ld + j] = target_o2n[tab[old * w + k]];
+  }
+  return off;
+}
+
+size_t pack_weight(Packer& P, const std::vector<double>& tab, int w, int wpad, int64_t n, int64_t ld,
+                   const std::vector<int32_t>& n2o) {
+  if (w > wpad) throw Error(TRISK_ERR_UNSUPPORTED, "neighbour table wider than this build supports");
+  const size_t off = P.add((size_t)wpad * ld * sizeof(double));
+  double* out = P.at<double>(off);
+  for (int64_t j = 0; j < n; ++j) {
+    const int64_t old = n2o[j];
+    for (int k = 0; k < w; ++k) out[k * ld + j] = tab[old * w + k];
+  }
+  return off;
+}
+
+void upload(TriskModel& m, const Coefficients& C) {
+  const int64_t nc = C.nc, ne = C.ne, nv = C.nv;
+  const int64_t ldc = round_up(nc, 32), lde = round_up(ne, 32), ldv = round_up(nv, 32);
+  if (C.vw > VW) throw Error(TRISK_ERR_UNSUPPORTED, "vertices with more than three edges are not supported");
+  const bool cellK = C.alpha != 0.0, vertK = C.alpha != 1.0;
+  Packer P;
+  struct Off {
+    size_t ce, dv, kin, cv, vkk, ec, eh, ev, invd, vkh, rh, gc, te, tr, ge, gp, gw, ve, cu, vc, vh, cor, vkw, ac, av;
+  } o{};
+  auto& cn = m.cell_n2o;
+  auto& en = m.edge_n2o;
+  auto& vn = m.vert_n2o;
+  o.ce = pack_index(P, C.cell_edges, C.cw, CW, nc, ldc, cn, m.edge_o2n);
+  o.dv = pack_weight(P, C.divergence, C.cw, CW, nc, ldc, cn);
+  if (cellK) o.kin = pack_weight(P, C.kinetic, C.cw, CW, nc, ldc, cn);
+  if (vertK) {
+    o.cv = pack_index(P, C.vk_cell_vertices, C.cw, CW, nc, ldc, cn, m.vert_o2n);
+    o.vkk = pack_weight(P, C.vk_kites, C.cw, CW, nc, ldc, cn);
+  }
+  o.ec = pack_index(P, C.edge_cells, 2, 2, ne, lde, en, m.cell_o2n);
+  if (cellK) o.eh = pack_weight(P, C.edge_height, 2, 2, ne, lde, en);
+  o.ev = pack_index(P, C.edge_vertices, 2, 2, ne, lde, en, m.vert_o2n);
+  o.invd = pack_weight(P, C.inverse_dual, 1, 1, ne, lde, en);
+  if (vertK) o.vkh = pack_weight(P, C.vk_height, 2, 2, ne, lde, en);
+  if (C.pv_flux != PV_TRISK) {
+    o.rh = pack_weight(P, C.rhombus, 2, 2, ne, lde, en);
+    o.gc = pack_weight(P, C.g_coriolis, 1, 1, ne, lde, en);
+    o.ge = pack_index(P, C.g_edges, 12, GW, ne, lde, en, m.edge_o2n);
+    if (C.pv_flux == PV_GASSMANN) o.gp = pack_index(P, C.g_pv_edges, 12, GW, ne, lde, en, m.edge_o2n);
+    o.gw = pack_weight(P, C.g_weights, 12, GW, ne, lde, en);
+  } else {
+    o.te = pack_index(P, C.trisk_edges, C.tw, TWD, ne, lde, en, m.edge_o2n);
+    o.tr = pack_weight(P, C.trisk, C.tw, TWD, ne, lde, en);
+  }
+  o.ve = pack_index(P, C.vertex_edges, C.vw, VW, nv, ldv, vn, m.edge_o2n);
+  o.cu = pack_weight(P, C.curl, C.vw, VW, nv, ldv, vn);
+  o.vc = pack_index(P, C.vertex_cells, C.vw, VW, nv, ldv, vn, m.cell_o2n);
+  o.vh = pack_weight(P, C.vertex_height, C.vw, VW, nv, ldv, vn);
+  o.cor = pack_weight(P, C.coriolis, 1, 1, nv, ldv, vn);
+  if (vertK) o.vkw = pack_weight(P, C.vk_weights, C.vw, VW, nv, ldv, vn);
+  o.ac = pack_weight(P, C.cell_areas, 1, 1, nc, ldc, cn);
+  o.av = pack_weight(P, C.vertex_areas, 1, 1, nv, ldv, vn);
+
+  char* base = m.alloc<char>(P.host.size());
+  CUDA_CHECK(cudaMemcpy(base, P.host.data(), P.host.size(), cudaMemcpyHostToDevice));
+  auto I = [&](size_t off, bool used) { return used ? reinterpret_cast<const int32_t*>(base + off) : nullptr; };
+  auto D = [&](size_t off, bool used) { return used ? reinterpret_cast<const double*>(base + off) : nullptr; };
+  const bool g = C.pv_flux != PV_TRISK;
+  DevTables& T = m.T;
+  T.nc = (int32_t)nc;
+  T.ne = (int32_t)ne;
+  T.nv = (int32_t)nv;
+  T.ldc = (int32_t)ldc;
+  T.lde = (int32_t)lde;
+  T.ldv = (int32_t)ldv;
+  T.gravity = C.gravity;
+  T.cell_edges = I(o.ce, true);
+  T.divergence = D(o.dv, true);
+  T.kinetic = D(o.kin, cellK);
+  T.cell_vertices = I(o.cv, vertK);
+  T.vk_kites = D(o.vkk, vertK);
+  T.edge_cells = I(o.ec, true);
+  T.edge_height = D(o.eh, cellK);
+  T.edge_vertices = I(o.ev, true);
+  T.inverse_dual = D(o.invd, true);
+  T.vk_height = D(o.vkh, vertK);
+  T.rhombus = D(o.rh, g);
+  T.g_coriolis = D(o.gc, g);
+  T.trisk_edges = I(o.te, !g);
+  T.trisk = D(o.tr, !g);
+  T.g_edges = I(o.ge, g);
+  T.g_pv_edges = I(o.gp, C.pv_flux == PV_GASSMANN);
+  T.g_weights = D(o.gw, g);
+  T.vertex_edges = I(o.ve, true);
+  T.curl = D(o.cu, true);
+  T.vertex_cells = I(o.vc, true);
+  T.vertex_height = D(o.vh, true);
+  T.coriolis = D(o.cor, true);
+  T.vk_weights = D(o.vkw, vertK);
+  m.area_c = const_cast<double*>(D(o.ac, true));
+  m.area_v = const_cast<double*>(D(o.av, true));
+
+  // Algorithmic bytes: every table the scheme needs once (int32 index, FP64 weight).
+  const double I4 = 4, F8 = 8;
+  const bool tr = C.pv_flux == PV_TRISK, gm = C.pv_flux == PV_GASSMANN;
+  double cellB = CW * (I4 + F8) + (cellK ? CW * F8 : 0) + (vertK ? CW * (I4 + F8) : 0);
+  double edgeB = 2 * I4 + 2 * I4 + F8 + (cellK ? 2 * F8 : 0) + (vertK ? 2 * F8 : 0) +
+                 (tr ? TWD * (I4 + F8) : GW * (I4 + F8) + (gm ? GW * I4 : 0) + 2 * F8 + F8);
+  double vertB = VW * (I4 + F8) * 2 + (tr ? F8 : 0) + (vertK ? VW * F8 : 0);
+  m.table_bytes_unique = nc * cellB + ne * edgeB + nv * vertB;
+  // Per launch: the tables the kernel streams plus each state or work vector it reads or
+  // writes, counted once.
+  const double vV = vertB * nv + F8 * (ne + nc) + F8 * nv * (2 + (tr ? 1 : 0) + (vertK ? 1 : 0));
+  const double eFlux = ne * (2 * I4 + (cellK ? 2 * I4 + 2 * F8 : 0) + (vertK ? 2 * F8 : 0) + (tr ? 0 : 3 * F8)) +
+                       nc * ((cellK ? CW * (I4 + F8) : 0) + (vertK ? CW * (I4 + F8) : 0)) +
+                       F8 * (ne + nc) /* u, h */ + F8 * nv * ((vertK || !tr ? 1 : 0) + 1 + (vertK ? 1 : 0)) +
+                       F8 * (2 * ne + nc) /* F, qe, B */;
+  const double eTend = ne * (2 * I4 + F8 + (tr ? TWD * (I4 + F8) : GW * (I4 + F8) + (gm ? GW * I4 : 0))) +
+                       nc * CW * (I4 + F8) + F8 * (2 * ne + nc) /* F, qe, B */ + 28.0 * (ne + nc) /* RK4 update */;
+  m.phase_bytes[0] = vV;
+  m.phase_bytes[1] = eFlux;
+  m.phase_bytes[2] = eTend;
+}
+
+void finish_create(TriskModel& m, const Coefficients& C, const std::vector<V3>* centroids, const TriskConfig* cfg) {
+  m.nc = C.nc;
+  m.ne = C.ne;
+  m.nv = C.nv;
+  m.N = C.ne + C.nc;
+  m.pv = C.pv_flux;
+  m.alpha = C.alpha;
+  m.gravity = C.gravity;
+  m.ke = C.alpha == 1.0 ? KE_CELL : (C.alpha == 0.0 ? KE_VERTEX : KE_MIXED);
+  if (cfg) {
+    m.use_graph = cfg->use_graph != 0;
+    m.use_pdl = cfg->use_pdl != 0;
+    if (cfg->block) {
+      if (cfg->block % 32 != 0 || cfg->block < 64 || cfg->block > 256)
+        throw Error(TRISK_ERR_ARGUMENT, "block must be a multiple of 32 in 64..256");
+      m.block = cfg->block;
+    }
+  }
+  if (m.nc >= (1LL << 30) || m.ne >= (1LL << 30)) throw Error(TRISK_ERR_UNSUPPORTED, "mesh too large for int32 tables");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    throw Error(TRISK_ERR_CUDA, "no CUDA device is available");
+  }
+  if (m.device < 0 || m.device >= ndev) throw Error(TRISK_ERR_ARGUMENT, "device ordinal out of range");
+  DeviceGuard guard(m.device);
+  CUDA_CHECK(cudaStreamCreateWithFlags(&m.stream, cudaStreamNonBlocking));
+  build_numbering(m, C, centroids);
+  upload(m, C);
+  m.W.K = m.alloc<double>(m.nc);
+  m.W.B = m.alloc<double>(m.nc);
+  m.W.F = m.alloc<double>(m.ne);
+  m.W.qe = m.alloc<double>(m.ne);
+  m.W.zv = m.alloc<double>(m.nv);
+  m.W.hv = m.alloc<double>(m.nv);
+  m.W.qv = m.alloc<double>(m.nv);
+  m.W.Kv = m.alloc<double>(m.nv);
+  m.y = m.alloc<double>(m.N);
+  m.acc = m.alloc<double>(m.N);
+  m.st = m.alloc<double>(m.N);
+  m.stage = m.alloc<double>(m.N);
+  m.dy = m.alloc<double>(m.N);
+  m.flag = m.alloc<int>(1);
+  m.scalars = m.alloc<double>(4);
+  m.partials = m.alloc<double>(cdiv(std::max(m.nc, m.nv), RED_BLOCK * RED_PER_THREAD) + 1);
+  CUDA_CHECK(cudaMemset(m.flag, 0, sizeof(int)));
+  CUDA_CHECK(cudaMemset(m.W.K, 0, m.nc * sizeof(double)));
+  // state permutation: internal state index -> file index and back
+  std::vector<int32_t> n2o(m.N), o2n(m.N);
+  for (int64_t j = 0; j < m.ne; ++j) n2o[j] = m.edge_n2o[j];
+  for (int64_t j = 0; j < m.nc; ++j) n2o[m.ne + j] = (int32_t)(m.ne + m.cell_n2o[j]);
+  for (int64_t j = 0; j < m.N; ++j) o2n[n2o[j]] = (int32_t)j;
+  m.state_n2o = m.alloc<int32_t>(m.N);
+  m.state_o2n = m.alloc<int32_t>(m.N);
+  m.vertex_o2n = m.alloc<int32_t>(m.nv);
+  CUDA_CHECK(cudaMemcpy(m.state_n2o, n2o.data(), m.N * sizeof(int32_t), cudaMemcpyHostToDevice));
+  CUDA_CHECK(cudaMemcpy(m.state_o2n, o2n.data(), m.N * sizeof(int32_t), cudaMemcpyHostToDevice));
+  CUDA_CHECK(cudaMemcpy(m.vertex_o2n, m.vert_o2n.data(), m.nv * sizeof(int32_t), cudaMemcpyHostToDevice));
+  m.C = C;
+  CUDA_CHECK(cudaDeviceSynchronize());
+}
+
+TriskModel* checked(TriskModel* m) {
+  if (!m) throw Error(TRISK_ERR_ARGUMENT, "model is NULL");
+  return m;
+}
+
+template <int MODE>
+double reduce(TriskModel& m, const double* a, const double* b, const double* c, double g, int64_t n) {
+  const int nb = (int)cdiv(n, RED_BLOCK * RED_PER_THREAD);
+  k_reduce_partial<MODE><<<nb, RED_BLOCK, 0, m.stream>>>(a, b, c, g, n, m.partials);
+  k_reduce_final<<<1, 32, 0, m.stream>>>(m.partials, nb, m.scalars);
+  CUDA_CHECK(cudaGetLastError());
+  m.launches += 2;
+  double out = 0;
+  CUDA_CHECK(cudaMemcpyAsync(&out, m.scalars, sizeof(double), cudaMemcpyDeviceToHost, m.stream));
+  CUDA_CHECK(cudaStreamSynchronize(m.stream));
+  return out;
+}
+
+void export_coefficients(const Coefficients& C, CoefficientExport& keep, TriskCoefficients* out) {
+  auto p1 = [](const std::vector<int64_t>& v, std::vector<int64_t>& k) -> const int64_t* {
+    if (v.empty()) return nullptr;
+    k.resize(v.size());
+    for (size_t i = 0; i < v.size(); ++i) k[i] = v[i] + 1;
+    return k.data();
+  };
+  auto d = [](const std::vector<double>& v) -> const double* { return v.empty() ? nullptr : v.data(); };
+  std::memset(out, 0, sizeof(*out));
+  out->nc = C.nc;
+  out->ne = C.ne;
+  out->nv = C.nv;
+  out->cw = C.cw;
+  out->vw = C.vw;
+  out->tw = C.tw;
+  out->pv_flux = C.pv_flux;
+  out->alpha = C.alpha;
+  out->gravity = C.gravity;
+  out->cell_edges = p1(C.cell_edges, keep.t[0]);
+  out->divergence = d(C.divergence);
+  out->kinetic = d(C.kinetic);
+  out->edge_cells = p1(C.edge_cells, keep.t[1]);
+  out->edge_height = d(C.edge_height);
+  out->edge_vertices = p1(C.edge_vertices, keep.t[2]);
+  out->inverse_dual = d(C.inverse_dual);
+  out->vertex_edges = p1(C.vertex_edges, keep.t[3]);
+  out->curl = d(C.curl);
+  out->vertex_cells = p1(C.vertex_cells, keep.t[4]);
+  out->vertex_height = d(C.vertex_height);
+  out->coriolis = d(C.coriolis);
+  out->trisk_edges = p1(C.trisk_edges, keep.t[5]);
+  out->trisk = d(C.trisk);
+  out->cell_areas = d(C.cell_areas);
+  out->vertex_areas = d(C.vertex_areas);
+  out->g_edges = p1(C.g_edges, keep.t[6]);
+  out->g_pv_edges = p1(C.g_pv_edges, keep.t[7]);
+  out->g_weights = d(C.g_weights);
+  out->rhombus = d(C.rhombus);
+  out->g_coriolis = d(C.g_coriolis);
+  out->vk_cell_vertices = p1(C.vk_cell_vertices, keep.t[8]);
+  out->vk_kites = d(C.vk_kites);
+  out->vk_weights = d(C.vk_weights);
+  out->vk_height = d(C.vk_height);
+}
+
+}  // namespace
+
+extern "C" {
+
+int trisk_model_create(const TriskGrid* grid, const TriskConfig* cfg, TriskModel** out) {
+  TRISK_API_BEGIN
+  if (!out || !cfg) throw Error(TRISK_ERR_ARGUMENT, "NULL argument");
+  *out = nullptr;
+  Grid G = grid_from_abi(grid);
+  if (!(cfg->alpha == cfg->alpha)) throw Error(TRISK_ERR_ARGUMENT, "kinetic_energy weight is NaN");
+  Coefficients C = build_coefficients(G, cfg->pv_flux, cfg->alpha, cfg->gravity, cfg->omega,
+                                      cfg->coriolis_vertices, cfg->coriolis_edges);
+  auto m = std::make_unique<TriskModel>();
+  m->device = cfg->device;
+  std::vector<V3> centroids;
+  if (cfg->reorder) {  // centroid of the cell's vertices, as hilbert_permutation takes it
+    centroids.resize(G.nc);
+    for (int64_t i = 0; i < G.nc; ++i) {
+      V3 s{0, 0, 0};
+      int n = 0;
+      for (int k = 0; k < G.cw; ++k)
+        if (G.cell_signs[i * G.cw + k] != 0.0) {
+          s = s + G.vertices[G.cell_vertices[i * G.cw + k]];
+          ++n;
+        }
+      centroids[i] = s / (double)n;
+    }
+  }
+  finish_create(*m, C, cfg->reorder ? &centroids : nullptr, cfg);
+  *out = m.release();
+  TRISK_API_END
+}
+
+int trisk_model_create_from_coefficients(const TriskCoefficients* coefficients, const TriskConfig* cfg,
+                                         TriskModel** out) {
+  TRISK_API_BEGIN
+  if (!out || !cfg) throw Error(TRISK_ERR_ARGUMENT, "NULL argument");
+  *out = nullptr;
+  Coefficients C = coefficients_from_abi(coefficients);
+  auto m = std::make_unique<TriskModel>();
+  m->device = cfg->device;
+  std::vector<V3> centroids;
+  const bool reorder = cfg->reorder && cfg->cell_positions;
+  if (reorder) {
+    centroids.resize(C.nc);
+    std::memcpy(centroids.data(), cfg->cell_positions, C.nc * sizeof(V3));
+  }
+  finish_create(*m, C, reorder ? &centroids : nullptr, cfg);
+  *out = m.release();
+  TRISK_API_END
+}
+
+void trisk_model_destroy(TriskModel* model) { delete model; }
+
+int trisk_model_coefficients(TriskModel* model, TriskCoefficients* out) {
+  TRISK_API_BEGIN
+  TriskModel& m = *checked(model);
+  if (!out) throw Error(TRISK_ERR_ARGUMENT, "out is NULL");
+  export_coefficients(m.C, m.exported, out);
+  TRISK_API_END
+}
+
+int trisk_tables_create(const TriskGrid* grid, const TriskConfig* cfg, TriskTables** out) {
+  TRISK_API_BEGIN
+  if (!out || !cfg) throw Error(TRISK_ERR_ARGUMENT, "NULL argument");
+  *out = nullptr;
+  Grid G = grid_from_abi(grid);
+  if (!(cfg->alpha == cfg->alpha)) throw Error(TRISK_ERR_ARGUMENT, "kinetic_energy weight is NaN");
+  auto t = std::make_unique<TriskTables>();
+  t->C = build_coefficients(G, cfg->pv_flux, cfg->alpha, cfg->gravity, cfg->omega, cfg->coriolis_vertices,
+                            cfg->coriolis_edges);
+  *out = t.release();
+  TRISK_API_END
+}
+
+int trisk_tables_view(TriskTables* tables, TriskCoefficients* out) {
+  TRISK_API_BEGIN
+  if (!tables || !out) throw Error(TRISK_ERR_ARGUMENT, "NULL argument");
+  export_coefficients(tables->C, tables->exported, out);
+  TRISK_API_END
+}
+
+void trisk_tables_destroy(TriskTables* tables) { delete tables; }
+
+int trisk_model_sizes(TriskModel* model, int64_t sizes[3]) {
+  TRISK_API_BEGIN
+  TriskModel& m = *checked(model);
+  sizes[0] = m.nc;
+  sizes[1] = m.ne;
+  sizes[2] = m.nv;
+  TRISK_API_END
+}
+
+int trisk_tendency(TriskModel* model, const double* y, double* dy) {
+  TRISK_API_BEGIN
+  TriskModel& m = *checked(model);
+  if (!y || !dy) throw Error(TRISK_ERR_ARGUMENT, "NULL state");
+  DeviceGuard guard(m.device);
+  state_in(m, y, m.y);
+  DevStage S{};
+  S.u = m.y;
+  S.h = m.y + m.ne;
+  S.dy = m.dy;
+  S.flag = m.flag;
+  enqueue_tendency(m, S, EPI_TENDENCY);
+  state_out(m, dy, m.dy);
+  CUDA_CHECK(cudaStreamSynchronize(m.stream));
+  TRISK_API_END
+}
+
+int trisk_rk4_step_async(TriskModel* model, double* y, double dt, int64_t nsteps) {
+  TRISK_API_BEGIN
+  TriskModel& m = *checked(model);
+  if (!y) throw Error(TRISK_ERR_ARGUMENT, "NULL state");
+  if (nsteps < 0) throw Error(TRISK_ERR_ARGUMENT, "nsteps must be non-negative");
+  if (!std::isfinite(dt)) throw Error(TRISK_ERR_ARGUMENT, "dt must be finite");
+  DeviceGuard guard(m.device);
+  if (!is_device_pointer(y)) throw Error(TRISK_ERR_ARGUMENT, "trisk_rk4_step_async needs a device state");
+  if (nsteps == 0) return TRISK_OK;
+  state_in(m, y, m.y);
+  run_steps(m, dt, nsteps);
+  state_out(m, y, m.y);
+  TRISK_API_END
+}
+
+int trisk_rk4_step(TriskModel* model, double* y, double dt, int64_t nsteps) {
+  TRISK_API_BEGIN
+  TriskModel& m = *checked(model);
+  if (!y) throw Error(TRISK_ERR_ARGUMENT, "NULL state");
+  if (nsteps < 0) throw Error(TRISK_ERR_ARGUMENT, "nsteps must be non-negative");
+  if (!std::isfinite(dt)) throw Error(TRISK_ERR_ARGUMENT, "dt must be finite");
+  DeviceGuard guard(m.device);
+  if (nsteps == 0) return TRISK_OK;
+  state_in(m, y, m.y);
+  run_steps(m, dt, nsteps);
+  state_out(m, y, m.y);
+  check_flag(m);
+  TRISK_API_END
+}
+
+int trisk_synchronize(TriskModel* model) {
+  TRISK_API_BEGIN
+  TriskModel& m = *checked(model);
+  DeviceGuard guard(m.device);
+  check_flag(m);
+  TRISK_API_END
+}
+
+int trisk_diagnostics(TriskModel* model, const double* y, double* mass, double* energy, double* enstrophy) {
+  TRISK_API_BEGIN
+  TriskModel& m = *checked(model);
+  if (!y) throw Error(TRISK_ERR_ARGUMENT, "NULL state");
+  DeviceGuard guard(m.device);
+  state_in(m, y, m.y);
+  const double* u = m.y;
+  const double* h = m.y + m.ne;
+  if (mass) *mass = reduce<0>(m, m.area_c, h, nullptr, 0.0, m.nc);
+  const int64_t B = m.block;
+  const bool saved = m.use_pdl;
+  m.use_pdl = false;
+  try {
+    if (energy) {  // kinetic_energy! then sum A h (K + g h / 2)   (TRiSKShallowWater.jl:406-411)
+      with_modes(m.pv, m.ke, [&](auto pvc, auto kec) {
+        constexpr int PV = decltype(pvc)::value, KE = decltype(kec)::value;
+        launch(m, k_vertex<PV, KE, false>, cdiv(m.nv, B), nullptr, nullptr, m.T, m.W, u, h, 1, 0);
+        launch(m, k_flux<PV, KE, false>, cdiv(m.nc, B), nullptr, nullptr, m.T, m.W, u, h, 1, 0, 1);
+      });
+      *energy = reduce<1>(m, m.area_c, h, m.W.K, m.gravity, m.nc);
+    }
+    if (enstrophy) {  // vertex_pv! then sum A_v h_v q_v^2 / 2   (:414-419)
+      with_modes(m.pv, m.ke, [&](auto pvc, auto kec) {
+        constexpr int PV = decltype(pvc)::value, KE = decltype(kec)::value;
+        launch(m, k_vertex<PV, KE, false>, cdiv(m.nv, B), nullptr, nullptr, m.T, m.W, u, h, 1, 1);
+      });
+      *enstrophy = reduce<2>(m, m.area_v, m.W.hv, m.W.qv, 0.0, m.nv) / 2;
+    }
+  } catch (...) {
+    m.use_pdl = saved;
+    throw;
+  }
+  m.use_pdl = saved;
+  TRISK_API_END
+}
+
+int trisk_relative_vorticity(TriskModel* model, const double* y, double* zeta) {
+  TRISK_API_BEGIN
+  TriskModel& m = *checked(model);
+  if (!y || !zeta) throw Error(TRISK_ERR_ARGUMENT, "NULL argument");
+  DeviceGuard guard(m.device);
+  state_in(m, y, m.y);
+  k_vertex_curl<<<(unsigned)cdiv(m.nv, 256), 256, 0, m.stream>>>(m.T, m.y, m.W.zv);
+  CUDA_CHECK(cudaGetLastError());
+  m.launches++;
+  // zeta_file[v] = zeta_int[o2n[v]]
+  gather(m, m.st, m.W.zv, m.vertex_o2n, m.nv);
+  if (is_device_pointer(zeta))
+    CUDA_CHECK(cudaMemcpyAsync(zeta, m.st, m.nv * sizeof(double), cudaMemcpyDeviceToDevice, m.stream));
+  else
+    CUDA_CHECK(cudaMemcpyAsync(zeta, m.st, m.nv * sizeof(double), cudaMemcpyDeviceToHost, m.stream));
+  CUDA_CHECK(cudaStreamSynchronize(m.stream));
+  TRISK_API_END
+}
+
+int trisk_model_stream(TriskModel* model, void** stream) {
+  TRISK_API_BEGIN
+  TriskModel& m = *checked(model);
+  if (!stream) throw Error(TRISK_ERR_ARGUMENT, "NULL argument");
+  *stream = (void*)m.stream;
+  TRISK_API_END
+}
+
+int64_t trisk_launch_count(TriskModel* model) { return model ? model->launches : -1; }
+
+int trisk_model_bytes(TriskModel* model, double out[4]) {
+  TRISK_API_BEGIN
+  TriskModel& m = *checked(model);
+  out[0] = m.phase_bytes[0];
+  out[1] = m.phase_bytes[1];
+  out[2] = m.phase_bytes[2];
+  const double N = 8.0 * (double)m.N;
+  out[3] = 4 * (m.table_bytes_unique + 2 * N) + 15 * N;
+  TRISK_API_END
+}
+
+int trisk_profile_phases(TriskModel* model, double* y, double dt, int64_t nsteps, double ms[3]) {
+  TRISK_API_BEGIN
+  TriskModel& m = *checked(model);
+  if (!y || !ms || nsteps <= 0) throw Error(TRISK_ERR_ARGUMENT, "bad argument");
+  DeviceGuard guard(m.device);
+  if (!is_device_pointer(y)) throw Error(TRISK_ERR_ARGUMENT, "trisk_profile_phases needs a device state");
+  cudaEvent_t ev[24];
+  for (auto& e : ev) CUDA_CHECK(cudaEventCreate(&e));
+  double acc[3] = {0, 0, 0};
+  try {
+    state_in(m, y, m.y);
+    for (int64_t s = 0; s < nsteps; ++s) {
+      enqueue_step(m, dt, ev);
+      CUDA_CHECK(cudaStreamSynchronize(m.stream));
+      for (int t = 0; t < 4; ++t)
+        for (int p = 0; p < 3; ++p) {
+          float f = 0;
+          CUDA_CHECK(cudaEventElapsedTime(&f, ev[6 * t + 2 * p], ev[6 * t + 2 * p + 1]));
+          acc[p] += f;
+        }
+    }
+    state_out(m, y, m.y);
+    CUDA_CHECK(cudaStreamSynchronize(m.stream));
+  } catch (...) {
+    for (auto& e : ev) cudaEventDestroy(e);
+    throw;
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  for (int p = 0; p < 3; ++p) ms[p] = acc[p] / (4.0 * nsteps);
+  TRISK_API_END
+}
+
+}  // extern "C"

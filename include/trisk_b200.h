@@ -1,0 +1,209 @@
+/*
+ * trisk_b200.h - C ABI of libtrisk_b200.so, the B200 (sm_100a) implementation of the
+ * TRiSK C-grid shallow-water hot path of dmplex.jl.
+ *
+ * In dmplex.jl the path sits behind Julia generic functions, not an FFI:
+ *   tendency!(dy, y, m::TRiSKShallowWater)          src/FiniteVolumes/TRiSKShallowWater.jl:379
+ *   rk4_step!(y, dt, tendency!, cache, model)       src/TimeSteppers/RungeKutta.jl:18
+ * The entry points below are what a `ccall` shim binds in their place (the shim is in
+ * INTEGRATION.md). Conventions shared by every entry point:
+ *   - State y = [u_1..u_ne; h_1..h_nc] in file (Plex) numbering, FP64, exactly the
+ *     reference's layout (TRiSKShallowWater.jl:172-174).
+ *   - Tables are passed as Julia holds them: column-major [k, entity] (k fastest),
+ *     Int64 indices 1-based, padded entries index 1 / weight 0.
+ *   - Pointers to state may be host or device memory; the library tells them apart.
+ *   - Every function returns a status (TRISK_OK = 0); trisk_last_error() gives the
+ *     message of the last failure on the calling thread. No C++ exception crosses the ABI.
+ *   - A model is not re-entrant (like the reference model, whose work vectors the tendency
+ *     mutates): calls on one model must be serialized. Each model owns one CUDA stream.
+ */
+#ifndef TRISK_B200_H
+#define TRISK_B200_H
+#include <stddef.h>
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes --------------------------------------------------------------- */
+enum {
+  TRISK_OK = 0,
+  TRISK_ERR_ARGUMENT = 1,    /* bad argument (the reference raises ArgumentError) */
+  TRISK_ERR_TABLE = 2,       /* a neighbour table fails the upload bounds check */
+  TRISK_ERR_CUDA = 3,        /* a CUDA call failed, or no GPU */
+  TRISK_ERR_NONFINITE = 4,   /* the state became non-finite during the call */
+  TRISK_ERR_TIMEOUT = 5,     /* a bounded device wait gave up */
+  TRISK_ERR_UNSUPPORTED = 6, /* valid input this build does not handle */
+  TRISK_ERR_MESH = 7         /* mesh generation or grid construction failed */
+};
+enum { TRISK_PV_TRISK = 0, TRISK_PV_GASSMANN = 1, TRISK_PV_GASSMANN_MEAN = 2 };
+
+/* Copies the last error message of this thread into buf (always NUL-terminated);
+ * returns its full length. */
+size_t trisk_last_error(char* buf, size_t len);
+int32_t trisk_abi_version(void);
+/* sizeof of the structs below, so a binding can check its layout */
+int32_t trisk_struct_size(int32_t which); /* 0 TriskGrid, 1 TriskCoefficients, 2 TriskConfig, 3 TriskPlex */
+
+/* ---- mesh generation (set-up, host) ------------------------------------------------
+ * Replaces create_hexagon_mesh(n; centroidal)   src/Grids/Hexagonal.jl:11-17
+ * (with create_spherical_mesh + lloyd!           src/Grids/Icosahedral.jl:22-61,126-183)
+ * and TRiSKGrid(dm; centers)                     src/FiniteVolumes/TRiSKGrid.jl:76-162,
+ * with centers = the icosahedral generators as the reference's examples pass them
+ * (examples/trisk_shallow_water.jl:50-52). */
+typedef struct TriskMesh TriskMesh;
+
+typedef struct { /* Plex (src/Topology/Plex.jl:23-34), 1-based point numbers */
+  int64_t nc, ne, nv, ncones;
+  const int64_t* cone_offsets;      /* nc+ne+nv+1, 1-based offsets into cones */
+  const int64_t* cones;             /* ncones */
+  const int64_t* cone_orientations; /* ncones: 0 or -1 */
+  const int64_t* support_offsets;   /* nc+ne+nv+1 */
+  const int64_t* supports;          /* ncones */
+  const double* coordinates;        /* 3 x nv */
+} TriskPlex;
+
+typedef struct { /* TRiSKGrid (src/FiniteVolumes/TRiSKGrid.jl:37-60) */
+  int64_t nc, ne, nv;
+  int32_t cw, vw, tw, pad_;
+  const double* centers;      /* 3 x nc */
+  const double* vertices;     /* 3 x nv */
+  const double* edge_points;  /* 3 x ne */
+  const double* edge_normals; /* 3 x ne */
+  const double* primal_lengths, *dual_lengths; /* ne */
+  const int64_t* edge_cells;     /* 2 x ne */
+  const int64_t* edge_vertices;  /* 2 x ne */
+  const double* cell_distances;  /* 2 x ne */
+  const double* cell_areas;      /* nc */
+  const double* vertex_areas;    /* nv */
+  const int64_t* cell_edges;     /* cw x nc */
+  const double* cell_signs;
+  const int64_t* cell_vertices;
+  const double* cell_kites;
+  const int64_t* vertex_edges;   /* vw x nv */
+  const double* vertex_signs;
+  const int64_t* vertex_cells;
+  const double* vertex_kites;
+  const int64_t* trisk_edges;    /* tw x ne */
+  const double* trisk_weights;
+} TriskGrid;
+
+/* spring_beta > 0 relaxes every bisection level by spring dynamics (Icosahedral.jl:49-56,
+ * 78-109), 0 leaves it off; centroidal != 0 runs Lloyd's algorithm after every level. */
+int trisk_mesh_create_hexagon(int32_t subdivisions, int32_t centroidal, double spring_beta, TriskMesh** out);
+void trisk_mesh_destroy(TriskMesh* mesh);
+/* The hexagon Plex (views into mesh-owned memory, valid until trisk_mesh_destroy). */
+int trisk_mesh_plex(TriskMesh* mesh, TriskPlex* out);
+/* The icosahedral generators (3 x nc), the `centers` of the reference's examples. */
+int trisk_mesh_generators(TriskMesh* mesh, const double** out);
+/* TRiSKGrid(dm; centers=generators) (views into mesh-owned memory). */
+int trisk_mesh_grid(TriskMesh* mesh, TriskGrid* out);
+/* create_spherical_mesh(n; spring_beta, centroidal) before plex_from_polygons
+ * (Icosahedral.jl:22-58): x gets 3 x (10*4^n+2) coordinates, triangles 3 x 20*4^n 1-based
+ * vertex indices. */
+int trisk_icosahedral_mesh(int32_t subdivisions, int32_t centroidal, double spring_beta, double* x,
+                           int64_t* triangles);
+/* lloyd!(x, triangles; fixed=1:n_fixed, history) (Icosahedral.jl:126-183), in place on
+ * 3 x n coordinates; iterations gets the count. */
+int trisk_lloyd(double* x, int64_t n, const int64_t* triangles, int64_t nt, int32_t n_fixed, int32_t history,
+                int32_t* iterations);
+/* hilbert_permutation(dm) (src/Topology/Ordering.jl:85-92), 1-based, nc entries. */
+int trisk_mesh_hilbert_permutation(TriskMesh* mesh, int64_t* perm);
+/* orthogonality_defect(dm, centers) (src/Grids/CellCenters.jl:90-101). */
+int trisk_mesh_orthogonality_defect(TriskMesh* mesh, double* out);
+/* vertex_edge_areas(g) (TRiSKGrid.jl:179-191): by_vertex vw x nv, by_edge 2 x ne. */
+int trisk_mesh_vertex_edge_areas(TriskMesh* mesh, double* by_vertex, double* by_edge);
+/* gassmann_coefficients(g) (TRiSKGrid.jl:214-251): 12 x ne each, 1-based indices. */
+int trisk_mesh_gassmann(TriskMesh* mesh, int64_t* edges, int64_t* pv_edges, double* weights);
+
+/* ---- model ---------------------------------------------------------------------------
+ * Replaces TRiSKShallowWater(grid; gravity, coriolis, pv_flux, kinetic_energy, backend)
+ * src/FiniteVolumes/TRiSKShallowWater.jl:94-170 (serial distribution). */
+typedef struct {
+  int32_t pv_flux;  /* TRISK_PV_*; :trisk, :gassmann, :gassmann_mean */
+  int32_t reorder;  /* 1: renumber cells along the Hilbert curve, edges and vertices by
+                       first appearance, inside the library (results stay in file numbering) */
+  double alpha;     /* kinetic_energy: 1 :cell, 0 :vertex, 3/8 :mixed, any real */
+  double gravity;   /* the reference's `gravity` (1 on the unit sphere) */
+  double omega;     /* coriolis(x) = 2 omega x[3] when the arrays below are NULL */
+  const double* coriolis_vertices; /* nv values of coriolis(x_v), or NULL */
+  const double* coriolis_edges;    /* ne values of coriolis(edge point), or NULL */
+  const double* cell_positions;    /* 3 x nc points for the Hilbert order (from-coefficient
+                                      creation only; NULL: keep the cell numbering) */
+  int32_t device;   /* CUDA device ordinal */
+  int32_t use_graph;/* 1: capture the RK4 step as a CUDA graph (default) */
+  int32_t use_pdl;  /* 1: programmatic dependent launch between the phases (default) */
+  int32_t block;    /* threads per block of the phase kernels (0: 256) */
+} TriskConfig;
+
+/* The premultiplied tables a TRiSKShallowWater model holds (TRiSKShallowWater.jl:67-92),
+ * 1-based Int64, column-major. Gassmann members NULL for :trisk; vk_* NULL for alpha == 1. */
+typedef struct {
+  int64_t nc, ne, nv;
+  int32_t cw, vw, tw;
+  int32_t pv_flux;
+  double alpha;
+  double gravity;
+  const int64_t* cell_edges;   const double* divergence;   const double* kinetic;
+  const int64_t* edge_cells;   const double* edge_height;
+  const int64_t* edge_vertices; const double* inverse_dual;
+  const int64_t* vertex_edges; const double* curl;
+  const int64_t* vertex_cells; const double* vertex_height; const double* coriolis;
+  const int64_t* trisk_edges;  const double* trisk;
+  const double* cell_areas;    const double* vertex_areas;
+  const int64_t* g_edges;      const int64_t* g_pv_edges;   const double* g_weights;
+  const double* rhombus;       const double* g_coriolis;
+  const int64_t* vk_cell_vertices; const double* vk_kites;
+  const double* vk_weights;    const double* vk_height;
+} TriskCoefficients;
+
+typedef struct TriskModel TriskModel;
+typedef struct TriskTables TriskTables;
+
+/* Host-only restatement of the constructor's table arithmetic (TRiSKShallowWater.jl:103-158
+ * with gassmann_coefficients and vertex_edge_areas): the premultiplied tables of a model,
+ * built on the CPU without a device. The view stays valid until trisk_tables_destroy. */
+int trisk_tables_create(const TriskGrid* grid, const TriskConfig* config, TriskTables** out);
+int trisk_tables_view(TriskTables* tables, TriskCoefficients* out);
+void trisk_tables_destroy(TriskTables* tables);
+
+/* Builds the coefficients from TRiSKGrid arrays (as the reference's constructor does) and
+ * uploads them once as int32/FP64 device tables. */
+int trisk_model_create(const TriskGrid* grid, const TriskConfig* config, TriskModel** out);
+/* Uploads the coefficient arrays of an existing TRiSKShallowWater model unchanged. */
+int trisk_model_create_from_coefficients(const TriskCoefficients* coefficients, const TriskConfig* config,
+                                         TriskModel** out);
+void trisk_model_destroy(TriskModel* model);
+/* The model's coefficient tables in the reference layout (host views, file numbering). */
+int trisk_model_coefficients(TriskModel* model, TriskCoefficients* out);
+/* nc, ne, nv; state length = ne + nc */
+int trisk_model_sizes(TriskModel* model, int64_t sizes[3]);
+
+/* tendency!(dy, y, m)   TRiSKShallowWater.jl:379-394. Synchronous. */
+int trisk_tendency(TriskModel* model, const double* y, double* dy);
+/* nsteps x rk4_step!(y, dt, tendency!, cache, m)   RungeKutta.jl:18-29, in place.
+ * Synchronous; returns TRISK_ERR_NONFINITE if y became non-finite. */
+int trisk_rk4_step(TriskModel* model, double* y, double dt, int64_t nsteps);
+/* Same, asynchronous on the model's stream; y must be device memory. */
+int trisk_rk4_step_async(TriskModel* model, double* y, double dt, int64_t nsteps);
+/* Waits for the model's stream; reports a non-finite state seen since the last check. */
+int trisk_synchronize(TriskModel* model);
+/* total_mass, total_energy, potential_enstrophy   TRiSKShallowWater.jl:397-419. */
+int trisk_diagnostics(TriskModel* model, const double* y, double* mass, double* energy, double* enstrophy);
+/* relative_vorticity(m, y)   TRiSKShallowWater.jl:422-426 (nv values, file numbering). */
+int trisk_relative_vorticity(TriskModel* model, const double* y, double* zeta);
+/* The model's CUDA stream (cudaStream_t), for event timing by the caller. */
+int trisk_model_stream(TriskModel* model, void** stream);
+/* Kernel launches issued by this model so far (graph replays count their kernels). */
+int64_t trisk_launch_count(TriskModel* model);
+/* Algorithmic bytes per launch of the three phase kernels (vertex, flux, tend) and per
+ * RK4 step (4 (T + 2N) + 15N with the model's tables T and state size N). */
+int trisk_model_bytes(TriskModel* model, double out[4]);
+/* Runs nsteps RK4 steps on the device-resident state with a CUDA event pair around every
+ * kernel launch and returns the mean duration in ms of each phase kernel in ms[3]. */
+int trisk_profile_phases(TriskModel* model, double* y_device, double dt, int64_t nsteps, double ms[3]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,198 @@
+"""Parity of the sm_100a path with the CPU oracle, through the C ABI (libtrisk_b200.so).
+
+Bar: the plain FP64 path matches the oracle to 1e-12 relative L2 per tendency and per RK4
+step (the tolerance of the task's target), and, because every per-entity sum keeps the
+reference's order and the library is built without FMA contraction, it is in fact
+bit-identical; both are asserted. Diagnostics match to 1e-12 relative (their reductions
+sum in a different order).
+"""
+import numpy as np
+import pytest
+
+import dmplex_b200 as d
+from dmplex_b200 import workloads as w
+from conftest import oracle_for, tables, tc2_state, trisk_grid
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-12
+SCHEMES = [("trisk", "cell"), ("trisk", "vertex"), ("trisk", "mixed"), ("gassmann", "cell"),
+           ("gassmann", "vertex"), ("gassmann_mean", "mixed"), ("gassmann_mean", "vertex")]
+
+
+def rel_l2(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def perturbed_tc2(g, seed=7):
+    y = tc2_state(g)
+    rng = np.random.default_rng(seed)
+    y[:g.ne] += 0.02 * rng.standard_normal(g.ne)
+    y[g.ne:] += 0.01 * rng.standard_normal(g.nc)
+    return y
+
+
+@pytest.mark.parametrize("pv,ke", SCHEMES)
+@pytest.mark.parametrize("reorder", [True, False])
+def test_tendency_parity(require_gpu, pv, ke, reorder):
+    n = 4
+    g = trisk_grid(n, True)
+    m = d.TRiSKShallowWater(g, pv_flux=pv, kinetic_energy=ke, reorder=reorder)
+    o = oracle_for(n, pv, ke, True)
+    y = perturbed_tc2(g)
+    dy = np.zeros_like(y)
+    d.tendency(dy, y, m)
+    ref = o.tendency(y)
+    assert rel_l2(dy, ref) <= RTOL
+    assert np.array_equal(dy, ref)
+
+
+@pytest.mark.parametrize("pv,ke", [("trisk", "cell"), ("gassmann", "vertex"), ("gassmann_mean", "mixed")])
+def test_rk4_parity_per_step(require_gpu, pv, ke):
+    n = 5
+    g = trisk_grid(n, True)
+    t = tables(n, pv, ke, True, None, w.si_parameters()["gravity"])
+    from oracle.oracle import Oracle
+    o = Oracle(t, threads=8)
+    m = d.TRiSKShallowWater(g, pv_flux=pv, kinetic_energy=ke, **w.si_parameters())
+    y = w.synthetic_state(g, seed=3)
+    ref = y.copy()
+    cache = d.RK4Cache(y)
+    for _ in range(20):
+        d.rk4_step(y, 300.0, d.tendency, cache, m)
+        o.rk4_step(ref, 300.0, 1)
+        assert rel_l2(y, ref) <= RTOL
+    assert np.array_equal(y, ref)
+
+
+def test_multi_step_call_matches_single_steps(require_gpu):
+    g = trisk_grid(4, True)
+    m = d.TRiSKShallowWater(g, pv_flux="gassmann", kinetic_energy="vertex")
+    y = perturbed_tc2(g)
+    a, b = y.copy(), y.copy()
+    d.rk4_step(a, 0.01, d.tendency, d.RK4Cache(a), m, nsteps=10)
+    for _ in range(10):
+        d.rk4_step(b, 0.01, d.tendency, d.RK4Cache(b), m)
+    assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("use_graph,use_pdl,block", [(False, False, 256), (True, False, 128), (False, True, 64)])
+def test_launch_modes_bitwise(require_gpu, use_graph, use_pdl, block):
+    g = trisk_grid(4, True)
+    y = perturbed_tc2(g)
+    ref = y.copy()
+    d.rk4_step(ref, 0.01, d.tendency, d.RK4Cache(ref), d.TRiSKShallowWater(g, pv_flux="trisk"), nsteps=5)
+    m = d.TRiSKShallowWater(g, pv_flux="trisk", use_graph=use_graph, use_pdl=use_pdl, block=block)
+    d.rk4_step(y, 0.01, d.tendency, d.RK4Cache(y), m, nsteps=5)
+    assert np.array_equal(y, ref)
+
+
+@pytest.mark.parametrize("pv,ke", [("trisk", "cell"), ("gassmann", "mixed")])
+def test_diagnostics(require_gpu, pv, ke):
+    g = trisk_grid(4, True)
+    m = d.TRiSKShallowWater(g, pv_flux=pv, kinetic_energy=ke)
+    o = oracle_for(4, pv, ke, True)
+    y = perturbed_tc2(g)
+    assert abs(d.total_mass(m, y) - o.total_mass(y)) <= RTOL * abs(o.total_mass(y))
+    assert abs(d.total_energy(m, y) - o.total_energy(y)) <= RTOL * abs(o.total_energy(y))
+    assert abs(d.potential_enstrophy(m, y) - o.potential_enstrophy(y)) <= RTOL * abs(o.potential_enstrophy(y))
+    assert np.array_equal(d.relative_vorticity(m, y), o.relative_vorticity(y))
+
+
+def test_williamson_tc2_gpu(require_gpu):
+    """The reference's TC2 assertions (test/finite_volumes.jl:97-109) through the GPU path."""
+    for pv in ("trisk", "gassmann", "gassmann_mean"):
+        errors = []
+        for n in (3, 4):
+            g = trisk_grid(n)
+            m = d.TRiSKShallowWater(g, pv_flux=pv)
+            y = tc2_state(g)
+            y0 = y.copy()
+            mass0, energy0 = d.total_mass(m, y), d.total_energy(m, y)
+            dt = 0.2 * np.sqrt(4 * np.pi / g.nc)
+            d.rk4_step(y, dt, d.tendency, d.RK4Cache(y), m, nsteps=int(np.ceil(1 / dt)))
+            assert abs(d.total_mass(m, y) - mass0) < 1e-13
+            assert abs(d.total_energy(m, y) - energy0) / energy0 < 1e-8
+            dh = (y - y0)[g.ne:]
+            errors.append(np.sqrt((g.cell_areas * dh ** 2).sum() / (4 * np.pi)))
+        assert errors[0] < 2e-3 and errors[1] < errors[0] / 2.5
+
+
+def test_device_pointers(require_gpu):
+    import torch
+    g = trisk_grid(4, True)
+    m = d.TRiSKShallowWater(g, pv_flux="gassmann", kinetic_energy="mixed")
+    y = perturbed_tc2(g)
+    dy_host = np.zeros_like(y)
+    d.tendency(dy_host, y, m)
+    yd = torch.from_numpy(y).cuda()
+    dyd = torch.zeros_like(yd)
+    d.tendency(dyd, yd, m)
+    assert np.array_equal(dyd.cpu().numpy(), dy_host)
+    a = y.copy()
+    d.rk4_step(a, 0.01, d.tendency, d.RK4Cache(a), m, nsteps=3)
+    d.rk4_step(yd, 0.01, d.tendency, d.RK4Cache(yd), m, nsteps=3)
+    assert np.array_equal(yd.cpu().numpy(), a)
+    m.rk4_async(yd, 0.01, 2)
+    m.synchronize()
+    d.rk4_step(a, 0.01, d.tendency, d.RK4Cache(a), m, nsteps=2)
+    assert np.array_equal(yd.cpu().numpy(), a)
+
+
+def test_nonfinite_state_is_reported(require_gpu):
+    g = trisk_grid(3)
+    m = d.TRiSKShallowWater(g)
+    y = tc2_state(g)
+    y[5] = np.nan
+    with pytest.raises(d.TriskError) as e:
+        d.rk4_step(y, 0.01, d.tendency, d.RK4Cache(y), m)
+    assert e.value.status == 4
+    y = tc2_state(g)  # the model stays usable
+    d.rk4_step(y, 0.01, d.tendency, d.RK4Cache(y), m)
+    assert np.isfinite(y).all()
+
+
+def test_launch_count(require_gpu):
+    g = trisk_grid(3)
+    m = d.TRiSKShallowWater(g)
+    y = tc2_state(g)
+    d.rk4_step(y, 0.01, d.tendency, d.RK4Cache(y), m)  # graph capture on the first call
+    before = m.launch_count()
+    d.rk4_step(y, 0.01, d.tendency, d.RK4Cache(y), m, nsteps=4)
+    assert m.launch_count() - before == 4 * 12 + 2  # 3 phases x 4 stages per step + 2 permutations
+
+
+def test_from_coefficients_matches(require_gpu):
+    """A model made from the reference model's own premultiplied arrays gives the same
+    results as one built from the grid."""
+    g = trisk_grid(4, True)
+    t = tables(4, "gassmann", "vertex", True)
+    a = d.TRiSKShallowWater(g, pv_flux="gassmann", kinetic_energy="vertex")
+    b = d.TRiSKShallowWater.from_coefficients(t, grid=g, pv_flux="gassmann", kinetic_energy="vertex")
+    y = perturbed_tc2(g)
+    ya, yb = np.zeros_like(y), np.zeros_like(y)
+    d.tendency(ya, y, a)
+    d.tendency(yb, y, b)
+    assert np.array_equal(ya, yb)
+
+
+@pytest.mark.slow
+def test_config_level7_gassmann_vertex(require_gpu):
+    """The drop-in configuration at full size (hexagon 7, Gassmann PV flux, vertex kinetic
+    energy, dt = 75 s): bit parity with the oracle for 3 steps, then mass conservation to
+    round-off over 200 steps."""
+    from oracle.oracle import Oracle
+    g = d.TRiSKGrid(d.create_hexagon_mesh(7, centroidal=True))
+    si = w.si_parameters()
+    m = d.TRiSKShallowWater(g, pv_flux="gassmann", kinetic_energy="vertex", **si)
+    o = Oracle(d.model_tables(g, pv_flux="gassmann", kinetic_energy="vertex", **si), threads=8)
+    y = w.synthetic_state(g, seed=11)
+    ref = y.copy()
+    for _ in range(3):
+        d.rk4_step(y, 75.0, d.tendency, d.RK4Cache(y), m)
+        o.rk4_step(ref, 75.0, 1)
+        assert rel_l2(y, ref) <= RTOL
+    assert np.array_equal(y, ref)
+    mass0 = d.total_mass(m, y)
+    d.rk4_step(y, 75.0, d.tendency, d.RK4Cache(y), m, nsteps=200)
+    assert abs(d.total_mass(m, y) - mass0) / mass0 < 1e-14

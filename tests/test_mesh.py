@@ -1,0 +1,193 @@
+"""Mesh generator and TRiSK grid builder (host set-up rows of the path), checked with the
+properties the reference's own test suite asserts:
+
+    test/finite_volumes.jl:25-77   "TRiSK grid and operators"
+    test/finite_volumes.jl:184-198 vertex-edge areas
+    test/grids.jl:105-131          "Centroidal Voronoi tessellation (Lloyd)"
+    test/topology.jl:42-61         "Hilbert order"
+    src/Topology/Plex.jl:329-359   check_plex
+"""
+import numpy as np
+import pytest
+
+import dmplex_b200 as d
+from conftest import hexagon_mesh, oracle_for, tables, trisk_grid
+
+
+@pytest.mark.parametrize("n", range(0, 6))
+def test_sizes(n):
+    m = hexagon_mesh(n)
+    assert (m.nc, m.ne, m.nv) == (10 * 4 ** n + 2, 30 * 4 ** n, 20 * 4 ** n)
+
+
+@pytest.mark.parametrize("n,centroidal", [(2, False), (3, True)])
+def test_check_plex(n, centroidal):
+    """check_plex (Plex.jl:329-359): cone/support symmetry, closed counter-clockwise cells,
+    one cell on each side of every edge, Euler characteristic 2."""
+    p = hexagon_mesh(n, centroidal).plex
+    nc, ne, nv = p.nc, p.ne, p.nv
+    for q in range(1, nc + ne + nv + 1):
+        for r in p.cone(q):
+            assert q in p.support(r)
+    orient = p.cone_orientations
+    for c in range(1, nc + 1):
+        cone = p.cone(c)
+        o = orient[p.cone_offsets[c - 1] - 1:p.cone_offsets[c] - 1]
+        start = [p.cone(e)[0 if oo == 0 else 1] for e, oo in zip(cone, o)]
+        stop = [p.cone(e)[1 if oo == 0 else 0] for e, oo in zip(cone, o)]
+        assert stop == start[1:] + start[:1]
+        x = p.coordinates[np.array(start) - nc - ne - 1]
+        normal = np.cross(x, np.roll(x, -1, axis=0)).sum(axis=0)
+        assert normal @ x.sum(axis=0) > 0
+    for e in range(nc + 1, nc + ne + 1):
+        sides = []
+        for c in p.support(e):
+            k = list(p.cone(c)).index(e)
+            sides.append(orient[p.cone_offsets[c - 1] - 1 + k])
+        assert sorted(sides) == [-1, 0]
+    assert nv - ne + nc == 2
+
+
+@pytest.mark.parametrize("n", [3])
+def test_grid_and_operators(n):
+    """test/finite_volumes.jl:25-64 on create_hexagon_mesh(3)."""
+    g = trisk_grid(n)
+    o = oracle_for(n)
+    nc, ne, nv = g.nc, g.ne, g.nv
+    assert np.isclose(g.cell_areas.sum(), 4 * np.pi, rtol=1.5e-8) and np.isclose(g.vertex_areas.sum(), 4 * np.pi)
+    assert np.allclose(g.cell_kites.sum(axis=1), g.cell_areas, rtol=1.5e-8)
+    left, right = g.edge_cells[:, 0] - 1, g.edge_cells[:, 1] - 1
+    assert np.all(np.einsum("ij,ij->i", g.edge_normals, g.centers[right] - g.centers[left]) > 0)
+    # antisymmetric TRiSK weights (:35-39)
+    W = np.zeros((ne, ne))
+    np.add.at(W, (np.repeat(np.arange(ne), g.trisk_edges.shape[1]), g.trisk_edges.ravel() - 1),
+              g.trisk_weights.ravel())
+    assert np.abs(W + W.T).max() < 1e-14
+    # dual divergence of the perpendicular fluxes = kite average of the divergence (:41-52)
+    rng = np.random.default_rng(5)
+    u = rng.standard_normal(ne)
+    ce = g.cell_edges - 1
+
+    def D(F):
+        return (g.cell_signs * g.primal_lengths[ce] * F[ce]).sum(axis=1) / g.cell_areas
+
+    perp = o.tangential_velocity(u) * g.dual_lengths
+    dual_div = (g.vertex_signs * perp[g.vertex_edges - 1]).sum(axis=1) / g.vertex_areas
+    Du = D(u)
+    average = (g.vertex_kites * Du[g.vertex_cells - 1]).sum(axis=1) / g.vertex_areas
+    assert np.abs(dual_div + average).max() < 1e-12 * np.abs(average).max()
+    # curl of a gradient and divergence of a skew gradient vanish (:53-58)
+    phi, psi = rng.standard_normal(nc), rng.standard_normal(nv)
+    gradient = (phi[right] - phi[left]) / g.dual_lengths
+    assert np.abs(o.relative_vorticity(np.concatenate([gradient, np.zeros(nc)]))).max() < 1e-12
+    skew = (psi[g.edge_vertices[:, 1] - 1] - psi[g.edge_vertices[:, 0] - 1]) / g.primal_lengths
+    assert np.abs(D(skew)).max() < 1e-11
+    # solid-body rotation: vorticity and TRiSK tangential reconstruction (:59-64)
+    w = np.array([0.3, -0.2, 1.0])
+    solid = np.einsum("ij,ij->i", np.cross(w, g.edge_points), g.edge_normals)
+    zeta = o.relative_vorticity(np.concatenate([solid, np.zeros(nc)]))
+    assert np.abs(zeta - 2 * g.vertices @ w).max() < 0.03
+    tangential = np.einsum("ij,ij->i", np.cross(w, g.edge_points), np.cross(g.edge_points, g.edge_normals))
+    assert np.abs(o.tangential_velocity(solid) - tangential).max() < 0.15
+
+
+def test_gassmann_coefficients():
+    """Gassmann reconstruction: antisymmetric with the same PV and consistent
+    (test/finite_volumes.jl:66-76)."""
+    g = trisk_grid(3)
+    E, P, Wg = g.gassmann_coefficients()
+    l, dd = g.primal_lengths, g.dual_lengths
+    for e in range(g.ne):
+        for k in range(12):
+            f = E[e, k] - 1
+            js = np.nonzero((E[f] == e + 1) & (P[f] == P[e, k]))[0]
+            assert len(js) > 0
+            j = js[0]
+            assert abs(l[e] * dd[e] * Wg[e, k] + l[f] * dd[f] * Wg[f, j]) < 1e-15
+    w = np.array([0.3, -0.2, 1.0])
+    solid = np.einsum("ij,ij->i", np.cross(w, g.edge_points), g.edge_normals)
+    tangential = np.einsum("ij,ij->i", np.cross(w, g.edge_points), np.cross(g.edge_points, g.edge_normals))
+    gassmann = (Wg * solid[E - 1]).sum(axis=1)
+    assert np.abs(gassmann - tangential).max() < 0.02
+
+
+def test_vertex_edge_areas():
+    """test/finite_volumes.jl:184-198 on the spring-dynamics hexagon mesh of level 4."""
+    g = trisk_grid(4, False, 1.2)
+    bv, be = g.vertex_edge_areas()
+    assert np.allclose(bv.sum(axis=1), g.vertex_areas, rtol=1.5e-8)
+    assert np.allclose(be[:, 0] + be[:, 1], g.primal_lengths * g.dual_lengths / 2, rtol=1e-3)
+    n = g.edge_normals[g.vertex_edges - 1]  # (nv, 3, 3)
+    T = np.einsum("vk,vki,vkj->vij", bv, n, n) / g.vertex_areas[:, None, None]
+    x = g.vertices
+    P = np.eye(3)[None] - np.einsum("vi,vj->vij", x, x)
+    assert np.abs(P @ T @ P - P / 2).max() < 2e-3
+
+
+def test_scvt():
+    """test/grids.jl:105-131: Lloyd's SCVT keeps the icosahedron vertices, is a fixed
+    point, agrees with plain Lloyd, and makes the TRiSK reconstruction consistent."""
+    x4, tri = d.icosahedral_mesh(4, centroidal=True)
+    x0, _ = d.icosahedral_mesh(0)
+    assert np.array_equal(x4[:12], x0)
+    assert np.abs(np.linalg.norm(x4, axis=1) - 1).max() < 1e-14
+    x = x4.copy()
+    assert d.lloyd(x, tri, fixed=12) < 3 and np.linalg.norm(x - x4, axis=1).max() < 1e-9
+    y, _ = d.icosahedral_mesh(4)
+    z = y.copy()
+    d.lloyd(y, tri, fixed=12)
+    d.lloyd(z, tri, fixed=12, history=0)
+    assert np.linalg.norm(y - z, axis=1).max() < 1e-7
+
+    def tangential_error(**opts):
+        m = hexagon_mesh(4, **opts)
+        assert m.orthogonality_defect() < 1e-10
+        g = trisk_grid(4, **opts)
+        w = np.array([0.3, -0.2, 1.0])
+        u = np.einsum("ij,ij->i", np.cross(w, g.edge_points), g.edge_normals)
+        te = g.trisk_edges - 1
+        vt = (g.trisk_weights * g.primal_lengths[te] * u[te]).sum(axis=1) / g.dual_lengths
+        exact = np.einsum("ij,ij->i", np.cross(w, g.edge_points), np.cross(g.edge_points, g.edge_normals))
+        return np.abs(vt - exact).max()
+
+    assert tangential_error(centroidal=True) < 0.1 * tangential_error(centroidal=False)
+
+
+def test_hilbert_permutation():
+    """hilbert_permutation (Ordering.jl:85-92): a permutation of the cells that brings
+    neighbouring cells close in memory (test/topology.jl:42-61)."""
+    m = hexagon_mesh(4)
+    g = trisk_grid(4)
+    perm = m.hilbert_permutation()
+    assert sorted(perm.tolist()) == list(range(1, m.nc + 1))
+    rank = np.empty(m.nc, dtype=np.int64)
+    rank[perm - 1] = np.arange(m.nc)
+    ec = g.edge_cells - 1
+    spread_file = np.abs(ec[:, 0] - ec[:, 1]).mean()
+    spread_hilbert = np.abs(rank[ec[:, 0]] - rank[ec[:, 1]]).mean()
+    assert spread_hilbert < 0.25 * spread_file
+
+
+def test_tables_match_grid():
+    """The premultiplied coefficients (TRiSKShallowWater.jl:103-158) against the grid."""
+    g = trisk_grid(3)
+    t = tables(3, "gassmann", "mixed")
+    alpha = 3 / 8
+    i = np.arange(g.nc)[:, None]
+    side = np.where(g.edge_cells[g.cell_edges - 1, 0] - 1 == i, 0, 1)
+    valid = g.cell_signs != 0
+    div = np.where(valid, g.cell_signs * g.primal_lengths[g.cell_edges - 1] / g.cell_areas[:, None], 0)
+    assert np.array_equal(t["divergence"], div)
+    kin = np.where(valid, alpha * g.primal_lengths[g.cell_edges - 1] *
+                   np.take_along_axis(g.cell_distances[g.cell_edges - 1], side[:, :, None], 2)[:, :, 0] /
+                   (2 * g.cell_areas[:, None]), 0)
+    assert np.array_equal(t["kinetic"], kin)
+    assert np.array_equal(t["trisk"], g.trisk_weights * g.primal_lengths[g.trisk_edges - 1] / g.dual_lengths[:, None])
+    assert np.array_equal(t["inverse_dual"], 1 / g.dual_lengths)
+    assert np.array_equal(t["coriolis"], 2 * g.vertices[:, 2])
+    E, P, W = g.gassmann_coefficients()
+    assert np.array_equal(t["g_edges"], E) and np.array_equal(t["g_pv_edges"], P) and np.array_equal(t["g_weights"], W)
+    with pytest.raises(ValueError):
+        d.model_tables(g, kinetic_energy="edge")
+    with pytest.raises(ValueError):
+        d.model_tables(g, pv_flux="upwind")
