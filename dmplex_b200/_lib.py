@@ -116,6 +116,7 @@ def _load():
         "trisk_launch_count": (_i64, [_p]),
         "trisk_model_bytes": (C.c_int, [_p, _p]),
         "trisk_profile_phases": (C.c_int, [_p, _p, _f64, _i64, _p]),
+        "trisk_weighted_sum_noalloc": (C.c_int, [_p, _p, _i64, _p, _p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

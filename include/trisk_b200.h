@@ -203,6 +203,22 @@ int trisk_model_bytes(TriskModel* model, double out[4]);
  * kernel launch and returns the mean duration in ms of each phase kernel in ms[3]. */
 int trisk_profile_phases(TriskModel* model, double* y_device, double dt, int64_t nsteps, double ms[3]);
 
+/* ---- allocation-free entry point ---------------------------------------------------
+ * No counterpart in the reference: it exists for callers that must not have the library
+ * allocate device memory (a host whose device memory all comes from its own pool, such as
+ * CUDA.jl's, or code running while a stream is being captured into a CUDA graph).
+ *
+ * *out = sum_i a[i] * b[i] over caller-owned device vectors (with a = the cell areas and
+ * b = the heights this is total_mass, TRiSKShallowWater.jl:397). a, b and out must be
+ * device pointers on one device; the work is enqueued on `stream` (a cudaStream_t, NULL for
+ * the default stream) and not waited for. The call makes no cudaMalloc, cudaFree or other
+ * allocating call: its scratch is a static 64 KiB device array that every GPU loading the
+ * library holds until exit, which limits n to 16777216 (larger n is rejected with
+ * TRISK_ERR_ARGUMENT). The first call on a device looks that array's address up
+ * (cudaGetSymbolAddress), so make it before any stream capture. All calls share the array:
+ * calls whose work overlaps on the GPU race and give wrong sums; serialize them. */
+int trisk_weighted_sum_noalloc(const double* a, const double* b, int64_t n, double* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
