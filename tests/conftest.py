@@ -28,10 +28,11 @@ def trisk_grid(n: int, centroidal: bool = False, spring_beta=None):
 
 
 @functools.lru_cache(maxsize=None)
-def tables(n: int, pv_flux="trisk", kinetic_energy="cell", centroidal=False, spring_beta=None, gravity=1.0):
+def tables(n: int, pv_flux="trisk", kinetic_energy="cell", centroidal=False, spring_beta=None, gravity=1.0,
+           omega=1.0):
     import dmplex_b200 as d
     return d.model_tables(trisk_grid(n, centroidal, spring_beta), pv_flux=pv_flux, kinetic_energy=kinetic_energy,
-                          gravity=gravity)
+                          gravity=gravity, omega=omega)
 
 
 def oracle_for(n, pv_flux="trisk", kinetic_energy="cell", centroidal=False, spring_beta=None, gravity=1.0,

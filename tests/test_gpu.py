@@ -51,7 +51,7 @@ def test_tendency_parity(require_gpu, pv, ke, reorder):
 def test_rk4_parity_per_step(require_gpu, pv, ke):
     n = 5
     g = trisk_grid(n, True)
-    t = tables(n, pv, ke, True, None, w.si_parameters()["gravity"])
+    t = tables(n, pv, ke, True, None, **w.si_parameters())
     from oracle.oracle import Oracle
     o = Oracle(t, threads=8)
     m = d.TRiSKShallowWater(g, pv_flux=pv, kinetic_energy=ke, **w.si_parameters())
