@@ -201,7 +201,8 @@ def run_b200(args, rank, world, local_rank):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    # warm-up (also captures the CUDA graph)
+    # block shapes from the autotuner, then warm-up (also captures the CUDA graph)
+    tuned_ms = m.autotune(yd, DT, 20)
     m.rk4_async(yd, DT, max(args.warmup, 3))
     m.synchronize()
     barrier()
@@ -245,9 +246,12 @@ def run_b200(args, rank, world, local_rank):
     peak, peak_kind = measured_peak()
     achieved = nbytes_phase["tend"] / (phases["tend"] * 1e-3) / 1e9
     step_gbs = nbytes_phase["rk4_step"] / (ms / args.steps * 1e-3) / 1e9
+    info = m.info()
     roofline = {"bound": "hbm", "kernel": "k_tend<gassmann,stage>", "achieved": achieved, "peak": peak,
                 "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
                 "traffic": ncu_traffic("k_tend"), "algorithmic_bytes_per_launch": nbytes_phase["tend"],
+                "implementation_bytes_per_launch": nbytes_phase["tend"] - info["derived_pv_bytes_saved"],
+                "pv_mode": info["pv_mode"], "block": info["block"], "autotune_ms_per_step": tuned_ms,
                 "launch_ms": phases["tend"], "phase_ms": phases,
                 "phase_bytes": {k: nbytes_phase[k] for k in ("vertex", "flux", "tend")},
                 "step_bytes": nbytes_phase["rk4_step"], "step_gbs": step_gbs, "step_frac": step_gbs / peak}

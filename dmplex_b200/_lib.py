@@ -117,6 +117,8 @@ def _load():
         "trisk_model_bytes": (C.c_int, [_p, _p]),
         "trisk_profile_phases": (C.c_int, [_p, _p, _f64, _i64, _p]),
         "trisk_weighted_sum_noalloc": (C.c_int, [_p, _p, _i64, _p, _p]),
+        "trisk_model_info": (C.c_int, [_p, C.POINTER(_i32), _p, C.POINTER(_f64)]),
+        "trisk_autotune": (C.c_int, [_p, _p, _f64, _i32, C.POINTER(_f64)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

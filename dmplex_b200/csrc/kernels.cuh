@@ -39,7 +39,14 @@ constexpr int VW = 3;   // vertex table width (Voronoi vertices have three edges
 constexpr int TWD = 10; // TRiSK table width (5 + 5 edges of the two hexagons)
 constexpr int GW = 12;  // Gassmann stencil width
 
-enum PvMode { PVM_TRISK = 0, PVM_GASSMANN = 1, PVM_GASSMANN_MEAN = 2 };
+// PVM_GASSMANN_DERIVED: Gassmann's PV edges are not read from a table but derived from the
+// flux edges. gassmann_coefficients (TRiSKGrid.jl:227-246) fills each vertex block of six
+// entries as [f1, o, o, f2, o', o'] with PV edges [f2, f1, f1, f1, f2, f2]: entry k takes
+// the PV of flux edge 3 or 0 of its block. The upload verifies this for every edge.
+enum PvMode { PVM_TRISK = 0, PVM_GASSMANN = 1, PVM_GASSMANN_MEAN = 2, PVM_GASSMANN_DERIVED = 3 };
+__host__ __device__ constexpr int derived_pv_source(int k) {
+  return (k / 6) * 6 + ((k % 6 == 0 || k % 6 == 4 || k % 6 == 5) ? 3 : 0);
+}
 enum KeMode { KE_CELL = 0, KE_VERTEX = 1, KE_MIXED = 2 };
 enum Epilogue { EPI_TENDENCY = 0, EPI_STAGE1 = 1, EPI_STAGE2 = 2, EPI_STAGE3 = 3, EPI_STAGE4 = 4 };
 
@@ -316,12 +323,21 @@ __global__ void __launch_bounds__(256) k_tend(DevTables T, DevWork W, DevStage S
       pdl_wait();
       double f[GW], q[GW];
       const double qself = PV == PVM_GASSMANN_MEAN ? W.qe[o] : 0.0;
+      if (PV == PVM_GASSMANN_DERIVED) {  // four distinct PV gathers per edge
+        const double q0 = W.qe[(size_t)ge[0] * M + mm], q3 = W.qe[(size_t)ge[3] * M + mm];
+        const double q6 = W.qe[(size_t)ge[6] * M + mm], q9 = W.qe[(size_t)ge[9] * M + mm];
+#pragma unroll
+        for (int k = 0; k < GW; ++k) {
+          const int src = derived_pv_source(k);
+          q[k] = src == 0 ? q0 : (src == 3 ? q3 : (src == 6 ? q6 : q9));
+        }
+      }
 #pragma unroll
       for (int k = 0; k < GW; ++k) {
         f[k] = W.F[(size_t)ge[k] * M + mm];
         if (PV == PVM_GASSMANN)
           q[k] = W.qe[(size_t)gp[k] * M + mm];
-        else
+        else if (PV == PVM_GASSMANN_MEAN)
           q[k] = (qself + W.qe[(size_t)ge[k] * M + mm]) / 2;
       }
       double s = 0.0;

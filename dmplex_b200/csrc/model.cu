@@ -129,10 +129,10 @@ struct TriskTables {
 struct TriskModel {
   int device = 0;
   cudaStream_t stream = nullptr;
-  int pv = 0, ke = 0;
+  int pv = 0, ke = 0;  // pv: the kernels' PvMode (PVM_GASSMANN_DERIVED when the table allows it)
   double alpha = 1.0, gravity = 1.0;
   int64_t nc = 0, ne = 0, nv = 0, N = 0;
-  int block = 256;
+  int block[3] = {128, 128, 128};  // threads per block of k_vertex, k_flux, k_tend
   bool use_graph = true, use_pdl = true, identity = true;
   Coefficients C;  // file numbering, 0-based (kept for export)
   CoefficientExport exported;
@@ -149,6 +149,7 @@ struct TriskModel {
   int64_t launches = 0;
   double table_bytes_unique = 0;
   double phase_bytes[3] = {0, 0, 0};
+  double pv_table_bytes_saved = 0;  // k_tend bytes per launch the derived PV edges do not read
 
   ~TriskModel() {
     int prev = -1;
@@ -178,13 +179,13 @@ namespace {
 // launch helpers
 
 template <typename... KArgs, typename... Args>
-void launch(TriskModel& m, void (*kernel)(KArgs...), int64_t grid, cudaEvent_t ev0, cudaEvent_t ev1,
+void launch(TriskModel& m, void (*kernel)(KArgs...), int64_t grid, int block, cudaEvent_t ev0, cudaEvent_t ev1,
             Args&&... args) {
   if (grid <= 0) return;
   if (ev0) CUDA_CHECK(cudaEventRecord(ev0, m.stream));
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)grid);
-  cfg.blockDim = dim3((unsigned)m.block);
+  cfg.blockDim = dim3((unsigned)block);
   cfg.dynamicSmemBytes = 0;
   cfg.stream = m.stream;
   cudaLaunchAttribute attr[1];
@@ -210,26 +211,34 @@ void with_modes(int pv, int ke, F&& f) {
     case 6: f(integral_constant<int, 2>{}, integral_constant<int, 0>{}); break;
     case 7: f(integral_constant<int, 2>{}, integral_constant<int, 1>{}); break;
     case 8: f(integral_constant<int, 2>{}, integral_constant<int, 2>{}); break;
+    case 9: f(integral_constant<int, 3>{}, integral_constant<int, 0>{}); break;
+    case 10: f(integral_constant<int, 3>{}, integral_constant<int, 1>{}); break;
+    case 11: f(integral_constant<int, 3>{}, integral_constant<int, 2>{}); break;
     default: throw Error(TRISK_ERR_ARGUMENT, "bad scheme");
   }
 }
 
 // One tendency: three phase launches. ev: optional 6 events (pairs around each launch).
 void enqueue_tendency(TriskModel& m, const DevStage& S, int epi, cudaEvent_t* ev = nullptr) {
-  const int64_t B = m.block;
-  const int64_t nbV = cdiv(m.nv, B), nbE = cdiv(m.ne, B), nbC = cdiv(m.nc, B);
+  const int bV = m.block[0], bF = m.block[1], bT = m.block[2];
+  const int64_t nbV = cdiv(m.nv, bV);
+  const int64_t nbEF = cdiv(m.ne, bF), nbCF = cdiv(m.nc, bF);
+  const int64_t nbET = cdiv(m.ne, bT), nbCT = cdiv(m.nc, bT);
   with_modes(m.pv, m.ke, [&](auto pvc, auto kec) {
     constexpr int PV = decltype(pvc)::value, KE = decltype(kec)::value;
-    launch(m, k_vertex<PV, KE, false>, nbV, ev ? ev[0] : nullptr, ev ? ev[1] : nullptr, m.T, m.W, S.u, S.h, 1, 0);
-    launch(m, k_flux<PV, KE, false>, nbE + nbC, ev ? ev[2] : nullptr, ev ? ev[3] : nullptr, m.T, m.W, S.u, S.h, 1,
-           (int)nbE, 0);
+    launch(m, k_vertex<PV, KE, false>, nbV, bV, ev ? ev[0] : nullptr, ev ? ev[1] : nullptr, m.T, m.W, S.u, S.h, 1,
+           0);
+    launch(m, k_flux<PV, KE, false>, nbEF + nbCF, bF, ev ? ev[2] : nullptr, ev ? ev[3] : nullptr, m.T, m.W, S.u,
+           S.h, 1, (int)nbEF, 0);
     cudaEvent_t e0 = ev ? ev[4] : nullptr, e1 = ev ? ev[5] : nullptr;
+    const int64_t g = nbET + nbCT;
+    const int nbE = (int)nbET;
     switch (epi) {
-      case EPI_TENDENCY: launch(m, k_tend<PV, EPI_TENDENCY, false>, nbE + nbC, e0, e1, m.T, m.W, S, 1, (int)nbE); break;
-      case EPI_STAGE1: launch(m, k_tend<PV, EPI_STAGE1, false>, nbE + nbC, e0, e1, m.T, m.W, S, 1, (int)nbE); break;
-      case EPI_STAGE2: launch(m, k_tend<PV, EPI_STAGE2, false>, nbE + nbC, e0, e1, m.T, m.W, S, 1, (int)nbE); break;
-      case EPI_STAGE3: launch(m, k_tend<PV, EPI_STAGE3, false>, nbE + nbC, e0, e1, m.T, m.W, S, 1, (int)nbE); break;
-      default: launch(m, k_tend<PV, EPI_STAGE4, false>, nbE + nbC, e0, e1, m.T, m.W, S, 1, (int)nbE); break;
+      case EPI_TENDENCY: launch(m, k_tend<PV, EPI_TENDENCY, false>, g, bT, e0, e1, m.T, m.W, S, 1, nbE); break;
+      case EPI_STAGE1: launch(m, k_tend<PV, EPI_STAGE1, false>, g, bT, e0, e1, m.T, m.W, S, 1, nbE); break;
+      case EPI_STAGE2: launch(m, k_tend<PV, EPI_STAGE2, false>, g, bT, e0, e1, m.T, m.W, S, 1, nbE); break;
+      case EPI_STAGE3: launch(m, k_tend<PV, EPI_STAGE3, false>, g, bT, e0, e1, m.T, m.W, S, 1, nbE); break;
+      default: launch(m, k_tend<PV, EPI_STAGE4, false>, g, bT, e0, e1, m.T, m.W, S, 1, nbE); break;
     }
   });
 }
@@ -577,11 +586,25 @@ void upload(TriskModel& m, const Coefficients& C) {
   o.ev = pack_index(P, C.edge_vertices, 2, 2, ne, lde, en, m.vert_o2n);
   o.invd = pack_weight(P, C.inverse_dual, 1, 1, ne, lde, en);
   if (vertK) o.vkh = pack_weight(P, C.vk_height, 2, 2, ne, lde, en);
+  // Gassmann PV edges follow from the flux edges whenever every edge has the block
+  // structure gassmann_coefficients produces; then the kernel derives them (exact).
+  bool derived = false;
+  if (C.pv_flux == PV_GASSMANN) {
+    derived = true;
+    for (int64_t e = 0; e < ne && derived; ++e)
+      for (int k = 0; k < 12; ++k)
+        if (C.g_pv_edges[12 * e + k] != C.g_edges[12 * e + derived_pv_source(k)]) {
+          derived = false;
+          break;
+        }
+    if (derived) m.pv = PVM_GASSMANN_DERIVED;
+  }
   if (C.pv_flux != PV_TRISK) {
     o.rh = pack_weight(P, C.rhombus, 2, 2, ne, lde, en);
     o.gc = pack_weight(P, C.g_coriolis, 1, 1, ne, lde, en);
     o.ge = pack_index(P, C.g_edges, 12, GW, ne, lde, en, m.edge_o2n);
-    if (C.pv_flux == PV_GASSMANN) o.gp = pack_index(P, C.g_pv_edges, 12, GW, ne, lde, en, m.edge_o2n);
+    if (C.pv_flux == PV_GASSMANN && !derived)
+      o.gp = pack_index(P, C.g_pv_edges, 12, GW, ne, lde, en, m.edge_o2n);
     o.gw = pack_weight(P, C.g_weights, 12, GW, ne, lde, en);
   } else {
     o.te = pack_index(P, C.trisk_edges, C.tw, TWD, ne, lde, en, m.edge_o2n);
@@ -624,7 +647,7 @@ void upload(TriskModel& m, const Coefficients& C) {
   T.trisk_edges = I(o.te, !g);
   T.trisk = D(o.tr, !g);
   T.g_edges = I(o.ge, g);
-  T.g_pv_edges = I(o.gp, C.pv_flux == PV_GASSMANN);
+  T.g_pv_edges = I(o.gp, C.pv_flux == PV_GASSMANN && !derived);
   T.g_weights = D(o.gw, g);
   T.vertex_edges = I(o.ve, true);
   T.curl = D(o.cu, true);
@@ -635,9 +658,11 @@ void upload(TriskModel& m, const Coefficients& C) {
   m.area_c = const_cast<double*>(D(o.ac, true));
   m.area_v = const_cast<double*>(D(o.av, true));
 
-  // Algorithmic bytes: every table the scheme needs once (int32 index, FP64 weight).
+  // Algorithmic bytes in the canonical form: every table the scheme needs once (int32
+  // index, FP64 weight), the Gassmann PV-edge table included even when it is derived.
   const double I4 = 4, F8 = 8;
   const bool tr = C.pv_flux == PV_TRISK, gm = C.pv_flux == PV_GASSMANN;
+  m.pv_table_bytes_saved = derived ? (double)ne * GW * I4 : 0.0;
   double cellB = CW * (I4 + F8) + (cellK ? CW * F8 : 0) + (vertK ? CW * (I4 + F8) : 0);
   double edgeB = 2 * I4 + 2 * I4 + F8 + (cellK ? 2 * F8 : 0) + (vertK ? 2 * F8 : 0) +
                  (tr ? TWD * (I4 + F8) : GW * (I4 + F8) + (gm ? GW * I4 : 0) + 2 * F8 + F8);
@@ -672,7 +697,7 @@ void finish_create(TriskModel& m, const Coefficients& C, const std::vector<V3>* 
     if (cfg->block) {
       if (cfg->block % 32 != 0 || cfg->block < 64 || cfg->block > 256)
         throw Error(TRISK_ERR_ARGUMENT, "block must be a multiple of 32 in 64..256");
-      m.block = cfg->block;
+      m.block[0] = m.block[1] = m.block[2] = cfg->block;
     }
   }
   if (m.nc >= (1LL << 30) || m.ne >= (1LL << 30)) throw Error(TRISK_ERR_UNSUPPORTED, "mesh too large for int32 tables");
@@ -939,22 +964,22 @@ int trisk_diagnostics(TriskModel* model, const double* y, double* mass, double* 
   const double* u = m.y;
   const double* h = m.y + m.ne;
   if (mass) *mass = reduce<0>(m, m.area_c, h, nullptr, 0.0, m.nc);
-  const int64_t B = m.block;
+  const int B = 128;
   const bool saved = m.use_pdl;
   m.use_pdl = false;
   try {
     if (energy) {  // kinetic_energy! then sum A h (K + g h / 2)   (TRiSKShallowWater.jl:406-411)
       with_modes(m.pv, m.ke, [&](auto pvc, auto kec) {
         constexpr int PV = decltype(pvc)::value, KE = decltype(kec)::value;
-        launch(m, k_vertex<PV, KE, false>, cdiv(m.nv, B), nullptr, nullptr, m.T, m.W, u, h, 1, 0);
-        launch(m, k_flux<PV, KE, false>, cdiv(m.nc, B), nullptr, nullptr, m.T, m.W, u, h, 1, 0, 1);
+        launch(m, k_vertex<PV, KE, false>, cdiv(m.nv, B), B, nullptr, nullptr, m.T, m.W, u, h, 1, 0);
+        launch(m, k_flux<PV, KE, false>, cdiv(m.nc, B), B, nullptr, nullptr, m.T, m.W, u, h, 1, 0, 1);
       });
       *energy = reduce<1>(m, m.area_c, h, m.W.K, m.gravity, m.nc);
     }
     if (enstrophy) {  // vertex_pv! then sum A_v h_v q_v^2 / 2   (:414-419)
       with_modes(m.pv, m.ke, [&](auto pvc, auto kec) {
         constexpr int PV = decltype(pvc)::value, KE = decltype(kec)::value;
-        launch(m, k_vertex<PV, KE, false>, cdiv(m.nv, B), nullptr, nullptr, m.T, m.W, u, h, 1, 1);
+        launch(m, k_vertex<PV, KE, false>, cdiv(m.nv, B), B, nullptr, nullptr, m.T, m.W, u, h, 1, 1);
       });
       *enstrophy = reduce<2>(m, m.area_v, m.W.hv, m.W.qv, 0.0, m.nv) / 2;
     }
@@ -1003,6 +1028,75 @@ int trisk_model_bytes(TriskModel* model, double out[4]) {
   out[2] = m.phase_bytes[2];
   const double N = 8.0 * (double)m.N;
   out[3] = 4 * (m.table_bytes_unique + 2 * N) + 15 * N;
+  TRISK_API_END
+}
+
+int trisk_model_info(TriskModel* model, int32_t* pv_mode, int32_t block[3], double* derived_saving) {
+  TRISK_API_BEGIN
+  TriskModel& m = *checked(model);
+  if (pv_mode) *pv_mode = m.pv;
+  if (block)
+    for (int p = 0; p < 3; ++p) block[p] = m.block[p];
+  if (derived_saving) *derived_saving = m.pv_table_bytes_saved;
+  TRISK_API_END
+}
+
+int trisk_autotune(TriskModel* model, double* y, double dt, int32_t steps, double* best_ms) {
+  TRISK_API_BEGIN
+  TriskModel& m = *checked(model);
+  if (!y || steps <= 0) throw Error(TRISK_ERR_ARGUMENT, "bad argument");
+  DeviceGuard guard(m.device);
+  if (!is_device_pointer(y)) throw Error(TRISK_ERR_ARGUMENT, "trisk_autotune needs a device state");
+  // Times `steps` RK4 steps (graph + PDL as configured) for every combination of the
+  // three phase block sizes and keeps the fastest. Every candidate computes the same
+  // numbers; the state is restored from the caller's copy before each trial.
+  static const int choices[] = {64, 128, 256};
+  cudaEvent_t e0, e1;
+  CUDA_CHECK(cudaEventCreate(&e0));
+  CUDA_CHECK(cudaEventCreate(&e1));
+  int best[3] = {m.block[0], m.block[1], m.block[2]};
+  double best_t = INFINITY;
+  try {
+    for (int a : choices)
+      for (int b : choices)
+        for (int c : choices) {
+          m.block[0] = a;
+          m.block[1] = b;
+          m.block[2] = c;
+          if (m.graph) {
+            cudaGraphExecDestroy(m.graph);
+            m.graph = nullptr;
+          }
+          state_in(m, y, m.y);
+          run_steps(m, dt, 2);  // warm-up (and graph capture)
+          CUDA_CHECK(cudaEventRecord(e0, m.stream));
+          run_steps(m, dt, steps);
+          CUDA_CHECK(cudaEventRecord(e1, m.stream));
+          CUDA_CHECK(cudaEventSynchronize(e1));
+          float ms = 0;
+          CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+          if (ms < best_t) {
+            best_t = ms;
+            best[0] = a;
+            best[1] = b;
+            best[2] = c;
+          }
+        }
+  } catch (...) {
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    throw;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  for (int p = 0; p < 3; ++p) m.block[p] = best[p];
+  if (m.graph) {
+    cudaGraphExecDestroy(m.graph);
+    m.graph = nullptr;
+  }
+  CUDA_CHECK(cudaMemsetAsync(m.flag, 0, sizeof(int), m.stream));
+  CUDA_CHECK(cudaStreamSynchronize(m.stream));
+  if (best_ms) *best_ms = best_t / steps;
   TRISK_API_END
 }
 

@@ -125,6 +125,19 @@ class TRiSKShallowWater:
         check(lib.trisk_profile_phases(self._h, ptr(y_device), float(dt), int(nsteps), ms.ctypes.data))
         return {"vertex": ms[0], "flux": ms[1], "tend": ms[2]}
 
+    def info(self) -> dict:
+        pv = C.c_int32()
+        block = np.zeros(3, dtype=np.int32)
+        saved = C.c_double()
+        check(lib.trisk_model_info(self._h, C.byref(pv), block.ctypes.data, C.byref(saved)))
+        return {"pv_mode": pv.value, "block": block.tolist(), "derived_pv_bytes_saved": saved.value}
+
+    def autotune(self, y_device, dt: float, steps: int = 20) -> float:
+        """Picks the fastest phase block sizes for this mesh and scheme; returns ms/step."""
+        best = C.c_double()
+        check(lib.trisk_autotune(self._h, ptr(y_device), float(dt), int(steps), C.byref(best)))
+        return best.value
+
     def rk4_async(self, y_device, dt: float, nsteps: int = 1) -> None:
         check(lib.trisk_rk4_step_async(self._h, ptr(y_device), float(dt), int(nsteps)))
 

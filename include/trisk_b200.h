@@ -199,6 +199,14 @@ int64_t trisk_launch_count(TriskModel* model);
 /* Algorithmic bytes per launch of the three phase kernels (vertex, flux, tend) and per
  * RK4 step (4 (T + 2N) + 15N with the model's tables T and state size N). */
 int trisk_model_bytes(TriskModel* model, double out[4]);
+/* The kernels' PV mode (3 = Gassmann with PV edges derived from the flux edges, verified
+ * at upload), the threads per block of the three phases, and the bytes per k_tend launch
+ * the derived PV edges save. No reference counterpart (implementation detail). */
+int trisk_model_info(TriskModel* model, int32_t* pv_mode, int32_t block[3], double* derived_saving);
+/* Autotuner (no reference counterpart): times `steps` RK4 steps of the device state y (left
+ * unchanged) for every combination of the phase block sizes {64, 128, 256} and keeps the
+ * fastest in the model; best_ms gets its time per step. */
+int trisk_autotune(TriskModel* model, double* y_device, double dt, int32_t steps, double* best_ms);
 /* Runs nsteps RK4 steps on the device-resident state with a CUDA event pair around every
  * kernel launch and returns the mean duration in ms of each phase kernel in ms[3]. */
 int trisk_profile_phases(TriskModel* model, double* y_device, double dt, int64_t nsteps, double ms[3]);

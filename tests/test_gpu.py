@@ -176,6 +176,42 @@ def test_from_coefficients_matches(require_gpu):
     assert np.array_equal(ya, yb)
 
 
+def test_gassmann_pv_modes(require_gpu):
+    """Gassmann tables in gassmann_coefficients' own order let the kernel derive the PV
+    edges (mode 3); a reordered table (entries 0 and 1 of each block swapped) has no such
+    structure, is uploaded explicitly (mode 1) and still matches the oracle bit for bit."""
+    from oracle.oracle import Oracle
+    g = trisk_grid(4, True)
+    t = dict(tables(4, "gassmann", "vertex", True))
+    y = perturbed_tc2(g)
+    a = d.TRiSKShallowWater.from_coefficients(t, grid=g, pv_flux="gassmann", kinetic_energy="vertex")
+    assert a.info()["pv_mode"] == 3
+    perm = np.arange(12)
+    perm[[0, 1, 6, 7]] = [1, 0, 7, 6]
+    for name in ("g_edges", "g_pv_edges", "g_weights"):
+        t[name] = np.ascontiguousarray(t[name][:, perm])
+    b = d.TRiSKShallowWater.from_coefficients(t, grid=g, pv_flux="gassmann", kinetic_energy="vertex")
+    assert b.info()["pv_mode"] == 1
+    dy = np.zeros_like(y)
+    d.tendency(dy, y, b)
+    assert np.array_equal(dy, Oracle(t).tendency(y))
+
+
+def test_autotune_keeps_results(require_gpu):
+    import torch
+    g = trisk_grid(5, True)
+    m = d.TRiSKShallowWater(g, pv_flux="gassmann", kinetic_energy="vertex")
+    y = perturbed_tc2(g)
+    ref = y.copy()
+    d.rk4_step(ref, 0.002, d.tendency, d.RK4Cache(ref), m, nsteps=4)
+    yd = torch.from_numpy(y).cuda()
+    ms = m.autotune(yd, 0.002, 5)
+    assert ms > 0 and all(b in (64, 128, 256) for b in m.info()["block"])
+    assert np.array_equal(yd.cpu().numpy(), y)  # the autotuner leaves the state alone
+    d.rk4_step(yd, 0.002, d.tendency, d.RK4Cache(yd), m, nsteps=4)
+    assert np.array_equal(yd.cpu().numpy(), ref)
+
+
 @pytest.mark.slow
 def test_config_level7_gassmann_vertex(require_gpu):
     """The drop-in configuration at full size (hexagon 7, Gassmann PV flux, vertex kinetic
