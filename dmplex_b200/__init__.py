@@ -6,12 +6,13 @@ hand-written sm_100a kernels. Names follow the reference (dmplex.jl); Julia's
 mutating ``f!`` functions are ``f`` here.
 """
 from ._lib import TriskError
+from .ensemble import Ensemble
 from .mesh import HexMesh, Plex, TRiSKGrid, create_hexagon_mesh, icosahedral_mesh, lloyd
 from .model import (RK4Cache, TRiSKShallowWater, height_dofs, initial_state, model_tables, potential_enstrophy,
                     relative_vorticity, rk4_step, tendency, total_energy, total_mass, velocity_dofs)
 
 __all__ = [
-    "TriskError", "HexMesh", "Plex", "TRiSKGrid", "create_hexagon_mesh", "icosahedral_mesh", "lloyd", "RK4Cache", "TRiSKShallowWater",
+    "TriskError", "Ensemble", "HexMesh", "Plex", "TRiSKGrid", "create_hexagon_mesh", "icosahedral_mesh", "lloyd", "RK4Cache", "TRiSKShallowWater",
     "height_dofs", "initial_state", "model_tables", "potential_enstrophy", "relative_vorticity", "rk4_step", "tendency",
     "total_energy", "total_mass", "velocity_dofs",
 ]

@@ -118,6 +118,17 @@ def _load():
         "trisk_profile_phases": (C.c_int, [_p, _p, _f64, _i64, _p]),
         "trisk_weighted_sum_noalloc": (C.c_int, [_p, _p, _i64, _p, _p]),
         "trisk_model_info": (C.c_int, [_p, C.POINTER(_i32), _p, C.POINTER(_f64)]),
+        "trisk_ensemble_create": (C.c_int, [_p, _p, _p, _p, _i32, C.POINTER(_p)]),
+        "trisk_ensemble_destroy": (None, [_p]),
+        "trisk_ensemble_set_member": (C.c_int, [_p, _i32, _i32, _p]),
+        "trisk_ensemble_get_member": (C.c_int, [_p, _i32, _i32, _p]),
+        "trisk_ensemble_run_async": (C.c_int, [_p, _i64]),
+        "trisk_ensemble_synchronize": (C.c_int, [_p]),
+        "trisk_ensemble_steps": (C.c_int, [_p, _p]),
+        "trisk_ensemble_reset": (C.c_int, [_p]),
+        "trisk_ensemble_stream": (C.c_int, [_p, C.POINTER(_p)]),
+        "trisk_ensemble_launch_count": (_i64, [_p]),
+        "trisk_ensemble_bytes": (C.c_int, [_p, C.POINTER(_f64)]),
         "trisk_autotune": (C.c_int, [_p, _p, _f64, _i32, C.POINTER(_f64)]),
     }
     for name, (res, args) in sig.items():

@@ -118,12 +118,14 @@ __device__ __forceinline__ void split(int t, int M, int& ent, int& mem) {
 
 // ------------------------------------------------------------------------------------
 // phase 1: vertices
+// Each phase is a __device__ body over one block's worth of entities (block index vb),
+// called by the one-model kernels with vb = blockIdx.x and by the persistent ensemble
+// kernels (ensemble.cu) for every block of work they take.
 template <int PV, int KE, bool ENS>
-__global__ void __launch_bounds__(256) k_vertex(DevTables T, DevWork W, const double* u, const double* h, int M,
-                                                int want_qv) {
-  pdl_trigger();
+__device__ __forceinline__ void vertex_body(const DevTables& T, const DevWork& W, const double* u, const double* h,
+                                            int M, int want_qv, int vb) {
   int v, mm;
-  split<ENS>(blockIdx.x * blockDim.x + threadIdx.x, M, v, mm);
+  split<ENS>(vb * blockDim.x + threadIdx.x, M, v, mm);
   if (v >= T.nv) return;
   int ve[VW], vc[VW];
   double cu[VW], vh[VW], vkw[VW];
@@ -162,15 +164,22 @@ __global__ void __launch_bounds__(256) k_vertex(DevTables T, DevWork W, const do
   }
 }
 
-// ------------------------------------------------------------------------------------
-// phase 2: edges (mass flux, edge PV) and cells (Bernoulli function)
 template <int PV, int KE, bool ENS>
-__global__ void __launch_bounds__(256) k_flux(DevTables T, DevWork W, const double* u, const double* h, int M,
-                                              int nbE, int want_K) {
+__global__ void __launch_bounds__(256) k_vertex(DevTables T, DevWork W, const double* u, const double* h, int M,
+                                                int want_qv) {
   pdl_trigger();
-  if ((int)blockIdx.x < nbE) {
+  vertex_body<PV, KE, ENS>(T, W, u, h, M, want_qv, blockIdx.x);
+}
+
+// ------------------------------------------------------------------------------------
+// phase 2: edges (mass flux, edge PV) and cells (Bernoulli function); blocks [0, nbE)
+// take edges, the rest cells
+template <int PV, int KE, bool ENS>
+__device__ __forceinline__ void flux_body(const DevTables& T, const DevWork& W, const double* u, const double* h,
+                                          int M, int nbE, int want_K, int vb) {
+  if (vb < nbE) {
     int e, mm;
-    split<ENS>(blockIdx.x * blockDim.x + threadIdx.x, M, e, mm);
+    split<ENS>(vb * blockDim.x + threadIdx.x, M, e, mm);
     if (e >= T.ne) return;
     const int ev0 = ldt(T.edge_vertices + e), ev1 = ldt(T.edge_vertices + T.lde + e);
     int ec0 = 0, ec1 = 0;
@@ -217,7 +226,7 @@ __global__ void __launch_bounds__(256) k_flux(DevTables T, DevWork W, const doub
     }
   } else {
     int i, mm;
-    split<ENS>((blockIdx.x - nbE) * blockDim.x + threadIdx.x, M, i, mm);
+    split<ENS>((vb - nbE) * blockDim.x + threadIdx.x, M, i, mm);
     if (i >= T.nc) return;
     int ce[CW], cv[CW];
     double kin[CW], kk[CW];
@@ -261,6 +270,13 @@ __global__ void __launch_bounds__(256) k_flux(DevTables T, DevWork W, const doub
   }
 }
 
+template <int PV, int KE, bool ENS>
+__global__ void __launch_bounds__(256) k_flux(DevTables T, DevWork W, const double* u, const double* h, int M,
+                                              int nbE, int want_K) {
+  pdl_trigger();
+  flux_body<PV, KE, ENS>(T, W, u, h, M, nbE, want_K, blockIdx.x);
+}
+
 // ------------------------------------------------------------------------------------
 // phase 3: tendencies and the RK4 stage update
 template <int EPI>
@@ -281,11 +297,11 @@ __device__ __forceinline__ void epilogue(const DevStage& S, size_t j, double kv)
 }
 
 template <int PV, int EPI, bool ENS>
-__global__ void __launch_bounds__(256) k_tend(DevTables T, DevWork W, DevStage S, int M, int nbE) {
-  pdl_trigger();
-  if ((int)blockIdx.x < nbE) {
+__device__ __forceinline__ void tend_body(const DevTables& T, const DevWork& W, const DevStage& S, int M, int nbE,
+                                          int vb) {
+  if (vb < nbE) {
     int e, mm;
-    split<ENS>(blockIdx.x * blockDim.x + threadIdx.x, M, e, mm);
+    split<ENS>(vb * blockDim.x + threadIdx.x, M, e, mm);
     if (e >= T.ne) return;
     const int ec0 = ldt(T.edge_cells + e), ec1 = ldt(T.edge_cells + T.lde + e);
     const double invd = ldt(T.inverse_dual + e);
@@ -348,7 +364,7 @@ __global__ void __launch_bounds__(256) k_tend(DevTables T, DevWork W, DevStage S
     epilogue<EPI>(S, o, du);
   } else {
     int i, mm;
-    split<ENS>((blockIdx.x - nbE) * blockDim.x + threadIdx.x, M, i, mm);
+    split<ENS>((vb - nbE) * blockDim.x + threadIdx.x, M, i, mm);
     if (i >= T.nc) return;
     int ce[CW];
     double dv[CW];
@@ -367,6 +383,12 @@ __global__ void __launch_bounds__(256) k_tend(DevTables T, DevWork W, DevStage S
     const size_t o = (size_t)i * M + mm;
     epilogue<EPI>(S, (size_t)T.ne * M + o, -s);
   }
+}
+
+template <int PV, int EPI, bool ENS>
+__global__ void __launch_bounds__(256) k_tend(DevTables T, DevWork W, DevStage S, int M, int nbE) {
+  pdl_trigger();
+  tend_body<PV, EPI, ENS>(T, W, S, M, nbE, blockIdx.x);
 }
 
 }  // namespace trisk

@@ -1,26 +1,14 @@
 // TRiSK shallow-water model on one B200: table upload, the internal (Hilbert) numbering,
 // the phase launches, the CUDA-graph RK4 step and the diagnostics, behind the C ABI of
 // include/trisk_b200.h.
-#include <cuda_runtime.h>
-
 #include <algorithm>
-#include <cmath>
 #include <cstring>
 #include <memory>
 #include <type_traits>
-#include <vector>
 
-#include "common.hpp"
-#include "kernels.cuh"
+#include "model.hpp"
 
 using trisk::Error;
-
-#define CUDA_CHECK(x)                                                                                   \
-  do {                                                                                                  \
-    cudaError_t err__ = (x);                                                                            \
-    if (err__ != cudaSuccess)                                                                           \
-      throw trisk::Error(TRISK_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(err__));          \
-  } while (0)
 
 namespace trisk {
 
@@ -81,21 +69,20 @@ __global__ void k_vertex_curl(DevTables T, const double* u, double* zeta) {  // 
   zeta[v] = s;
 }
 
-static inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
-static inline int64_t round_up(int64_t a, int64_t b) { return cdiv(a, b) * b; }
+bool is_device_pointer(const void* p) {
+  cudaPointerAttributes a;
+  cudaError_t e = cudaPointerGetAttributes(&a, p);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
 
-struct DeviceGuard {
-  int prev = -1;
-  explicit DeviceGuard(int dev) {
-    cudaGetDevice(&prev);
-    if (prev != dev) CUDA_CHECK(cudaSetDevice(dev));
-  }
-  ~DeviceGuard() {
-    int cur = -1;
-    cudaGetDevice(&cur);
-    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
-  }
-};
+void launch_gather(cudaStream_t stream, double* dst, const double* src, const int32_t* idx, int64_t n) {
+  k_gather<<<(unsigned)cdiv(n, 256), 256, 0, stream>>>(dst, src, idx, n);
+  CUDA_CHECK(cudaGetLastError());
+}
 
 // Host staging of all tables in one allocation (256-byte aligned pieces).
 struct Packer {
@@ -114,64 +101,6 @@ struct Packer {
 }  // namespace trisk
 
 using namespace trisk;
-
-// 1-based copies of the index tables handed out through TriskCoefficients views.
-struct CoefficientExport {
-  std::vector<int64_t> t[9];
-};
-
-// Host-side premultiplied tables (the reference constructor's output), no device.
-struct TriskTables {
-  Coefficients C;
-  CoefficientExport exported;
-};
-
-struct TriskModel {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  int pv = 0, ke = 0;  // pv: the kernels' PvMode (PVM_GASSMANN_DERIVED when the table allows it)
-  double alpha = 1.0, gravity = 1.0;
-  int64_t nc = 0, ne = 0, nv = 0, N = 0;
-  int block[3] = {128, 128, 128};  // threads per block of k_vertex, k_flux, k_tend
-  bool use_graph = true, use_pdl = true, identity = true;
-  Coefficients C;  // file numbering, 0-based (kept for export)
-  CoefficientExport exported;
-  std::vector<int32_t> cell_n2o, edge_n2o, vert_n2o, cell_o2n, edge_o2n, vert_o2n;
-  std::vector<void*> allocations;
-  DevTables T{};
-  DevWork W{};
-  double *y = nullptr, *acc = nullptr, *st = nullptr, *stage = nullptr, *dy = nullptr;
-  int32_t *state_n2o = nullptr, *state_o2n = nullptr, *vertex_o2n = nullptr;
-  double *area_c = nullptr, *area_v = nullptr, *partials = nullptr, *scalars = nullptr;
-  int* flag = nullptr;
-  cudaGraphExec_t graph = nullptr;
-  double graph_dt = NAN;
-  int64_t launches = 0;
-  double table_bytes_unique = 0;
-  double phase_bytes[3] = {0, 0, 0};
-  double pv_table_bytes_saved = 0;  // k_tend bytes per launch the derived PV edges do not read
-
-  ~TriskModel() {
-    int prev = -1;
-    cudaGetDevice(&prev);
-    cudaSetDevice(device);
-    if (graph) cudaGraphExecDestroy(graph);
-    if (stream) {
-      cudaStreamSynchronize(stream);
-      cudaStreamDestroy(stream);
-    }
-    for (void* p : allocations) cudaFree(p);
-    if (prev >= 0) cudaSetDevice(prev);
-  }
-
-  template <class T>
-  T* alloc(size_t count) {
-    void* p = nullptr;
-    CUDA_CHECK(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
-    allocations.push_back(p);
-    return static_cast<T*>(p);
-  }
-};
 
 namespace {
 
@@ -300,19 +229,8 @@ void run_steps(TriskModel& m, double dt, int64_t nsteps) {
   }
 }
 
-bool is_device_pointer(const void* p) {
-  cudaPointerAttributes a;
-  cudaError_t e = cudaPointerGetAttributes(&a, p);
-  if (e != cudaSuccess) {
-    cudaGetLastError();
-    return false;
-  }
-  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
-}
-
 void gather(TriskModel& m, double* dst, const double* src, const int32_t* idx, int64_t n) {
-  k_gather<<<(unsigned)cdiv(n, 256), 256, 0, m.stream>>>(dst, src, idx, n);
-  CUDA_CHECK(cudaGetLastError());
+  launch_gather(m.stream, dst, src, idx, n);
   m.launches++;
 }
 

@@ -1,0 +1,102 @@
+// The model object behind the C ABI and the helpers the model and ensemble translation
+// units share.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "common.hpp"
+#include "kernels.cuh"
+
+#define CUDA_CHECK(x)                                                                          \
+  do {                                                                                         \
+    cudaError_t err__ = (x);                                                                   \
+    if (err__ != cudaSuccess)                                                                  \
+      throw trisk::Error(TRISK_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(err__)); \
+  } while (0)
+
+namespace trisk {
+
+inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
+inline int64_t round_up(int64_t a, int64_t b) { return cdiv(a, b) * b; }
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) CUDA_CHECK(cudaSetDevice(dev));
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+// true for device or managed memory, false for host memory (pageable or pinned)
+bool is_device_pointer(const void* p);
+
+// dst[j] = src[idx[j]], j < n, on `stream`
+void launch_gather(cudaStream_t stream, double* dst, const double* src, const int32_t* idx, int64_t n);
+
+}  // namespace trisk
+
+// 1-based copies of the index tables handed out through TriskCoefficients views.
+struct CoefficientExport {
+  std::vector<int64_t> t[9];
+};
+
+// Host-side premultiplied tables (the reference constructor's output), no device.
+struct TriskTables {
+  trisk::Coefficients C;
+  CoefficientExport exported;
+};
+
+struct TriskModel {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int pv = 0, ke = 0;  // pv: the kernels' PvMode (PVM_GASSMANN_DERIVED when the table allows it)
+  double alpha = 1.0, gravity = 1.0;
+  int64_t nc = 0, ne = 0, nv = 0, N = 0;
+  int block[3] = {128, 128, 128};  // threads per block of k_vertex, k_flux, k_tend
+  bool use_graph = true, use_pdl = true, identity = true;
+  trisk::Coefficients C;  // file numbering, 0-based (kept for export)
+  CoefficientExport exported;
+  std::vector<int32_t> cell_n2o, edge_n2o, vert_n2o, cell_o2n, edge_o2n, vert_o2n;
+  std::vector<void*> allocations;
+  trisk::DevTables T{};
+  trisk::DevWork W{};
+  double *y = nullptr, *acc = nullptr, *st = nullptr, *stage = nullptr, *dy = nullptr;
+  int32_t *state_n2o = nullptr, *state_o2n = nullptr, *vertex_o2n = nullptr;
+  double *area_c = nullptr, *area_v = nullptr, *partials = nullptr, *scalars = nullptr;
+  int* flag = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  double graph_dt = NAN;
+  int64_t launches = 0;
+  double table_bytes_unique = 0;
+  double phase_bytes[3] = {0, 0, 0};
+  double pv_table_bytes_saved = 0;  // k_tend bytes per launch the derived PV edges do not read
+
+  ~TriskModel() {
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(device);
+    if (graph) cudaGraphExecDestroy(graph);
+    if (stream) {
+      cudaStreamSynchronize(stream);
+      cudaStreamDestroy(stream);
+    }
+    for (void* p : allocations) cudaFree(p);
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+
+  template <class T>
+  T* alloc(size_t count) {
+    void* p = nullptr;
+    CUDA_CHECK(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
+    allocations.push_back(p);
+    return static_cast<T*>(p);
+  }
+};

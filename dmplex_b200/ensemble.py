@@ -1,0 +1,78 @@
+"""Batched ensembles: many members on meshes of several levels in one persistent launch.
+
+There is no ensemble in the reference (it runs one model per process); each member here
+follows rk4_step! (src/TimeSteppers/RungeKutta.jl:18-29) on its group's model bit for bit.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._lib import check, lib, ptr
+from .model import TRiSKShallowWater, _state
+
+
+class Ensemble:
+    """groups: a list of (model, members, dt, nsteps). Members of a group share the model's
+    tables; every group has its own time step and number of RK4 steps."""
+
+    def __init__(self, groups):
+        self.groups = list(groups)
+        n = len(self.groups)
+        models = (C.c_void_p * n)(*[g[0].handle.value for g in self.groups])
+        members = np.array([g[1] for g in self.groups], dtype=np.int32)
+        dts = np.array([g[2] for g in self.groups], dtype=np.float64)
+        steps = np.array([g[3] for g in self.groups], dtype=np.int64)
+        handle = C.c_void_p()
+        check(lib.trisk_ensemble_create(models, members.ctypes.data, dts.ctypes.data, steps.ctypes.data, n,
+                                        C.byref(handle)))
+        self._h = handle
+        self._models = [g[0] for g in self.groups]  # the ensemble uses their device tables
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib.trisk_ensemble_destroy(self._h)
+            self._h = None
+
+    def set_member(self, group: int, member: int, y) -> None:
+        m: TRiSKShallowWater = self._models[group]
+        check(lib.trisk_ensemble_set_member(self._h, group, member, _state(y, m)))
+
+    def get_member(self, group: int, member: int, y=None):
+        m: TRiSKShallowWater = self._models[group]
+        if y is None:
+            y = np.zeros(m.state_size)
+        check(lib.trisk_ensemble_get_member(self._h, group, member, _state(y, m)))
+        return y
+
+    def run_async(self, steps: int) -> None:
+        check(lib.trisk_ensemble_run_async(self._h, int(steps)))
+
+    def synchronize(self) -> None:
+        check(lib.trisk_ensemble_synchronize(self._h))
+
+    def run(self, steps: int) -> None:
+        self.run_async(steps)
+        self.synchronize()
+
+    def steps_taken(self) -> list:
+        out = np.zeros(len(self.groups), dtype=np.int64)
+        check(lib.trisk_ensemble_steps(self._h, out.ctypes.data))
+        return out.tolist()
+
+    def reset(self) -> None:
+        check(lib.trisk_ensemble_reset(self._h))
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        check(lib.trisk_ensemble_stream(self._h, C.byref(s)))
+        return s.value or 0
+
+    def launch_count(self) -> int:
+        return int(lib.trisk_ensemble_launch_count(self._h))
+
+    def step_bytes(self) -> float:
+        b = C.c_double()
+        check(lib.trisk_ensemble_bytes(self._h, C.byref(b)))
+        return b.value

@@ -89,6 +89,25 @@ def courant_dt(grid, courant: float = 0.5, umax: float = 40.0) -> float:
     return courant * grid.dual_lengths.min() * EARTH_RADIUS / c
 
 
+def day_steps(grid, days: float = 1.0, courant: float = 0.5):
+    """(nsteps, dt) covering `days` simulated days at the Courant-number time step, with dt
+    shortened to divide the span exactly (examples/trisk_galewsky.jl:139-141)."""
+    span = 86400.0 * days
+    n = int(np.ceil(span / courant_dt(grid, courant)))
+    return n, span / n
+
+
+def ensemble_members(grid, count: int, seed: int, degree: int = 12, rms_range=(50.0, 300.0)):
+    """`count` member states with their own seeds, harmonic degree <= `degree` and rms drawn
+    uniformly from rms_range."""
+    rng = np.random.default_rng(seed)
+    states = []
+    for k in range(count):
+        rms = rng.uniform(*rms_range)
+        states.append(synthetic_state(grid, seed=seed * 100003 + k, degree=degree, rms=rms))
+    return states
+
+
 # Named workloads (sizes and schemes of the benchmark configurations).
 CONFIGS = {
     "L5-trisk-cell": {"level": 5, "pv_flux": "trisk", "kinetic_energy": "cell", "dt": 300.0, "steps": 100},

@@ -211,6 +211,31 @@ int trisk_autotune(TriskModel* model, double* y_device, double dt, int32_t steps
  * kernel launch and returns the mean duration in ms of each phase kernel in ms[3]. */
 int trisk_profile_phases(TriskModel* model, double* y_device, double dt, int64_t nsteps, double ms[3]);
 
+/* ---- batched ensembles ------------------------------------------------------------
+ * No counterpart in the reference, which runs one model per process (examples/
+ * trisk_shallow_water.jl:71-111); each member's arithmetic is that of rk4_step!
+ * (RungeKutta.jl:18-29) on its group's model, bit for bit. A group = `members[g]` states
+ * that share models[g]'s device tables (same mesh and scheme; all groups one scheme and
+ * device), with its own dt[g] and step count nsteps[g]. Up to 8 groups. One RK4 step of
+ * all unfinished groups is one CUDA graph of persistent kernels; the models must outlive
+ * the ensemble. */
+typedef struct TriskEnsemble TriskEnsemble;
+int trisk_ensemble_create(TriskModel* const* models, const int32_t* members, const double* dt,
+                          const int64_t* nsteps, int32_t ngroups, TriskEnsemble** out);
+void trisk_ensemble_destroy(TriskEnsemble* ensemble);
+/* Member state y = [u; h] in file numbering, host or device memory. */
+int trisk_ensemble_set_member(TriskEnsemble* ensemble, int32_t group, int32_t member, const double* y);
+int trisk_ensemble_get_member(TriskEnsemble* ensemble, int32_t group, int32_t member, double* y);
+/* Enqueues `steps` graph replays; a group stops advancing once it has taken nsteps[g]. */
+int trisk_ensemble_run_async(TriskEnsemble* ensemble, int64_t steps);
+int trisk_ensemble_synchronize(TriskEnsemble* ensemble);
+int trisk_ensemble_steps(TriskEnsemble* ensemble, int64_t* steps_taken); /* per group */
+int trisk_ensemble_reset(TriskEnsemble* ensemble);                        /* step counters to 0 */
+int trisk_ensemble_stream(TriskEnsemble* ensemble, void** stream);
+int64_t trisk_ensemble_launch_count(TriskEnsemble* ensemble);
+/* Algorithmic bytes of one RK4 step of all groups: sum 4 (T + 2 M N) + 15 M N. */
+int trisk_ensemble_bytes(TriskEnsemble* ensemble, double* step_bytes);
+
 /* ---- allocation-free entry point ---------------------------------------------------
  * No counterpart in the reference: it exists for callers that must not have the library
  * allocate device memory (a host whose device memory all comes from its own pool, such as
