@@ -118,6 +118,16 @@ def _load():
         "trisk_profile_phases": (C.c_int, [_p, _p, _f64, _i64, _p]),
         "trisk_weighted_sum_noalloc": (C.c_int, [_p, _p, _i64, _p, _p]),
         "trisk_model_info": (C.c_int, [_p, C.POINTER(_i32), _p, C.POINTER(_f64)]),
+        "trisk_closure_create": (C.c_int, [_i32, _p, C.POINTER(_p)]),
+        "trisk_closure_destroy": (None, [_p]),
+        "trisk_closure_param_count": (_i32, []),
+        "trisk_closure_get_params": (C.c_int, [_p, _p]),
+        "trisk_closure_set_params": (C.c_int, [_p, _p]),
+        "trisk_closure_forward": (C.c_int, [_p, _p, _i64, _p]),
+        "trisk_closure_gradients": (C.c_int, [_p, _p, _p, _i64, _p, C.POINTER(C.c_float)]),
+        "trisk_closure_adam": (C.c_int, [_p, C.c_float, C.c_float, C.c_float, C.c_float]),
+        "trisk_closure_synchronize": (C.c_int, [_p]),
+        "trisk_closure_stream": (C.c_int, [_p, C.POINTER(_p)]),
         "trisk_ensemble_create": (C.c_int, [_p, _p, _p, _p, _i32, C.POINTER(_p)]),
         "trisk_ensemble_destroy": (None, [_p]),
         "trisk_ensemble_set_member": (C.c_int, [_p, _i32, _i32, _p]),

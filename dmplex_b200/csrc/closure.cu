@@ -1,0 +1,617 @@
+// Learned flux closure: an edge-local MLP 24 -> 64 -> 64 -> 2 (GELU) whose two hidden
+// layers run on the 5th-generation tensor cores (tcgen05.mma, BF16 operands in shared
+// memory, FP32 accumulators in tensor memory), for inference and for training.
+//
+// There is no closure in the reference; this is the north star's addition. The MLP reads
+// 24 normalized features of an edge and returns two corrections (to the edge mass flux and
+// to the edge momentum tendency).
+//
+// One CTA = 4 warps = 128 threads; a tile = 128 edges, thread t owns row t. Shared-memory
+// operands use the no-swizzle "core matrix" layout (8 rows x 16 bytes, rows 16 bytes
+// apart). A buffer tiled as
+//     offset(r, c) = (c / 8) * CHUNK + (r / 8) * 128 + (r % 8) * 16 + (c % 8) * 2
+// is a K-major operand with rows r along M/N and columns c along K (SBO = 128, LBO =
+// CHUNK), and the same bytes are an MN-major operand with c along M/N and r along K
+// (SBO = CHUNK, LBO = 128). Forward GEMMs use the first view, backward GEMMs the second,
+// so no operand is ever transposed in memory.
+//
+//   forward    Z1 = X W1^T       M=128 N=64 K=32   (A = HX[:, 64:96] K-major, B = W1 K-major)
+//              H1 = gelu(Z1 + b1) -> bf16 -> HX[:, 0:64]
+//              Z2 = H1 W2^T      M=128 N=64 K=64   (A = HX[:, 0:64], B = W2 K-major)
+//              H2 = gelu(Z2 + b2);  Y = H2 W3^T + b3 on the CUDA cores (N = 2)
+//   backward   dH2 = (dY W3) * gelu'(Z2)                       CUDA cores -> DD[:, 0:64]
+//              G = dH2 W2        M=128 N=64 K=64   (A = DD[:, 0:64] K-major, B = W2 MN-major)
+//              dH1 = G * gelu'(Z1)                             -> DD[:, 64:128]
+//              DW += DD^T [H1 | X]   M=128 N=96 K=128 (A = DD MN-major, B = HX MN-major):
+//                   rows 0..63 x cols 0..63 = dW2, rows 64..127 x cols 64..87 = dW1
+//
+// Tensor memory (256 columns): Z1 at 0, Z2 (then G) at 64, DW at 128..224.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <memory>
+
+#include "model.hpp"
+
+namespace trisk {
+namespace closure {
+
+constexpr int NIN = 24, KIN = 32, NH = 64, NOUT = 2, TILE = 128;
+constexpr int HX_CHUNK = TILE * 16;  // 2048 B: one 8-column chunk of a 128-row tile
+constexpr int W_CHUNK = NH * 16;     // 1024 B: one 8-column chunk of a 64-row weight
+constexpr int HX_BYTES = 12 * HX_CHUNK;  // 96 columns: H1 (0..63) | X (64..95)
+constexpr int DD_BYTES = 16 * HX_CHUNK;  // 128 columns: dH2 (0..63) | dH1 (64..127)
+constexpr int W1_BYTES = 4 * W_CHUNK;    // 64 x 32
+constexpr int W2_BYTES = 8 * W_CHUNK;    // 64 x 64
+// + 64 B (mbarrier, TMEM address) + H2 (128 x 64 BF16) and dY (128 x 2 FP32) for training
+constexpr int SMEM_BYTES = HX_BYTES + DD_BYTES + W1_BYTES + W2_BYTES + 64 + TILE * NH * 2 + TILE * NOUT * 4;
+constexpr uint32_t TMEM_COLS = 256;
+constexpr int MBAR_SPIN_LIMIT = 1 << 20;
+
+// FP32 master parameters and their BF16 tensor-core copies (one contiguous block each).
+struct Params {
+  float W1[NH * NIN], b1[NH], W2[NH * NH], b2[NH], W3[NOUT * NH], b3[NOUT];
+};
+constexpr int NPARAM = sizeof(Params) / sizeof(float);
+struct ParamsBF16 {
+  __nv_bfloat16 W1[NH * KIN];  // padded to 32 inputs
+  __nv_bfloat16 W2[NH * NH];
+  __nv_bfloat16 W3[NOUT * NH];
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// no-swizzle shared-memory matrix descriptor (sm100 layout: version 1 at bit 46)
+__device__ __forceinline__ uint64_t sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
+}
+
+// instruction descriptor of kind::f16 with BF16 operands and an FP32 accumulator
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N, int a_mn, int b_mn) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)a_mn << 15) | ((uint32_t)b_mn << 16) |
+         ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, int accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+      "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+               : "memory");
+}
+
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// Waits for the mbarrier phase with a bounded number of tries; false after the bound.
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase) {
+  for (int i = 0; i < MBAR_SPIN_LIMIT; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(mbar), "r"(phase)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// 16 consecutive FP32 columns of this thread's TMEM lane
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int k = 0; k < 16; ++k) v[k] = __uint_as_float(r[k]);
+}
+
+__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+__device__ __forceinline__ float gelu_grad(float x) {
+  return 0.5f * (1.0f + erff(x * 0.70710678118654752f)) + x * 0.39894228040143268f * expf(-0.5f * x * x);
+}
+__device__ __forceinline__ float bf(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
+
+__device__ __forceinline__ uint32_t tile_off(int r, int c, int chunk) {
+  return (uint32_t)((c >> 3) * chunk + (r >> 3) * 128 + (r & 7) * 16 + (c & 7) * 2);
+}
+
+// 8 consecutive columns (c0 multiple of 8) of row r as one 16-byte store
+__device__ __forceinline__ void store8(unsigned char* base, int r, int c0, int chunk, const float* v) {
+  __align__(16) __nv_bfloat16 t[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) t[k] = __float2bfloat16_rn(v[k]);
+  *reinterpret_cast<uint4*>(base + tile_off(r, c0, chunk)) = *reinterpret_cast<const uint4*>(t);
+}
+
+struct Status {
+  int error;  // 1: a bounded tensor-core wait gave up
+};
+// Forward (TRAIN = 0) writes Y; training (TRAIN = 1) also accumulates the gradients of the
+// mean squared error (1/n) sum_rows sum_k (y_k - t_k)^2 into grad (FP32, zeroed by the
+// caller) and the squared-error sum into *loss. Column 88 of HX (the first padding column
+// of the input chunk) holds 1 for valid rows, so the weight-gradient MMA also returns the
+// bias gradients: DW[j][88] = sum_rows dH2[:, j] = db2[j], DW[64 + i][88] = db1[i]. W1's
+// padded input columns are 0, so the forward product ignores it.
+constexpr int ONES_COL = 64 + NIN;
+
+template <int TRAIN>
+__global__ void __launch_bounds__(TILE, 1) k_mlp(const __nv_bfloat16* __restrict__ X, int64_t n,
+                                                  const ParamsBF16* __restrict__ wbf, const Params* __restrict__ p,
+                                                  const float* __restrict__ target, float* __restrict__ Y,
+                                                  Params* __restrict__ grad, float* loss, float inv_n,
+                                                  Status* status) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  unsigned char* HX = smem;
+  unsigned char* DD = smem + HX_BYTES;
+  unsigned char* W1s = DD + DD_BYTES;
+  unsigned char* W2s = W1s + W1_BYTES;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(W2s + W2_BYTES);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(W2s + W2_BYTES + 16);
+  __nv_bfloat16* sH2 = reinterpret_cast<__nv_bfloat16*>(W2s + W2_BYTES + 64);  // 128 x 64 (training)
+  float* sDY = reinterpret_cast<float*>(W2s + W2_BYTES + 64 + TILE * NH * 2);   // 128 x 2 (training)
+  __shared__ float sb1[NH], sb2[NH], sw3[NOUT * NH], sb3[NOUT];
+  __shared__ int s_abort;
+
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const int64_t ntiles = (n + TILE - 1) / TILE;
+  if ((int64_t)blockIdx.x >= ntiles) return;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (t == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    s_abort = 0;
+  }
+  // weights: W1 (64 x 32, inputs padded with 0) and W2 (64 x 64) as K-major B operands
+  for (int idx = t; idx < NH * 4; idx += TILE) {
+    const int r = idx >> 2, c0 = (idx & 3) * 8;
+    *reinterpret_cast<uint4*>(W1s + tile_off(r, c0, W_CHUNK)) =
+        *reinterpret_cast<const uint4*>(wbf->W1 + r * KIN + c0);
+  }
+  for (int idx = t; idx < NH * 8; idx += TILE) {
+    const int r = idx >> 3, c0 = (idx & 7) * 8;
+    *reinterpret_cast<uint4*>(W2s + tile_off(r, c0, W_CHUNK)) =
+        *reinterpret_cast<const uint4*>(wbf->W2 + r * NH + c0);
+  }
+  for (int idx = t; idx < NH; idx += TILE) {
+    sb1[idx] = p->b1[idx];
+    sb2[idx] = p->b2[idx];
+  }
+  for (int idx = t; idx < NOUT * NH; idx += TILE) sw3[idx] = __bfloat162float(wbf->W3[idx]);
+  if (t < NOUT) sb3[t] = p->b3[t];
+  fence_async_smem();
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+  const uint32_t mb = smem_u32(mbar);
+  const uint32_t hx = smem_u32(HX), dd = smem_u32(DD), w1 = smem_u32(W1s), w2 = smem_u32(W2s);
+  const uint32_t ID_FWD = idesc_bf16(128, 64, 0, 0), ID_BWD = idesc_bf16(128, 64, 0, 1),
+                 ID_WGRAD = idesc_bf16(128, 96, 1, 1);
+  uint32_t phase = 0;
+  bool first_wgrad = true;
+  float loss_local = 0.0f, gw3 = 0.0f, gb3 = 0.0f;  // thread t: dW3[t / 64][t % 64]; t < 2: db3[t]
+
+  auto wait_mma = [&]() {  // the whole CTA waits; one give-up aborts the remaining tiles
+    bool ok = mbar_wait(mb, phase);
+    phase ^= 1;
+    if (!ok) atomicExch(&s_abort, 1);
+    fence_after();
+  };
+  auto sync_for_mma = [&]() {  // shared-memory writes -> visible to the tensor core
+    fence_async_smem();
+    fence_before();
+    __syncthreads();
+    fence_after();
+  };
+
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    if (s_abort) break;
+    const int64_t row = tile * TILE + t;
+    const bool valid = row < n;
+    // X -> HX[:, 64:96]: 24 features as three 16-byte chunks, then [1 (valid rows), 0 x 7]
+    {
+      uint4 q[3] = {make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0)};
+      if (valid) {
+        const uint4* src = reinterpret_cast<const uint4*>(X + row * NIN);
+        q[0] = src[0];
+        q[1] = src[1];
+        q[2] = src[2];
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) *reinterpret_cast<uint4*>(HX + tile_off(t, 64 + 8 * c, HX_CHUNK)) = q[c];
+      float ones[8] = {TRAIN && valid ? 1.0f : 0.0f, 0, 0, 0, 0, 0, 0, 0};
+      store8(HX, t, ONES_COL, HX_CHUNK, ones);
+    }
+    sync_for_mma();
+    if (t == 0) {  // Z1 = X W1^T
+#pragma unroll
+      for (int kk = 0; kk < 2; ++kk)
+        mma_bf16(tmem + 0, sdesc(hx + (8 + 2 * kk) * HX_CHUNK, HX_CHUNK, 128),
+                 sdesc(w1 + 2 * kk * W_CHUNK, W_CHUNK, 128), ID_FWD, kk);
+      mma_commit(mb);
+    }
+    wait_mma();
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {  // H1 = gelu(Z1 + b1) -> HX[:, 0:64]
+      float v[16];
+      tmem_ld16(lane_base + 16 * c, v);
+#pragma unroll
+      for (int k = 0; k < 16; ++k) v[k] = gelu(v[k] + sb1[16 * c + k]);
+      store8(HX, t, 16 * c, HX_CHUNK, v);
+      store8(HX, t, 16 * c + 8, HX_CHUNK, v + 8);
+    }
+    sync_for_mma();
+    if (t == 0) {  // Z2 = H1 W2^T
+#pragma unroll
+      for (int kk = 0; kk < 4; ++kk)
+        mma_bf16(tmem + 64, sdesc(hx + 2 * kk * HX_CHUNK, HX_CHUNK, 128), sdesc(w2 + 2 * kk * W_CHUNK, W_CHUNK, 128),
+                 ID_FWD, kk);
+      mma_commit(mb);
+    }
+    wait_mma();
+    float y[NOUT] = {sb3[0], sb3[1]};
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {  // Y = bf16(gelu(Z2 + b2)) W3^T + b3, FP32 accumulation
+      float v[16];
+      tmem_ld16(lane_base + 64 + 16 * c, v);
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        const int j = 16 * c + k;
+        const float h2 = bf(gelu(v[k] + sb2[j]));
+        y[0] += h2 * sw3[j];
+        y[1] += h2 * sw3[NH + j];
+        if (TRAIN) sH2[t * NH + j] = __float2bfloat16_rn(h2);
+      }
+    }
+    if (!TRAIN) {
+      if (valid) {
+        Y[row * NOUT + 0] = y[0];
+        Y[row * NOUT + 1] = y[1];
+      }
+      fence_before();
+      __syncthreads();  // the next tile rewrites HX
+      fence_after();
+      continue;
+    }
+    // ---- backward ----
+    float dy[NOUT];
+#pragma unroll
+    for (int k = 0; k < NOUT; ++k) {
+      const float diff = valid ? y[k] - target[row * NOUT + k] : 0.0f;
+      loss_local += diff * diff;
+      dy[k] = 2.0f * diff * inv_n;
+      sDY[t * NOUT + k] = dy[k];
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {  // dH2 = (dY W3) * gelu'(Z2 + b2) -> DD[:, 0:64]
+      float v[16];
+      tmem_ld16(lane_base + 64 + 16 * c, v);
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        const int j = 16 * c + k;
+        v[k] = (dy[0] * sw3[j] + dy[1] * sw3[NH + j]) * gelu_grad(v[k] + sb2[j]);
+      }
+      store8(DD, t, 16 * c, HX_CHUNK, v);
+      store8(DD, t, 16 * c + 8, HX_CHUNK, v + 8);
+    }
+    sync_for_mma();  // also publishes sH2 and sDY
+    if (t == 0) {    // G = dH2 W2 (overwrites Z2)
+#pragma unroll
+      for (int kk = 0; kk < 4; ++kk)
+        mma_bf16(tmem + 64, sdesc(dd + 2 * kk * HX_CHUNK, HX_CHUNK, 128), sdesc(w2 + 2 * kk * 128, 128, W_CHUNK),
+                 ID_BWD, kk);
+      mma_commit(mb);
+    }
+    {  // meanwhile: dW3[o][j] += sum_rows dY[:, o] H2[:, j], db3 += sum_rows dY
+      const int o = t / NH, j = t % NH;
+      float s = 0.0f;
+      for (int r = 0; r < TILE; ++r) s += sDY[r * NOUT + o] * __bfloat162float(sH2[r * NH + j]);
+      gw3 += s;
+      if (t < NOUT) {
+        float b = 0.0f;
+        for (int r = 0; r < TILE; ++r) b += sDY[r * NOUT + t];
+        gb3 += b;
+      }
+    }
+    wait_mma();
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {  // dH1 = G * gelu'(Z1 + b1) -> DD[:, 64:128]
+      float g[16], z[16];
+      tmem_ld16(lane_base + 64 + 16 * c, g);
+      tmem_ld16(lane_base + 16 * c, z);
+#pragma unroll
+      for (int k = 0; k < 16; ++k) g[k] *= gelu_grad(z[k] + sb1[16 * c + k]);
+      store8(DD, t, 64 + 16 * c, HX_CHUNK, g);
+      store8(DD, t, 64 + 16 * c + 8, HX_CHUNK, g + 8);
+    }
+    sync_for_mma();
+    if (t == 0) {  // DW += DD^T [H1 | X | 1]
+#pragma unroll
+      for (int kk = 0; kk < 8; ++kk)
+        mma_bf16(tmem + 128, sdesc(dd + 2 * kk * 128, 128, HX_CHUNK), sdesc(hx + 2 * kk * 128, 128, HX_CHUNK),
+                 ID_WGRAD, (first_wgrad && kk == 0) ? 0 : 1);
+      mma_commit(mb);
+    }
+    first_wgrad = false;
+    wait_mma();
+    fence_before();
+    __syncthreads();  // the next tile rewrites HX, DD, sH2 and sDY
+    fence_after();
+  }
+
+  if (TRAIN) {
+    if (!s_abort && !first_wgrad) {  // row t of DW: dW2 and db2 (t < 64) or dW1 and db1
+      float v[16];
+      if (t < NH) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          tmem_ld16(lane_base + 128 + 16 * c, v);
+#pragma unroll
+          for (int k = 0; k < 16; ++k) atomicAdd(&grad->W2[t * NH + 16 * c + k], v[k]);
+        }
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+          tmem_ld16(lane_base + 128 + 64 + 16 * c, v);
+          if (c == 1) atomicAdd(&grad->b2[t], v[ONES_COL - 64 - 16]);
+        }
+      } else {
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+          tmem_ld16(lane_base + 128 + 64 + 16 * c, v);
+#pragma unroll
+          for (int k = 0; k < 16; ++k) {
+            const int in = 16 * c + k;
+            if (in < NIN) atomicAdd(&grad->W1[(t - NH) * NIN + in], v[k]);
+            if (in == NIN) atomicAdd(&grad->b1[t - NH], v[k]);
+          }
+        }
+      }
+      atomicAdd(&grad->W3[t], gw3);
+      if (t < NOUT) atomicAdd(&grad->b3[t], gb3);
+    }
+    float l = loss_local;
+#pragma unroll
+    for (int s = 16; s > 0; s >>= 1) l += __shfl_xor_sync(0xffffffffu, l, s);
+    if (lane == 0) atomicAdd(loss, l);
+  }
+  if (s_abort && t == 0) atomicExch(&status->error, 1);
+  fence_before();
+  __syncthreads();
+  fence_after();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+}
+
+// Adam on the FP32 master parameters; refreshes the BF16 copies.
+__global__ void k_adam(Params* p, const Params* g, Params* m, Params* v, ParamsBF16* wbf, float lr, float beta1,
+                       float beta2, float eps, float c1, float c2) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= NPARAM) return;
+  float* P = reinterpret_cast<float*>(p);
+  const float* G = reinterpret_cast<const float*>(g);
+  float* Mm = reinterpret_cast<float*>(m);
+  float* Vv = reinterpret_cast<float*>(v);
+  const float gi = G[i];
+  const float mi = beta1 * Mm[i] + (1 - beta1) * gi;
+  const float vi = beta2 * Vv[i] + (1 - beta2) * gi * gi;
+  Mm[i] = mi;
+  Vv[i] = vi;
+  P[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+__global__ void k_refresh_bf16(const Params* p, ParamsBF16* wbf) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < NH * KIN) {
+    const int r = i / KIN, c = i % KIN;
+    wbf->W1[i] = __float2bfloat16_rn(c < NIN ? p->W1[r * NIN + c] : 0.0f);
+  }
+  if (i < NH * NH) wbf->W2[i] = __float2bfloat16_rn(p->W2[i]);
+  if (i < NOUT * NH) wbf->W3[i] = __float2bfloat16_rn(p->W3[i]);
+}
+
+}  // namespace closure
+}  // namespace trisk
+
+using namespace trisk;
+using namespace trisk::closure;
+
+// The closure works on the legacy default stream, so it is ordered with the caller's
+// default-stream work on the feature and target arrays it reads.
+struct TriskClosure {
+  int device = 0;
+  cudaStream_t stream = cudaStreamLegacy;
+  Params* p = nullptr;
+  Params *g = nullptr, *m = nullptr, *v = nullptr;
+  ParamsBF16* wbf = nullptr;
+  float* loss = nullptr;
+  Status* status = nullptr;
+  int64_t adam_step = 0;
+  int64_t launches = 0;
+  int grid_limit = 0;
+  ~TriskClosure() {
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(device);
+    cudaStreamSynchronize(stream);
+    for (void* q : {(void*)p, (void*)g, (void*)m, (void*)v, (void*)wbf, (void*)loss, (void*)status})
+      if (q) cudaFree(q);
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+namespace {
+
+TriskClosure* checked_c(TriskClosure* c) {
+  if (!c) throw Error(TRISK_ERR_ARGUMENT, "closure is NULL");
+  return c;
+}
+
+void check_status(TriskClosure& c) {
+  Status s{};
+  CUDA_CHECK(cudaMemcpyAsync(&s, c.status, sizeof(s), cudaMemcpyDeviceToHost, c.stream));
+  CUDA_CHECK(cudaStreamSynchronize(c.stream));
+  if (s.error) {
+    CUDA_CHECK(cudaMemset(c.status, 0, sizeof(Status)));
+    throw Error(TRISK_ERR_TIMEOUT, "a bounded tensor-core wait in the closure MLP gave up");
+  }
+}
+
+int mlp_grid(TriskClosure& c, int64_t n) {
+  const int64_t tiles = (n + TILE - 1) / TILE;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(tiles, c.grid_limit));
+}
+
+template <int TRAIN>
+void launch_mlp(TriskClosure& c, const __nv_bfloat16* X, int64_t n, const float* target, float* Y, float inv_n) {
+  if (n == 0) return;
+  k_mlp<TRAIN><<<mlp_grid(c, n), TILE, SMEM_BYTES, c.stream>>>(X, n, c.wbf, c.p, target, Y, c.g, c.loss, inv_n,
+                                                                 c.status);
+  CUDA_CHECK(cudaGetLastError());
+  c.launches++;
+}
+
+}  // namespace
+
+extern "C" {
+
+int trisk_closure_create(int32_t device, const float* params, TriskClosure** out) {
+  TRISK_API_BEGIN
+  if (!out) throw Error(TRISK_ERR_ARGUMENT, "NULL argument");
+  *out = nullptr;
+  auto c = std::make_unique<TriskClosure>();
+  c->device = device;
+  DeviceGuard guard(device);
+  CUDA_CHECK(cudaMalloc(&c->p, sizeof(Params)));
+  CUDA_CHECK(cudaMalloc(&c->g, sizeof(Params)));
+  CUDA_CHECK(cudaMalloc(&c->m, sizeof(Params)));
+  CUDA_CHECK(cudaMalloc(&c->v, sizeof(Params)));
+  CUDA_CHECK(cudaMalloc(&c->wbf, sizeof(ParamsBF16)));
+  CUDA_CHECK(cudaMalloc(&c->loss, sizeof(float)));
+  CUDA_CHECK(cudaMalloc(&c->status, sizeof(Status)));
+  CUDA_CHECK(cudaMemset(c->m, 0, sizeof(Params)));
+  CUDA_CHECK(cudaMemset(c->v, 0, sizeof(Params)));
+  CUDA_CHECK(cudaMemset(c->status, 0, sizeof(Status)));
+  if (params) CUDA_CHECK(cudaMemcpy(c->p, params, sizeof(Params), cudaMemcpyHostToDevice));
+  else CUDA_CHECK(cudaMemset(c->p, 0, sizeof(Params)));
+  k_refresh_bf16<<<(NH * NH + 255) / 256, 256, 0, c->stream>>>(c->p, c->wbf);
+  CUDA_CHECK(cudaGetLastError());
+  CUDA_CHECK(cudaFuncSetAttribute(k_mlp<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+  CUDA_CHECK(cudaFuncSetAttribute(k_mlp<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+  int sms = 0;
+  CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  c->grid_limit = sms * 2;  // two CTAs of 256 TMEM columns fit an SM's 512
+  CUDA_CHECK(cudaStreamSynchronize(c->stream));
+  *out = c.release();
+  TRISK_API_END
+}
+
+void trisk_closure_destroy(TriskClosure* c) { delete c; }
+
+int32_t trisk_closure_param_count(void) { return NPARAM; }
+
+int trisk_closure_get_params(TriskClosure* closure, float* params) {
+  TRISK_API_BEGIN
+  TriskClosure& c = *checked_c(closure);
+  if (!params) throw Error(TRISK_ERR_ARGUMENT, "NULL argument");
+  DeviceGuard guard(c.device);
+  CUDA_CHECK(cudaMemcpyAsync(params, c.p, sizeof(Params), cudaMemcpyDeviceToHost, c.stream));
+  CUDA_CHECK(cudaStreamSynchronize(c.stream));
+  TRISK_API_END
+}
+
+int trisk_closure_set_params(TriskClosure* closure, const float* params) {
+  TRISK_API_BEGIN
+  TriskClosure& c = *checked_c(closure);
+  if (!params) throw Error(TRISK_ERR_ARGUMENT, "NULL argument");
+  DeviceGuard guard(c.device);
+  CUDA_CHECK(cudaMemcpyAsync(c.p, params, sizeof(Params), cudaMemcpyHostToDevice, c.stream));
+  k_refresh_bf16<<<(NH * NH + 255) / 256, 256, 0, c.stream>>>(c.p, c.wbf);
+  CUDA_CHECK(cudaGetLastError());
+  CUDA_CHECK(cudaStreamSynchronize(c.stream));
+  TRISK_API_END
+}
+
+// Y (n x 2, FP32) = MLP(X) for X (n x 24, BF16), all device pointers.
+int trisk_closure_forward(TriskClosure* closure, const void* X, int64_t n, float* Y) {
+  TRISK_API_BEGIN
+  TriskClosure& c = *checked_c(closure);
+  if (!X || !Y || n < 0) throw Error(TRISK_ERR_ARGUMENT, "bad argument");
+  DeviceGuard guard(c.device);
+  launch_mlp<0>(c, static_cast<const __nv_bfloat16*>(X), n, nullptr, Y, 0.0f);
+  check_status(c);
+  TRISK_API_END
+}
+
+// Gradients (FP32, same layout as the parameters) of the mean squared error over the batch
+// and the loss; grads may be NULL (then kept on the device for trisk_closure_adam).
+int trisk_closure_gradients(TriskClosure* closure, const void* X, const float* target, int64_t n, float* grads,
+                            float* loss) {
+  TRISK_API_BEGIN
+  TriskClosure& c = *checked_c(closure);
+  if (!X || !target || n <= 0) throw Error(TRISK_ERR_ARGUMENT, "bad argument");
+  DeviceGuard guard(c.device);
+  CUDA_CHECK(cudaMemsetAsync(c.g, 0, sizeof(Params), c.stream));
+  CUDA_CHECK(cudaMemsetAsync(c.loss, 0, sizeof(float), c.stream));
+  launch_mlp<1>(c, static_cast<const __nv_bfloat16*>(X), n, target, nullptr, 1.0f / (float)n);
+  if (grads) CUDA_CHECK(cudaMemcpyAsync(grads, c.g, sizeof(Params), cudaMemcpyDeviceToHost, c.stream));
+  float l = 0;
+  CUDA_CHECK(cudaMemcpyAsync(&l, c.loss, sizeof(float), cudaMemcpyDeviceToHost, c.stream));
+  check_status(c);
+  if (loss) *loss = l / (float)n;
+  TRISK_API_END
+}
+
+// One Adam step with the gradients left by the last trisk_closure_gradients call.
+int trisk_closure_adam(TriskClosure* closure, float lr, float beta1, float beta2, float eps) {
+  TRISK_API_BEGIN
+  TriskClosure& c = *checked_c(closure);
+  DeviceGuard guard(c.device);
+  c.adam_step++;
+  const float c1 = 1.0f - powf(beta1, (float)c.adam_step), c2 = 1.0f - powf(beta2, (float)c.adam_step);
+  k_adam<<<(NPARAM + 255) / 256, 256, 0, c.stream>>>(c.p, c.g, c.m, c.v, c.wbf, lr, beta1, beta2, eps, c1, c2);
+  k_refresh_bf16<<<(NH * NH + 255) / 256, 256, 0, c.stream>>>(c.p, c.wbf);
+  CUDA_CHECK(cudaGetLastError());
+  c.launches += 2;
+  TRISK_API_END
+}
+
+int trisk_closure_synchronize(TriskClosure* closure) {
+  TRISK_API_BEGIN
+  TriskClosure& c = *checked_c(closure);
+  DeviceGuard guard(c.device);
+  check_status(c);
+  TRISK_API_END
+}
+
+int trisk_closure_stream(TriskClosure* closure, void** stream) {
+  TRISK_API_BEGIN
+  TriskClosure& c = *checked_c(closure);
+  if (!stream) throw Error(TRISK_ERR_ARGUMENT, "NULL argument");
+  *stream = (void*)c.stream;
+  TRISK_API_END
+}
+
+}  // extern "C"

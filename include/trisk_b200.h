@@ -236,6 +236,28 @@ int64_t trisk_ensemble_launch_count(TriskEnsemble* ensemble);
 /* Algorithmic bytes of one RK4 step of all groups: sum 4 (T + 2 M N) + 15 M N. */
 int trisk_ensemble_bytes(TriskEnsemble* ensemble, double* step_bytes);
 
+/* ---- learned flux closure: the network ------------------------------------------------
+ * No counterpart in the reference. An edge-local MLP 24 -> 64 -> 64 -> 2 (GELU) whose two
+ * hidden layers run as tcgen05 BF16 MMAs with FP32 accumulators in tensor memory, for
+ * inference and training (FP32 master weights, Adam). Parameters are 5890 floats: W1 (64 x
+ * 24), b1, W2 (64 x 64), b2, W3 (2 x 64), b3, row-major. Device arrays: X (n x 24, BF16),
+ * targets and outputs (n x 2, FP32). A bounded wait on the tensor core that gives up
+ * returns TRISK_ERR_TIMEOUT. */
+typedef struct TriskClosure TriskClosure;
+int trisk_closure_create(int32_t device, const float* params, TriskClosure** out); /* params: host, or NULL */
+void trisk_closure_destroy(TriskClosure* closure);
+int32_t trisk_closure_param_count(void);
+int trisk_closure_get_params(TriskClosure* closure, float* params);
+int trisk_closure_set_params(TriskClosure* closure, const float* params);
+int trisk_closure_forward(TriskClosure* closure, const void* X, int64_t n, float* Y);
+/* Gradient of (1/n) sum_rows sum_k (Y_k - target_k)^2 into grads (host, or NULL to keep it on
+ * the device for trisk_closure_adam) and the mean loss into *loss. */
+int trisk_closure_gradients(TriskClosure* closure, const void* X, const float* target, int64_t n, float* grads,
+                            float* loss);
+int trisk_closure_adam(TriskClosure* closure, float lr, float beta1, float beta2, float eps);
+int trisk_closure_synchronize(TriskClosure* closure);
+int trisk_closure_stream(TriskClosure* closure, void** stream);
+
 /* ---- allocation-free entry point ---------------------------------------------------
  * No counterpart in the reference: it exists for callers that must not have the library
  * allocate device memory (a host whose device memory all comes from its own pool, such as

@@ -1,0 +1,81 @@
+"""The closure MLP on the tensor cores (tcgen05) against its FP64 oracle.
+
+The oracle's gradients are pinned by central finite differences (CPU test); the GPU kernels
+are compared with the oracle that rounds to BF16 where the kernels hold BF16 values.
+Tolerance: 2e-2 relative (Frobenius norm per parameter block) for gradients, 1e-2 for
+outputs; the differences come from FP32 accumulation order and from activations that land
+on the other side of a BF16 rounding boundary.
+"""
+import numpy as np
+import pytest
+
+from oracle import closure_oracle as co
+
+
+def _data(n, seed):
+    rng = np.random.default_rng(seed)
+    X = co.bf16(rng.standard_normal((n, co.NIN)))
+    T = np.stack([np.sin(X[:, 0]) + 0.3 * X[:, 1] * X[:, 2], np.cos(X[:, 3]) - 0.2 * X[:, 4]], axis=1)
+    return X, T
+
+
+def test_oracle_gradients_finite_differences():
+    X, T = _data(37, 1)
+    p = co.init_params(3)
+    g, _ = co.gradients(p, X, T, rounding=False)
+    rng = np.random.default_rng(0)
+    for idx in rng.choice(co.NPARAM, 40, replace=False):
+        e = np.zeros(co.NPARAM)
+        e[idx] = 1e-6
+        fd = (co.loss(p + e, X, T, rounding=False) - co.loss(p - e, X, T, rounding=False)) / 2e-6
+        assert abs(fd - g[idx]) <= 1e-6 + 1e-5 * abs(fd)
+
+
+def _blocks(v):
+    out, k = {}, 0
+    for name, shape in co.SHAPES:
+        n = int(np.prod(shape))
+        out[name] = v[k:k + n]
+        k += n
+    return out
+
+
+def _rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [1, 100, 128, 1000, 70000])
+def test_forward_and_gradients_match_oracle(require_gpu, n):
+    import torch
+    import dmplex_b200.closure as cl
+    X, T = _data(n, n)
+    p = co.init_params(7)
+    p[co.NH * co.NIN:co.NH * co.NIN + co.NH] = 0.1  # nonzero b1
+    mlp = cl.ClosureMLP(p.astype(np.float32))
+    Xd = torch.from_numpy(X.astype(np.float32)).to(torch.bfloat16).cuda().contiguous()
+    Td = torch.from_numpy(T.astype(np.float32)).cuda().contiguous()
+    pf = mlp.params().astype(np.float64)
+    Y = mlp.forward(Xd).cpu().numpy()
+    Yo, _ = co.forward(pf, X)
+    assert _rel(Y, Yo) <= 1e-2
+    g, loss = mlp.gradients(Xd, Td)
+    go, lo = co.gradients(pf, X, T)
+    assert abs(loss - lo) <= 1e-2 * lo
+    gb, gob = _blocks(g), _blocks(go)
+    for name, _ in co.SHAPES:
+        assert _rel(gb[name], gob[name]) <= 2e-2, name
+
+
+@pytest.mark.gpu
+def test_training_reduces_loss(require_gpu):
+    import torch
+    import dmplex_b200.closure as cl
+    X, T = _data(65536, 5)
+    mlp = cl.ClosureMLP(seed=1)
+    Xd = torch.from_numpy(X.astype(np.float32)).to(torch.bfloat16).cuda().contiguous()
+    Td = torch.from_numpy(T.astype(np.float32)).cuda().contiguous()
+    first = mlp.train_step(Xd, Td, 3e-3)
+    for _ in range(300):
+        last = mlp.train_step(Xd, Td, 3e-3)
+    assert np.isfinite(last) and last < 0.1 * first
