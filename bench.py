@@ -46,6 +46,7 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=15.0, help="bounded CPU-baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble leg")
+    p.add_argument("--no-closure", action="store_true", help="skip the learned-closure leg")
     p.add_argument("--level", type=int, default=LEVEL, help="mesh level (7 is the benchmark workload)")
     args = p.parse_args()
     return args
@@ -206,6 +207,100 @@ def run_ensemble_leg(local_rank, seed):
             "frac": nbytes / (ms * 1e-3) / 1e9 / peak}
 
 
+CLOSURE_WEIGHTS = os.path.join(ROOT, "dmplex_b200", "data", "closure_hexagon6.npz")
+CLOSURE_SUMMARY = os.path.join(ROOT, "dmplex_b200", "data", "closure_hexagon6.json")
+
+
+def run_closure_leg(local_rank, members=128, seed=7):
+    """GPU seconds per simulated day: hexagon 6 x `members` with the learned closure (dt 150
+    s, TRiSK, FP64 state), the same ensemble without it, and one plain hexagon-8 member
+    (dt 20 s); plus the errors of the committed closure experiment, when present."""
+    import torch
+    import dmplex_b200 as d
+    from dmplex_b200 import workloads as w
+    from dmplex_b200.closure import ClosureMLP
+    from dmplex_b200.coarsen import edge_geometry
+    from dmplex_b200._lib import TriskError
+    si = w.si_parameters()
+    out = {"workload": f"hexagon6 x {members} members, TRiSK/cell, dt 150 s, FP64 state, 1 simulated day",
+           "members": members}
+    g6 = d.TRiSKGrid(d.create_hexagon_mesh(6, centroidal=True))
+    m6 = d.TRiSKShallowWater(g6, pv_flux="trisk", kinetic_energy="cell", device=local_rank, **si)
+    states = w.ensemble_members(g6, members, seed=seed, degree=8, rms_range=(100.0, 100.0))
+    steps = 576
+    net, norm = None, None
+    if os.path.exists(CLOSURE_WEIGHTS):
+        z = np.load(CLOSURE_WEIGHTS)
+        net, norm = ClosureMLP(z["params"], device=local_rank), z["norm"]
+        out["weights"] = "trained (dmplex_b200/data/closure_hexagon6.npz)"
+    else:
+        net = ClosureMLP(device=local_rank, seed=0)
+        norm = np.concatenate([np.zeros(24), np.ones(24), [0.0, 0.0]])
+        out["weights"] = "untrained, zero output scales (timing only)"
+
+    def timed(with_closure):
+        ens = d.Ensemble([(m6, members, 150.0, steps)])
+        for k, y in enumerate(states):
+            ens.set_member(0, k, y)
+        if with_closure:
+            ens.set_closure(0, net, edge_geometry(g6), norm)
+        e0 = ens.energy(0)
+        ens.run(2)
+        ens.reset()
+        for k, y in enumerate(states):
+            ens.set_member(0, k, y)
+        stream = torch.cuda.ExternalStream(ens.stream(), device=local_rank)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        launches0 = ens.launch_count()
+        a.record(stream)
+        ens.run_async(steps)
+        b.record(stream)
+        try:
+            ens.synchronize()
+        except TriskError as err:  # a member blew up: the day was still computed and timed
+            if err.status != 4:
+                raise
+            torch.cuda.synchronize(local_rank)
+            return a.elapsed_time(b) / 1e3, ens.launch_count() - launches0, "non-finite state"
+        if with_closure:
+            ens.closure_check()
+        drift = np.abs(ens.energy(0) - e0) / np.abs(e0)
+        return a.elapsed_time(b) / 1e3, ens.launch_count() - launches0, float(drift.max())
+
+    out["closure_gpu_seconds_per_simulated_day"], out["closure_gpu_launches"], out["closure_max_energy_drift_day"] = \
+        timed(True)
+    out["plain_gpu_seconds_per_simulated_day"], _, out["plain_max_energy_drift_day"] = timed(False)
+    out["closure_cell_steps_per_s"] = members * g6.nc * steps / out["closure_gpu_seconds_per_simulated_day"]
+    # one plain hexagon-8 member at dt = 20 s: time 40 steps, scale to a day
+    g8 = d.TRiSKGrid(d.create_hexagon_mesh(8, centroidal=True))
+    m8 = d.TRiSKShallowWater(g8, pv_flux="trisk", kinetic_energy="cell", device=local_rank, **si)
+    y8 = torch.from_numpy(w.synthetic_state(g8, seed=seed)).to(f"cuda:{local_rank}")
+    s8 = torch.cuda.ExternalStream(m8.stream(), device=local_rank)
+    m8.rk4_async(y8, 20.0, 5)
+    m8.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(s8)
+    m8.rk4_async(y8, 20.0, 40)
+    b.record(s8)
+    m8.synchronize()
+    per_day8 = a.elapsed_time(b) / 1e3 / 40 * 4320
+    out["plain_hexagon8_gpu_seconds_per_member_day"] = per_day8
+    per_member = out["closure_gpu_seconds_per_simulated_day"] / members
+    out["closure_gpu_seconds_per_member_day"] = per_member
+    out["gpu_seconds_ratio_hexagon8_over_closure_hexagon6"] = per_day8 / per_member
+    if os.path.exists(CLOSURE_SUMMARY):
+        with open(CLOSURE_SUMMARY) as f:
+            s = json.load(f)
+        out["errors_vs_coarse_grained_hexagon8"] = {
+            k: {"h_l2_last_day_m": float(np.mean(s[k]["h_l2"][-1])),
+                "zeta_l2_last_day": float(np.mean(s[k]["zeta_l2"][-1])),
+                "fallback_members": s[k].get("fallback_members")}
+            for k in ("plain_coarse", "closure_coarse", "closure_coarse_no_fallback",
+                      "closure_mass_flux_only_no_fallback") if k in s}
+        out["errors_source"] = "dmplex_b200/data/closure_hexagon6.json (python -m dmplex_b200.closure_pipeline)"
+    return out
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -311,6 +406,9 @@ def run_b200(args, rank, world, local_rank):
         ensemble = run_ensemble_leg(local_rank, seed=1000 * (rank + 1))
         if world > 1:
             ensemble["value_all_ranks"] = world * ensemble["value"]
+    closure = None
+    if not args.no_closure:
+        closure = run_closure_leg(local_rank)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -323,7 +421,8 @@ def run_b200(args, rank, world, local_rank):
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": config_dict(g, world, args.level), "clocks": clocks.summary(), "e2e": e2e,
-                "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu, "ensemble": ensemble}
+                "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu, "ensemble": ensemble,
+                "closure": closure}
         print(json.dumps(line), flush=True)
     del m
 

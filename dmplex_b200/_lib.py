@@ -139,6 +139,11 @@ def _load():
         "trisk_ensemble_stream": (C.c_int, [_p, C.POINTER(_p)]),
         "trisk_ensemble_launch_count": (_i64, [_p]),
         "trisk_ensemble_bytes": (C.c_int, [_p, C.POINTER(_f64)]),
+        "trisk_ensemble_energy": (C.c_int, [_p, _i32, _p]),
+        "trisk_ensemble_set_closure": (C.c_int, [_p, _i32, _p, _p, _p, _i32]),
+        "trisk_ensemble_closure_mask": (C.c_int, [_p, _i32, _p]),
+        "trisk_ensemble_features": (C.c_int, [_p, _i32, _p, _p, _p]),
+        "trisk_ensemble_closure_check": (C.c_int, [_p]),
         "trisk_autotune": (C.c_int, [_p, _p, _f64, _i32, C.POINTER(_f64)]),
     }
     for name, (res, args) in sig.items():

@@ -1,0 +1,404 @@
+"""Learned flux closure: training data, training and evaluation (no reference counterpart).
+
+1. Fine runs. Plain TRiSK runs on a fine hexagon mesh (a batched ensemble, one member per
+   seed) are coarse-grained (coarsen.CoarseGrainer) to the coarse mesh at snapshot times t
+   and t + delta.
+2. Targets. One coarse RK4 step of length delta from the coarse-grained state at t gives
+   Y_hat; the missing tendency r = (Y_c(t + delta) - Y_hat) / delta splits into
+     - the momentum correction dQ_e = r_u (edges), and
+     - a mass-flux correction dF with -D dF = r_h (D: the coarse divergence), the minimum-
+       norm solution dF = D^T psi, (D D^T) psi = -r_h, by batched conjugate gradients. The
+       continuity equation stays in flux form, so the corrected model conserves mass to
+       round-off.
+3. Training: the edge-local MLP (closure.ClosureMLP, tensor cores) on normalized features
+   and targets, Adam, batches of 65536 edges.
+4. Evaluation: coarse ensembles with and without the closure, started from the coarse-
+   grained fine state, against the coarse-grained fine run; h and relative-vorticity L2
+   errors per day; the closure is switched off for a member whose energy drifts by more
+   than a threshold per day (the plain FP64 step is the fallback).
+"""
+from __future__ import annotations
+
+import json
+import time
+
+import numpy as np
+
+from . import workloads as w
+from .closure import ClosureMLP
+from .coarsen import CoarseGrainer, divergence_matrix, edge_geometry, relative_vorticity_matrix
+from .ensemble import Ensemble
+from .mesh import TRiSKGrid, create_hexagon_mesh
+from .model import TRiSKShallowWater, model_tables
+
+PV, KE = "trisk", "cell"
+NFEAT = 24
+
+
+def _grid(level):
+    return TRiSKGrid(create_hexagon_mesh(level, centroidal=True))
+
+
+def _torch_sparse(m, device):
+    import torch
+    m = m.tocsr()
+    return torch.sparse_csr_tensor(torch.from_numpy(m.indptr), torch.from_numpy(m.indices),
+                                   torch.from_numpy(m.data), size=m.shape, dtype=torch.float64, device=device)
+
+
+def fine_snapshots(gf, gc, seeds, days, snapshots_per_member, dt_fine=20.0, pair_steps=8, spinup_days=0.25,
+                   device=0, record_days=False):
+    """Coarse-grained pairs (Y0 at t, Y1 at t + pair_steps dt_fine) of fine runs, as CUDA
+    float64 tensors (state x snapshots); with record_days also the coarse state at every
+    whole day (days + 1 states per seed). Returns (Y0, Y1, delta, daily, seconds)."""
+    import torch
+    si = w.si_parameters()
+    mf = TRiSKShallowWater(gf, pv_flux=PV, kinetic_energy=KE, device=device, **si)
+    total = int(round(days * 86400 / dt_fine))
+    ens = Ensemble([(mf, len(seeds), dt_fine, total)])
+    for k, seed in enumerate(seeds):
+        ens.set_member(0, k, w.synthetic_state(gf, seed=seed))
+    cg = CoarseGrainer(gf, gc)
+    dev = f"cuda:{device}"
+    buf = torch.empty((mf.state_size, len(seeds)), dtype=torch.float64, device=dev)
+    col = torch.empty(mf.state_size, dtype=torch.float64, device=dev)
+
+    def coarse_now():
+        for k in range(len(seeds)):
+            ens.get_member(0, k, col)
+            buf[:, k] = col
+        torch.cuda.synchronize()
+        return cg.torch_apply(buf)
+
+    spinup = int(round(spinup_days * 86400 / dt_fine))
+    span = max(total - spinup - pair_steps, 1)
+    every = max(span // max(snapshots_per_member, 1), pair_steps + 1)
+    marks = set(range(spinup, total - pair_steps, every)) if snapshots_per_member else set()
+    day_steps = int(round(86400 / dt_fine))
+    Y0, Y1, daily = [], [], []
+    step, seconds = 0, 0.0
+    if record_days:
+        daily.append(coarse_now())
+    while step < total:
+        nxt = [s for s in sorted(marks) if s > step]
+        targets = [total] + ([nxt[0]] if nxt else []) + ([(step // day_steps + 1) * day_steps] if record_days else [])
+        stop = min(targets)
+        t0 = time.perf_counter()
+        ens.run(stop - step)
+        seconds += time.perf_counter() - t0
+        step = stop
+        if step in marks:
+            Y0.append(coarse_now())
+            t0 = time.perf_counter()
+            ens.run(pair_steps)
+            seconds += time.perf_counter() - t0
+            step += pair_steps
+            Y1.append(coarse_now())
+        if record_days and step % day_steps == 0:
+            daily.append(coarse_now())
+    cat = (lambda a: torch.cat(a, dim=1)) if Y0 else (lambda a: None)
+    return cat(Y0), cat(Y1), pair_steps * dt_fine, daily, seconds
+
+
+def cg_solve(DDt, rhs, null, iters=500, rtol=1e-9):
+    """Solve (D D^T) x = rhs column by column (batched CG), rhs projected orthogonal to the
+    null vector `null` first."""
+    import torch
+    rhs = rhs - null[:, None] * (null @ rhs)[None, :] / (null @ null)
+    x = torch.zeros_like(rhs)
+    r = rhs.clone()
+    p = r.clone()
+    rs = (r * r).sum(0)
+    rs0 = rs.clone().clamp_min(1e-300)
+    for _ in range(iters):
+        Ap = DDt(p)
+        alpha = rs / (p * Ap).sum(0).clamp_min(1e-300)
+        x += alpha * p
+        r -= alpha * Ap
+        rs_new = (r * r).sum(0)
+        if float((rs_new / rs0).max().sqrt()) < rtol:
+            break
+        p = r + (rs_new / rs.clamp_min(1e-300)) * p
+        rs = rs_new
+    return x
+
+
+def residual_targets(gc, Y0, Y1, delta, device=0, coarse_steps=1):
+    """(dF, dQ): edges x snapshots (CUDA float64). The coarse model covers delta in
+    `coarse_steps` RK4 steps; the residual is the mean missing tendency over the window."""
+    import torch
+    si = w.si_parameters()
+    mc = TRiSKShallowWater(gc, pv_flux=PV, kinetic_energy=KE, device=device, **si)
+    S = Y0.shape[1]
+    ens = Ensemble([(mc, S, delta / coarse_steps, coarse_steps)])
+    col = torch.empty(mc.state_size, dtype=torch.float64, device=Y0.device)
+    for k in range(S):
+        col.copy_(Y0[:, k])
+        ens.set_member(0, k, col)
+    ens.run(coarse_steps)
+    ens.reset()
+    Yh = torch.empty_like(Y0)
+    for k in range(S):
+        ens.get_member(0, k, col)
+        Yh[:, k] = col
+    for k in range(S):  # the features are those of the state at t
+        col.copy_(Y0[:, k])
+        ens.set_member(0, k, col)
+    r = (Y1 - Yh) / delta
+    ne = gc.ne
+    coeffs = model_tables(gc, pv_flux=PV, kinetic_energy=KE, **si)
+    D = _torch_sparse(divergence_matrix(coeffs), Y0.device)
+    Dt = _torch_sparse(divergence_matrix(coeffs).T.tocsr(), Y0.device)
+    A = torch.from_numpy(gc.cell_areas).to(Y0.device)
+    psi = cg_solve(lambda p: D @ (Dt @ p), -r[ne:], A)
+    dF = Dt @ psi
+    return dF, r[:ne].clone(), mc, ens
+
+
+def features(ens, group, gc, norm, device=0):
+    import torch
+    rows = gc.ne * ens.groups[group][1]
+    X = torch.empty((rows, NFEAT), dtype=torch.bfloat16, device=f"cuda:{device}")
+    return ens.features(group, X, norm, edge_geometry(gc))
+
+
+def build_dataset(gc, Y0, dF, dQ, ens, device=0, sample=2_000_000):
+    """Normalized (X, T) over all (edge, snapshot) rows in file edge order e * S + s, the
+    feature normalization and the target scales."""
+    import torch
+    S = Y0.shape[1]
+    raw_norm = np.concatenate([np.zeros(NFEAT), np.ones(NFEAT), [1.0, 1.0]])
+    Xraw = features(ens, 0, gc, raw_norm, device)
+    idx = torch.randint(0, Xraw.shape[0], (min(sample, Xraw.shape[0]),), device=Xraw.device)
+    xs = Xraw[idx].double()
+    mean = xs.mean(0).cpu().numpy()
+    std = xs.std(0).cpu().numpy()
+    std[std == 0] = 1.0
+    del Xraw
+    T = torch.stack([dF.reshape(-1), dQ.reshape(-1)], dim=1)  # rows e * S + s
+    tstd = T.std(0).cpu().numpy()
+    tstd[tstd == 0] = 1.0
+    norm = np.concatenate([mean, 1.0 / std, tstd])
+    X = features(ens, 0, gc, norm, device)
+    Tn = (T / torch.from_numpy(tstd).to(T.device)).float().contiguous()
+    return X, Tn, norm
+
+
+def train(mlp: ClosureMLP, X, T, epochs=3, batch=65536, lr=1e-3, holdout=0.05, seed=0):
+    """Adam on random batches; returns per-epoch mean losses, the held-out loss and the
+    held-out loss of predicting zero (the coarse model without the closure)."""
+    import torch
+    g = torch.Generator(device=X.device)
+    g.manual_seed(seed)
+    n = X.shape[0]
+    perm = torch.randperm(n, device=X.device, generator=g)
+    nh = int(n * holdout)
+    hold, tr = perm[:nh], perm[nh:]
+    history = []
+    steps = max(1, (len(tr) // batch))
+    total = epochs * steps
+    k = 0
+    for ep in range(epochs):
+        order = tr[torch.randperm(len(tr), device=X.device, generator=g)]
+        losses = []
+        for b in range(steps):
+            idx = order[b * batch:(b + 1) * batch]
+            rate = lr * 0.5 * (1 + np.cos(np.pi * k / total))  # cosine schedule
+            losses.append(mlp.train_step(X[idx].contiguous(), T[idx].contiguous(), rate))
+            k += 1
+        history.append(float(np.mean(losses)))
+    held = []
+    for b in range(0, nh, batch):
+        idx = hold[b:b + batch]
+        _, l = mlp.gradients(X[idx].contiguous(), T[idx].contiguous())
+        held.append(l * len(idx))
+    zero = float((T[hold].double() ** 2).sum(1).mean()) if nh else float("nan")
+    return history, float(np.sum(held) / max(nh, 1)), zero
+
+
+def output_skill(mlp: ClosureMLP, X, T, rows=2_000_000, seed=1):
+    """Per output: 1 - MSE / mean square of the target on a random sample (1: perfect, 0:
+    no better than the coarse model without the closure)."""
+    import torch
+    g = torch.Generator(device=X.device)
+    g.manual_seed(seed)
+    idx = torch.randint(0, X.shape[0], (min(rows, X.shape[0]),), device=X.device, generator=g)
+    Y = mlp.forward(X[idx].contiguous()).double()
+    Tt = T[idx].double()
+    return (1 - ((Y - Tt) ** 2).mean(0) / (Tt ** 2).mean(0)).cpu().numpy().tolist()
+
+
+def l2_errors(gc, Vc, Y, Yt):
+    """h and relative-vorticity area-weighted L2 errors (columns = members)."""
+    ne = gc.ne
+    dh = Y[ne:] - Yt[ne:]
+    eh = np.sqrt((gc.cell_areas[:, None] * dh ** 2).sum(0) / (4 * np.pi))
+    dz = Vc @ (Y[:ne] - Yt[:ne])
+    ez = np.sqrt((gc.vertex_areas[:, None] * dz ** 2).sum(0) / (4 * np.pi))
+    return eh, ez
+
+
+def run_coarse(gc, Y_init, days, dt, daily_truth, mlp=None, norm=None, drift_per_day=1e-6, device=0,
+               every_stage=False, momentum_scale=1.0):
+    """Coarse ensemble (members = columns of Y_init) for `days` days; h and vorticity errors
+    against the daily truth, GPU seconds, and the members that fell back to the plain step.
+    momentum_scale multiplies the closure's momentum correction (0 keeps only the mass-flux
+    correction)."""
+    if norm is not None:
+        norm = np.array(norm, dtype=np.float64)
+        norm[2 * NFEAT + 1] *= momentum_scale
+    import torch
+    si = w.si_parameters()
+    mc = TRiSKShallowWater(gc, pv_flux=PV, kinetic_energy=KE, device=device, **si)
+    S = Y_init.shape[1]
+    steps_day = int(round(86400 / dt))
+    ens = Ensemble([(mc, S, 86400 / steps_day, steps_day * days)])
+    col = torch.empty(mc.state_size, dtype=torch.float64, device=Y_init.device)
+    for k in range(S):
+        col.copy_(Y_init[:, k])
+        ens.set_member(0, k, col)
+    if mlp is not None:
+        ens.set_closure(0, mlp, edge_geometry(gc), norm, every_stage)
+    on = np.ones(S, dtype=np.float32)
+    e0 = ens.energy(0)
+    Vc = relative_vorticity_matrix(model_tables(gc, pv_flux=PV, kinetic_energy=KE, **si))
+    stream = torch.cuda.ExternalStream(ens.stream(), device=Y_init.device)
+    from ._lib import TriskError
+    errs_h, errs_z, drifts, gpu_ms = [], [], [], 0.0
+    diverged = None
+    for day in range(1, days + 1):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        ens.run_async(steps_day)
+        b.record(stream)
+        try:
+            ens.synchronize()
+        except TriskError as err:
+            if err.status != 4:
+                raise
+            diverged = day  # a member's state became non-finite during this day
+            break
+        gpu_ms += a.elapsed_time(b)
+        drift = np.abs(ens.energy(0) - e0) / np.abs(e0) / day
+        drifts.append(float(drift.max()))
+        if mlp is not None:
+            ens.closure_check()
+            newly = (drift > drift_per_day) & (on > 0)
+            if newly.any():
+                on[newly] = 0.0
+                ens.closure_mask(0, on)
+        Y = np.stack([ens.get_member(0, k) for k in range(S)], axis=1)
+        eh, ez = l2_errors(gc, Vc, Y, daily_truth[day].cpu().numpy())
+        errs_h.append(eh.tolist())
+        errs_z.append(ez.tolist())
+    done = len(errs_h)
+    return {"h_l2": errs_h, "zeta_l2": errs_z, "max_energy_drift_per_day": drifts, "diverged_on_day": diverged,
+            "gpu_seconds": gpu_ms / 1e3, "gpu_seconds_per_member_day": gpu_ms / 1e3 / (S * max(done, 1)),
+            "fallback_members": int((on == 0).sum()) if mlp is not None else None, "members": S}
+
+
+def pipeline(fine_level=8, coarse_level=6, train_seeds=32, train_days=10, snapshots=2000, eval_seeds=4,
+             eval_days=10, coarse_dt=150.0, window=1800.0, fine_dt=20.0, epochs=3, device=0, out_params=None,
+             log=print):
+    """The whole closure experiment; returns a JSON-able summary. The targets are mean missing
+    tendencies over `window` seconds (window / fine_dt fine steps, window / coarse_dt coarse
+    steps)."""
+    import torch
+    t_start = time.perf_counter()
+    gf, gc = _grid(fine_level), _grid(coarse_level)
+    log(f"meshes: fine {gf.nc} cells, coarse {gc.nc} cells ({time.perf_counter() - t_start:.1f} s)")
+    per_member = max(1, snapshots // max(train_seeds, 1))
+    pair_steps = max(1, int(round(window / fine_dt)))
+    coarse_steps = max(1, int(round(window / coarse_dt)))
+    Y0, Y1, delta, _, fine_train_s = fine_snapshots(gf, gc, list(range(1, train_seeds + 1)), train_days,
+                                                    per_member, dt_fine=fine_dt, pair_steps=pair_steps,
+                                                    device=device)
+    log(f"training snapshots: {Y0.shape[1]} pairs over {delta:.0f} s, fine GPU {fine_train_s:.1f} s")
+    dF, dQ, mc, ens = residual_targets(gc, Y0, Y1, delta, device, coarse_steps=coarse_steps)
+    X, T, norm = build_dataset(gc, Y0, dF, dQ, ens, device)
+    del ens, Y1
+    torch.cuda.empty_cache()
+    log(f"dataset: {X.shape[0]} rows")
+    mlp = ClosureMLP(device=device, seed=0)
+    history, held, zero = train(mlp, X, T, epochs=epochs)
+    skill = output_skill(mlp, X, T)
+    log(f"training loss per epoch {history}, held-out {held:.4f} (without the closure {zero:.4f}), "
+        f"skill (mass flux, momentum) {skill}")
+    if out_params:
+        np.savez(out_params, params=mlp.params(), norm=norm, fine_level=fine_level, coarse_level=coarse_level,
+                 window=window)
+    del X, T
+    torch.cuda.empty_cache()
+    summary = {
+        "fine_level": fine_level, "coarse_level": coarse_level, "train_seeds": train_seeds,
+        "train_days": train_days, "training_pairs": int(Y0.shape[1]), "window_seconds": delta,
+        "coarse_steps_per_window": coarse_steps, "epochs": epochs, "train_loss": history, "heldout_loss": held,
+        "heldout_loss_without_closure": zero, "output_skill": skill, "fine_training_gpu_seconds": fine_train_s,
+    }
+    summary.update(evaluate(gf, gc, mlp, norm, eval_seeds, eval_days, coarse_dt, fine_dt, device, log))
+    summary["wall_seconds"] = time.perf_counter() - t_start
+    return summary
+
+
+def evaluate(gf, gc, mlp, norm, eval_seeds=4, eval_days=10, coarse_dt=150.0, fine_dt=20.0, device=0, log=print):
+    """Coarse runs from the coarse-grained state of held-out seeds against the coarse-grained
+    fine run: plain, closure with the energy-drift fallback, closure without it, and the
+    mass-flux correction alone."""
+    eval_list = list(range(1001, 1001 + eval_seeds))
+    _, _, _, daily, fine_eval_s = fine_snapshots(gf, gc, eval_list, eval_days, 0, dt_fine=fine_dt, device=device,
+                                                 spinup_days=0.0, record_days=True)
+    out = {"eval_seeds": eval_seeds, "eval_days": eval_days, "coarse_dt": coarse_dt, "fine_dt": fine_dt,
+           "fine_gpu_seconds_per_member_day": fine_eval_s / (eval_seeds * eval_days)}
+    init = daily[0]
+    variants = {"plain_coarse": {},
+                "closure_coarse": {"mlp": mlp, "norm": norm},
+                "closure_coarse_no_fallback": {"mlp": mlp, "norm": norm, "drift_per_day": np.inf},
+                "closure_mass_flux_only_no_fallback": {"mlp": mlp, "norm": norm, "drift_per_day": np.inf,
+                                                       "momentum_scale": 0.0}}
+    for name, kw in variants.items():
+        r = run_coarse(gc, init, eval_days, coarse_dt, daily, device=device, **kw)
+        out[name] = r
+        log(f"{name}: h L2 per day {[round(float(np.mean(x)), 2) for x in r['h_l2']]}, vorticity "
+            f"{[float('%.3g' % np.mean(x)) for x in r['zeta_l2']]}, fallback {r['fallback_members']}, "
+            f"diverged on day {r['diverged_on_day']}")
+    return out
+
+
+def main():
+    import argparse
+    p = argparse.ArgumentParser(description=__doc__)
+    p.add_argument("--fine", type=int, default=8)
+    p.add_argument("--coarse", type=int, default=6)
+    p.add_argument("--train-seeds", type=int, default=32)
+    p.add_argument("--train-days", type=float, default=10)
+    p.add_argument("--snapshots", type=int, default=2000)
+    p.add_argument("--eval-seeds", type=int, default=4)
+    p.add_argument("--eval-days", type=int, default=10)
+    p.add_argument("--coarse-dt", type=float, default=150.0)
+    p.add_argument("--fine-dt", type=float, default=20.0)
+    p.add_argument("--window", type=float, default=1800.0)
+    p.add_argument("--epochs", type=int, default=3)
+    p.add_argument("--out", default="closure_summary.json")
+    p.add_argument("--params", default=None, help="where to save the trained network")
+    p.add_argument("--evaluate", default=None, help="skip training: evaluate this saved network (.npz)")
+    p.add_argument("--training-summary", default=None, help="JSON of the training run to merge (with --evaluate)")
+    a = p.parse_args()
+    if a.evaluate:
+        z = np.load(a.evaluate)
+        gf, gc = _grid(int(z["fine_level"])), _grid(int(z["coarse_level"]))
+        s = {}
+        if a.training_summary:
+            with open(a.training_summary) as f:
+                s.update(json.load(f))
+        s.update(evaluate(gf, gc, ClosureMLP(z["params"]), z["norm"], a.eval_seeds, a.eval_days, a.coarse_dt,
+                          a.fine_dt))
+    else:
+        s = pipeline(a.fine, a.coarse, a.train_seeds, a.train_days, a.snapshots, a.eval_seeds, a.eval_days,
+                     a.coarse_dt, a.window, a.fine_dt, a.epochs, out_params=a.params)
+    with open(a.out, "w") as f:
+        json.dump(s, f, indent=1)
+    print(json.dumps({k: v for k, v in s.items() if not isinstance(v, dict)}))
+
+
+if __name__ == "__main__":
+    main()

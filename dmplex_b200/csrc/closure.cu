@@ -495,6 +495,22 @@ void launch_mlp(TriskClosure& c, const __nv_bfloat16* X, int64_t n, const float*
 
 }  // namespace
 
+namespace trisk {
+
+void closure_forward_on(TriskClosure* c, const void* X, int64_t n, float* Y, cudaStream_t stream) {
+  if (n == 0) return;
+  k_mlp<0><<<mlp_grid(*c, n), TILE, SMEM_BYTES, stream>>>(static_cast<const __nv_bfloat16*>(X), n, c->wbf, c->p,
+                                                           nullptr, Y, nullptr, nullptr, 0.0f, c->status);
+  CUDA_CHECK(cudaGetLastError());
+  c->launches++;
+}
+
+void closure_check(TriskClosure* c) { check_status(*c); }
+
+int closure_device(const TriskClosure* c) { return c->device; }
+
+}  // namespace trisk
+
 extern "C" {
 
 int trisk_closure_create(int32_t device, const float* params, TriskClosure** out) {

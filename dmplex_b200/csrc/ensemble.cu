@@ -9,6 +9,8 @@
 #include <cstring>
 #include <memory>
 
+#include <cuda_bf16.h>
+
 #include "model.hpp"
 
 using namespace trisk;
@@ -59,14 +61,14 @@ __global__ void __launch_bounds__(256) kg_vertex(const GroupSet G, int first_sta
 }
 
 template <int PV, int KE>
-__global__ void __launch_bounds__(256) kg_flux(const GroupSet G, int first_stage) {
+__global__ void __launch_bounds__(256) kg_flux(const GroupSet G, int first_stage, int want_K) {
   pdl_trigger();
   for (int vb = blockIdx.x; vb < G.totalF; vb += gridDim.x) {
     const int gi = group_of(G, vb, 1);
     const GroupDesc& D = G.g[gi];
     if (G.counters[gi] >= D.nsteps) continue;
     const double* u = first_stage ? D.y : D.st;
-    flux_body<PV, KE, true>(D.T, D.W, u, u + (size_t)D.T.ne * D.M, D.M, D.nEF, 0, vb - D.startF);
+    flux_body<PV, KE, true>(D.T, D.W, u, u + (size_t)D.T.ne * D.M, D.M, D.nEF, want_K, vb - D.startF);
   }
 }
 
@@ -84,8 +86,88 @@ __global__ void __launch_bounds__(256) kg_tend(const GroupSet G) {
     S.flag = G.flag;
     S.c = EPI == EPI_STAGE3 ? D.dt : D.dt / 2;
     S.sixth = D.dt / 6;
-    tend_body<PV, EPI, true>(D.T, D.W, S, D.M, D.nET, vb - D.startT);
+    if (D.W.dq)
+      tend_body<PV, EPI, true, true>(D.T, D.W, S, D.M, D.nET, vb - D.startT);
+    else
+      tend_body<PV, EPI, true, false>(D.T, D.W, S, D.M, D.nET, vb - D.startT);
   }
+}
+
+// ---- learned closure: features, corrections, energy -------------------------------------
+
+constexpr int NFEAT = 24, NGEOM = 7;
+
+// Feature normalization (x - mean) * scale and the output scales of the two corrections.
+struct FeatureNorm {
+  double mean[NFEAT];
+  double scale[NFEAT];
+  double out_scale[2];
+};
+
+// The network's 24 inputs of (edge, member) rows e * M + m: u_e, u at the 10 TRiSK stencil
+// edges (0 for padded entries), h at the two cells, q at the two vertices, K = B - g h at
+// the two cells, and 7 geometry values of the edge. Output row: row_map ? row_map[e] * M + m
+// (file edge numbering) : the internal row.
+__global__ void kg_features(DevTables T, DevWork W, const double* y, int M, const float* geom,
+                            const FeatureNorm N, __nv_bfloat16* X, const int32_t* row_map, int64_t rows) {
+  const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (r >= rows) return;
+  const int e = (int)(r / M), m = (int)(r - (int64_t)e * M);
+  const double* u = y;
+  const double* h = y + (size_t)T.ne * M;
+  double f[NFEAT];
+  f[0] = u[(size_t)e * M + m];
+#pragma unroll
+  for (int k = 0; k < TWD; ++k) {
+    const int ep = T.trisk_edges[k * T.lde + e];
+    f[1 + k] = T.trisk[k * T.lde + e] != 0.0 ? u[(size_t)ep * M + m] : 0.0;
+  }
+  const int c0 = T.edge_cells[e], c1 = T.edge_cells[T.lde + e];
+  const int v0 = T.edge_vertices[e], v1 = T.edge_vertices[T.lde + e];
+  const double h0 = h[(size_t)c0 * M + m], h1 = h[(size_t)c1 * M + m];
+  f[11] = h0;
+  f[12] = h1;
+  f[13] = W.qv[(size_t)v0 * M + m];
+  f[14] = W.qv[(size_t)v1 * M + m];
+  f[15] = W.B[(size_t)c0 * M + m] - T.gravity * h0;
+  f[16] = W.B[(size_t)c1 * M + m] - T.gravity * h1;
+#pragma unroll
+  for (int k = 0; k < NGEOM; ++k) f[17 + k] = geom[(size_t)e * NGEOM + k];
+  const int64_t out = row_map ? (int64_t)row_map[e] * M + m : r;
+#pragma unroll
+  for (int k = 0; k < NFEAT; ++k) X[out * NFEAT + k] = __float2bfloat16_rn((float)((f[k] - N.mean[k]) * N.scale[k]));
+}
+
+// dF = on[m] sF y0 (mass flux: added to F in the flux-form continuity equation only, so
+// mass stays conserved and the PV flux keeps the resolved F); dq = on[m] sQ y1 (momentum
+// tendency).
+__global__ void kg_closure_apply(double* dF, double* dq, const float* Y, const float* member_on, int64_t rows, int M,
+                                 double sF, double sQ) {
+  const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (r >= rows) return;
+  const double on = member_on[r % M];
+  dF[r] = on * sF * (double)Y[2 * r];
+  dq[r] = on * sQ * (double)Y[2 * r + 1];
+}
+
+// energy[m] += sum_i A_i h_i (K_i + g h_i / 2) over this block's cells (TRiSKShallowWater.jl:406-411)
+__global__ void kg_energy(const double* y, const double* K, const double* area, int nc, int ne, int M, double g,
+                          double* energy) {
+  __shared__ double sm[256];
+  const int m = blockIdx.y;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double s = 0.0;
+  if (i < nc) {
+    const double hi = y[(size_t)ne * M + (size_t)i * M + m];
+    s = area[i] * hi * (K[(size_t)i * M + m] + g * hi / 2);
+  }
+  sm[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) sm[threadIdx.x] += sm[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) atomicAdd(&energy[m], sm[0]);
 }
 
 __global__ void kg_advance(int* counters, int n) {
@@ -104,6 +186,19 @@ __global__ void kg_gather_member(double* dst, const double* src, const int32_t* 
 
 }  // namespace trisk
 
+// A group's learned closure: network, buffers of its (edge, member) rows and settings.
+struct ClosureSlot {
+  TriskClosure* net = nullptr;
+  __nv_bfloat16* X = nullptr;  // rows x 24 features
+  float* Y = nullptr;          // rows x 2 corrections
+  float* geom = nullptr;       // ne x 7, internal edge order
+  float* member_on = nullptr;  // M flags (1: closure on, 0: plain step)
+  double* dF = nullptr;        // rows: mass-flux correction (continuity equation only)
+  double* dq = nullptr;        // rows: momentum-tendency correction
+  trisk::FeatureNorm norm{};
+  bool every_stage = false;    // false: the network runs at stage 1 and its output is reused
+};
+
 struct TriskEnsemble {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -111,14 +206,18 @@ struct TriskEnsemble {
   int block = 128;
   int grid[3] = {0, 0, 0};
   GroupSet G{};
+  ClosureSlot cl[trisk::MAX_GROUPS];
+  double* energy = nullptr;  // per-member energies of the diagnostic
   std::vector<TriskModel*> models;
   std::vector<void*> allocations;
   int* counters = nullptr;
   int* flag = nullptr;
   double* staging = nullptr;
   int64_t max_state = 0;
+  int max_members = 0;
   cudaGraphExec_t graph = nullptr;
   int64_t launches = 0;
+  int64_t graph_kernels = 0;
   double step_bytes = 0;
 
   ~TriskEnsemble() {
@@ -182,12 +281,45 @@ void elaunch(TriskEnsemble& e, void (*kernel)(KArgs...), int grid, bool pdl, Arg
 // One RK4 step of every unfinished group. The first phase of a step and the counter update
 // wait for the full completion of the launch before them (no PDL): both depend on, or
 // change, the step counters the others read.
+// The closure of every group that has one, after the flux phase of `stage`: features and
+// the network (at stage 1, or at every stage), then the corrections of F and du.
+void enqueue_closure(TriskEnsemble& e, int stage) {
+  for (int g = 0; g < e.G.n; ++g) {
+    ClosureSlot& c = e.cl[g];
+    if (!c.net) continue;
+    const GroupDesc& D = e.G.g[g];
+    const int64_t rows = (int64_t)D.T.ne * D.M;
+    const unsigned nb = (unsigned)cdiv(rows, 256);
+    if (stage == 1 || c.every_stage) {
+      kg_features<<<nb, 256, 0, e.stream>>>(D.T, D.W, stage == 1 ? D.y : D.st, D.M, c.geom, c.norm, c.X, nullptr,
+                                            rows);
+      CUDA_CHECK(cudaGetLastError());
+      closure_forward_on(c.net, c.X, rows, c.Y, e.stream);
+      e.launches += 2;
+    }
+    if (stage == 1 || c.every_stage) {
+      kg_closure_apply<<<nb, 256, 0, e.stream>>>(c.dF, c.dq, c.Y, c.member_on, rows, D.M, c.norm.out_scale[0],
+                                                 c.norm.out_scale[1]);
+      CUDA_CHECK(cudaGetLastError());
+      e.launches++;
+    }
+  }
+}
+
+bool any_closure(const TriskEnsemble& e) {
+  for (int g = 0; g < e.G.n; ++g)
+    if (e.cl[g].net) return true;
+  return false;
+}
+
 void enqueue_ensemble_step(TriskEnsemble& e) {
+  const bool closure = any_closure(e);
   with_modes_e(e.pv, e.ke, [&](auto pvc, auto kec) {
     constexpr int PV = decltype(pvc)::value, KE = decltype(kec)::value;
     for (int stage = 1; stage <= 4; ++stage) {
       elaunch(e, kg_vertex<PV, KE>, e.grid[0], stage != 1, e.G, stage == 1 ? 1 : 0);
-      elaunch(e, kg_flux<PV, KE>, e.grid[1], true, e.G, stage == 1 ? 1 : 0);
+      elaunch(e, kg_flux<PV, KE>, e.grid[1], true, e.G, stage == 1 ? 1 : 0, 0);
+      if (closure) enqueue_closure(e, stage);
       switch (stage) {
         case 1: elaunch(e, kg_tend<PV, EPI_STAGE1>, e.grid[2], true, e.G); break;
         case 2: elaunch(e, kg_tend<PV, EPI_STAGE2>, e.grid[2], true, e.G); break;
@@ -215,10 +347,18 @@ void ensure_ensemble_graph(TriskEnsemble& e) {
     throw;
   }
   CUDA_CHECK(cudaStreamEndCapture(e.stream, &g));
+  e.graph_kernels = e.launches - before;  // counted again at every replay
   e.launches = before;
   cudaError_t err = cudaGraphInstantiate(&e.graph, g, 0);
   cudaGraphDestroy(g);
   CUDA_CHECK(err);
+}
+
+void drop_graph(TriskEnsemble& e) {
+  if (e.graph) {
+    cudaGraphExecDestroy(e.graph);
+    e.graph = nullptr;
+  }
 }
 
 TriskEnsemble* checked_e(TriskEnsemble* e) {
@@ -291,6 +431,7 @@ int trisk_ensemble_create(TriskModel* const* models, const int32_t* members, con
     sT += D.nET + D.nCT;
     e->models.push_back(m);
     e->max_state = std::max(e->max_state, m->N);
+    e->max_members = std::max(e->max_members, (int)M);
     const double Nb = 8.0 * (double)m->N * M;
     e->step_bytes += 4 * (m->table_bytes_unique + 2 * Nb) + 15 * Nb;
   }
@@ -366,7 +507,7 @@ int trisk_ensemble_run_async(TriskEnsemble* ens, int64_t steps) {
   ensure_ensemble_graph(e);
   for (int64_t s = 0; s < steps; ++s) {
     CUDA_CHECK(cudaGraphLaunch(e.graph, e.stream));
-    e.launches += 13;
+    e.launches += e.graph_kernels;
   }
   TRISK_API_END
 }
@@ -421,6 +562,152 @@ int trisk_ensemble_bytes(TriskEnsemble* ens, double* step_bytes) {
   TriskEnsemble& e = *checked_e(ens);
   if (!step_bytes) throw Error(TRISK_ERR_ARGUMENT, "NULL argument");
   *step_bytes = e.step_bytes;
+  TRISK_API_END
+}
+
+int trisk_ensemble_set_closure(TriskEnsemble* ens, int32_t group, TriskClosure* net, const float* geometry,
+                               const double* norm, int32_t every_stage) {
+  TRISK_API_BEGIN
+  TriskEnsemble& e = *checked_e(ens);
+  if (group < 0 || group >= e.G.n) throw Error(TRISK_ERR_ARGUMENT, "group out of range");
+  DeviceGuard guard(e.device);
+  GroupDesc& D = e.G.g[group];
+  ClosureSlot& c = e.cl[group];
+  drop_graph(e);
+  if (!net) {  // back to the plain step
+    c.net = nullptr;
+    D.W.dq = D.W.dF = nullptr;
+    return TRISK_OK;
+  }
+  TriskModel& m = *e.models[group];
+  if (m.pv != PVM_TRISK) throw Error(TRISK_ERR_UNSUPPORTED, "the closure's features need the TRiSK PV flux");
+  if (closure_device(net) != e.device) throw Error(TRISK_ERR_ARGUMENT, "closure on another device");
+  if (!geometry || !norm) throw Error(TRISK_ERR_ARGUMENT, "NULL argument");
+  const int64_t rows = m.ne * (int64_t)D.M;
+  if (!c.X) {
+    c.X = e.alloc<__nv_bfloat16>(rows * NFEAT);
+    c.Y = e.alloc<float>(rows * 2);
+    c.geom = e.alloc<float>(m.ne * NGEOM);
+    c.member_on = e.alloc<float>(D.M);
+    c.dF = e.alloc<double>(rows);
+    c.dq = e.alloc<double>(rows);
+    std::vector<float> on(D.M, 1.0f);
+    CUDA_CHECK(cudaMemcpy(c.member_on, on.data(), D.M * sizeof(float), cudaMemcpyHostToDevice));
+    CUDA_CHECK(cudaMemset(c.Y, 0, rows * 2 * sizeof(float)));
+    CUDA_CHECK(cudaMemset(c.dF, 0, rows * sizeof(double)));
+    CUDA_CHECK(cudaMemset(c.dq, 0, rows * sizeof(double)));
+  }
+  D.W.dq = c.dq;
+  D.W.dF = c.dF;
+  std::vector<float> g((size_t)m.ne * NGEOM);
+  for (int64_t j = 0; j < m.ne; ++j)  // internal edge j = file edge edge_n2o[j]
+    for (int k = 0; k < NGEOM; ++k) g[j * NGEOM + k] = geometry[(size_t)m.edge_n2o[j] * NGEOM + k];
+  CUDA_CHECK(cudaMemcpy(c.geom, g.data(), g.size() * sizeof(float), cudaMemcpyHostToDevice));
+  for (int k = 0; k < NFEAT; ++k) {
+    c.norm.mean[k] = norm[k];
+    c.norm.scale[k] = norm[NFEAT + k];
+  }
+  c.norm.out_scale[0] = norm[2 * NFEAT];
+  c.norm.out_scale[1] = norm[2 * NFEAT + 1];
+  c.every_stage = every_stage != 0;
+  c.net = net;
+  TRISK_API_END
+}
+
+int trisk_ensemble_closure_mask(TriskEnsemble* ens, int32_t group, const float* member_on) {
+  TRISK_API_BEGIN
+  TriskEnsemble& e = *checked_e(ens);
+  if (group < 0 || group >= e.G.n || !member_on) throw Error(TRISK_ERR_ARGUMENT, "bad argument");
+  ClosureSlot& c = e.cl[group];
+  if (!c.net) throw Error(TRISK_ERR_ARGUMENT, "the group has no closure");
+  DeviceGuard guard(e.device);
+  CUDA_CHECK(cudaMemcpyAsync(c.member_on, member_on, e.G.g[group].M * sizeof(float), cudaMemcpyHostToDevice,
+                             e.stream));
+  CUDA_CHECK(cudaStreamSynchronize(e.stream));
+  TRISK_API_END
+}
+
+// The closure features of the group's current member states (file edge order, rows
+// e * M + m) into the device array X (rows x 24 BF16), normalized with `norm`.
+int trisk_ensemble_features(TriskEnsemble* ens, int32_t group, void* X, const double* norm,
+                            const float* geometry) {
+  TRISK_API_BEGIN
+  TriskEnsemble& e = *checked_e(ens);
+  if (group < 0 || group >= e.G.n || !X || !norm || !geometry) throw Error(TRISK_ERR_ARGUMENT, "bad argument");
+  TriskModel& m = *e.models[group];
+  if (m.pv != PVM_TRISK) throw Error(TRISK_ERR_UNSUPPORTED, "the closure's features need the TRiSK PV flux");
+  DeviceGuard guard(e.device);
+  const GroupDesc& D = e.G.g[group];
+  const int M = D.M;
+  FeatureNorm N{};
+  for (int k = 0; k < NFEAT; ++k) {
+    N.mean[k] = norm[k];
+    N.scale[k] = norm[NFEAT + k];
+  }
+  std::vector<float> g((size_t)m.ne * NGEOM);
+  for (int64_t j = 0; j < m.ne; ++j)
+    for (int k = 0; k < NGEOM; ++k) g[j * NGEOM + k] = geometry[(size_t)m.edge_n2o[j] * NGEOM + k];
+  float* geom = nullptr;
+  int32_t* map = nullptr;
+  CUDA_CHECK(cudaMallocAsync((void**)&geom, g.size() * sizeof(float), e.stream));
+  CUDA_CHECK(cudaMallocAsync((void**)&map, m.ne * sizeof(int32_t), e.stream));
+  CUDA_CHECK(cudaMemcpyAsync(geom, g.data(), g.size() * sizeof(float), cudaMemcpyHostToDevice, e.stream));
+  CUDA_CHECK(cudaMemcpyAsync(map, m.edge_n2o.data(), m.ne * sizeof(int32_t), cudaMemcpyHostToDevice, e.stream));
+  const int B = 128;
+  with_modes_e(e.pv, e.ke, [&](auto pvc, auto kec) {
+    constexpr int PV = decltype(pvc)::value, KE = decltype(kec)::value;
+    const double* u = D.y;
+    const double* h = D.y + (size_t)m.ne * M;
+    k_vertex<PV, KE, true><<<(unsigned)cdiv(m.nv * M, B), B, 0, e.stream>>>(D.T, D.W, u, h, M, 0);
+    const int nbE = (int)cdiv(m.ne * M, B);
+    k_flux<PV, KE, true><<<(unsigned)(nbE + cdiv(m.nc * M, B)), B, 0, e.stream>>>(D.T, D.W, u, h, M, nbE, 1);
+  });
+  const int64_t rows = m.ne * (int64_t)M;
+  kg_features<<<(unsigned)cdiv(rows, 256), 256, 0, e.stream>>>(D.T, D.W, D.y, M, geom, N,
+                                                                static_cast<__nv_bfloat16*>(X), map, rows);
+  CUDA_CHECK(cudaGetLastError());
+  CUDA_CHECK(cudaFreeAsync(geom, e.stream));
+  CUDA_CHECK(cudaFreeAsync(map, e.stream));
+  CUDA_CHECK(cudaStreamSynchronize(e.stream));
+  e.launches += 3;
+  TRISK_API_END
+}
+
+// Total energy sum_i A_i h_i (K_i + g h_i / 2) of every member of the group (host, M values).
+int trisk_ensemble_energy(TriskEnsemble* ens, int32_t group, double* energies) {
+  TRISK_API_BEGIN
+  TriskEnsemble& e = *checked_e(ens);
+  if (group < 0 || group >= e.G.n || !energies) throw Error(TRISK_ERR_ARGUMENT, "bad argument");
+  TriskModel& m = *e.models[group];
+  DeviceGuard guard(e.device);
+  const GroupDesc& D = e.G.g[group];
+  const int M = D.M;
+  if (!e.energy) e.energy = e.alloc<double>(e.max_members);
+  CUDA_CHECK(cudaMemsetAsync(e.energy, 0, M * sizeof(double), e.stream));
+  const int B = 128;
+  with_modes_e(e.pv, e.ke, [&](auto pvc, auto kec) {
+    constexpr int PV = decltype(pvc)::value, KE = decltype(kec)::value;
+    const double* u = D.y;
+    const double* h = D.y + (size_t)m.ne * M;
+    k_vertex<PV, KE, true><<<(unsigned)cdiv(m.nv * M, B), B, 0, e.stream>>>(D.T, D.W, u, h, M, 0);
+    const int nbE = (int)cdiv(m.ne * M, B);
+    k_flux<PV, KE, true><<<(unsigned)(nbE + cdiv(m.nc * M, B)), B, 0, e.stream>>>(D.T, D.W, u, h, M, nbE, 1);
+  });
+  kg_energy<<<dim3((unsigned)cdiv(m.nc, 256), (unsigned)M), 256, 0, e.stream>>>(D.y, D.W.K, m.area_c, (int)m.nc,
+                                                                                (int)m.ne, M, m.gravity, e.energy);
+  CUDA_CHECK(cudaGetLastError());
+  CUDA_CHECK(cudaMemcpyAsync(energies, e.energy, M * sizeof(double), cudaMemcpyDeviceToHost, e.stream));
+  CUDA_CHECK(cudaStreamSynchronize(e.stream));
+  e.launches += 3;
+  TRISK_API_END
+}
+
+int trisk_ensemble_closure_check(TriskEnsemble* ens) {
+  TRISK_API_BEGIN
+  TriskEnsemble& e = *checked_e(ens);
+  DeviceGuard guard(e.device);
+  for (int g = 0; g < e.G.n; ++g)
+    if (e.cl[g].net) closure_check(e.cl[g].net);
   TRISK_API_END
 }
 

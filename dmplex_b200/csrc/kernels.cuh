@@ -79,9 +79,13 @@ struct DevTables {
   const double* vk_weights;      // VW x ldv (alpha != 1)
 };
 
-// Work vectors of one member group, [entity][member].
+// Work vectors of one member group, [entity][member]. dq, dF: the closure's momentum-
+// tendency and mass-flux corrections per edge (only read by the closure variant of the
+// tendency phase).
 struct DevWork {
   double *K, *B, *F, *qe, *zv, *hv, *qv, *Kv;
+  double* dq = nullptr;
+  double* dF = nullptr;
 };
 
 // State pointers of one stage. y = [u (ne x M); h (nc x M)].
@@ -296,7 +300,7 @@ __device__ __forceinline__ void epilogue(const DevStage& S, size_t j, double kv)
   }
 }
 
-template <int PV, int EPI, bool ENS>
+template <int PV, int EPI, bool ENS, bool CL = false>
 __device__ __forceinline__ void tend_body(const DevTables& T, const DevWork& W, const DevStage& S, int M, int nbE,
                                           int vb) {
   if (vb < nbE) {
@@ -361,6 +365,7 @@ __device__ __forceinline__ void tend_body(const DevTables& T, const DevWork& W, 
       for (int k = 0; k < GW; ++k) s += gw[k] * f[k] * q[k];
       du = s - (W.B[(size_t)ec1 * M + mm] - W.B[(size_t)ec0 * M + mm]) * invd;
     }
+    if (CL) du += W.dq[o];  // learned momentum correction
     epilogue<EPI>(S, o, du);
   } else {
     int i, mm;
@@ -376,7 +381,10 @@ __device__ __forceinline__ void tend_body(const DevTables& T, const DevWork& W, 
     pdl_wait();
     double f[CW];
 #pragma unroll
-    for (int k = 0; k < CW; ++k) f[k] = W.F[(size_t)ce[k] * M + mm];
+    for (int k = 0; k < CW; ++k) {
+      f[k] = W.F[(size_t)ce[k] * M + mm];
+      if (CL) f[k] += W.dF[(size_t)ce[k] * M + mm];  // learned mass-flux correction
+    }
     double s = 0.0;
 #pragma unroll
     for (int k = 0; k < CW; ++k) s += dv[k] * f[k];

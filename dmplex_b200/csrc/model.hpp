@@ -43,6 +43,15 @@ void launch_gather(cudaStream_t stream, double* dst, const double* src, const in
 
 }  // namespace trisk
 
+struct TriskClosure;
+namespace trisk {
+// The closure network's forward pass Y = MLP(X) enqueued on `stream` (no wait).
+void closure_forward_on(TriskClosure* c, const void* X, int64_t n, float* Y, cudaStream_t stream);
+// Throws TRISK_ERR_TIMEOUT if a bounded tensor-core wait of the network gave up.
+void closure_check(TriskClosure* c);
+int closure_device(const TriskClosure* c);
+}  // namespace trisk
+
 // 1-based copies of the index tables handed out through TriskCoefficients views.
 struct CoefficientExport {
   std::vector<int64_t> t[9];

@@ -76,3 +76,36 @@ class Ensemble:
         b = C.c_double()
         check(lib.trisk_ensemble_bytes(self._h, C.byref(b)))
         return b.value
+
+    def energy(self, group: int) -> np.ndarray:
+        """total_energy of every member of the group."""
+        out = np.zeros(self.groups[group][1])
+        check(lib.trisk_ensemble_energy(self._h, group, out.ctypes.data))
+        return out
+
+    def set_closure(self, group: int, net, geometry: np.ndarray, norm: np.ndarray, every_stage: bool = False):
+        """Learned closure for a group (net: closure.ClosureMLP, or None to remove it)."""
+        if net is None:
+            check(lib.trisk_ensemble_set_closure(self._h, group, None, None, None, 0))
+            self._net = None
+            return
+        geometry = np.ascontiguousarray(geometry, dtype=np.float32)
+        norm = np.ascontiguousarray(norm, dtype=np.float64)
+        check(lib.trisk_ensemble_set_closure(self._h, group, net.handle, geometry.ctypes.data, norm.ctypes.data,
+                                             int(every_stage)))
+        self._net = net  # the ensemble launches it
+
+    def closure_mask(self, group: int, member_on) -> None:
+        on = np.ascontiguousarray(member_on, dtype=np.float32)
+        check(lib.trisk_ensemble_closure_mask(self._h, group, on.ctypes.data))
+
+    def features(self, group: int, X, norm: np.ndarray, geometry: np.ndarray):
+        """Closure features of the group's member states into the CUDA bfloat16 tensor X
+        (rows e * M + m in file edge order, 24 columns)."""
+        norm = np.ascontiguousarray(norm, dtype=np.float64)
+        geometry = np.ascontiguousarray(geometry, dtype=np.float32)
+        check(lib.trisk_ensemble_features(self._h, group, X.data_ptr(), norm.ctypes.data, geometry.ctypes.data))
+        return X
+
+    def closure_check(self) -> None:
+        check(lib.trisk_ensemble_closure_check(self._h))

@@ -159,6 +159,7 @@ typedef struct {
 
 typedef struct TriskModel TriskModel;
 typedef struct TriskTables TriskTables;
+typedef struct TriskClosure TriskClosure; /* the closure network, declared below */
 
 /* Host-only restatement of the constructor's table arithmetic (TRiSKShallowWater.jl:103-158
  * with gassmann_coefficients and vertex_edge_areas): the premultiplied tables of a model,
@@ -235,6 +236,29 @@ int trisk_ensemble_stream(TriskEnsemble* ensemble, void** stream);
 int64_t trisk_ensemble_launch_count(TriskEnsemble* ensemble);
 /* Algorithmic bytes of one RK4 step of all groups: sum 4 (T + 2 M N) + 15 M N. */
 int trisk_ensemble_bytes(TriskEnsemble* ensemble, double* step_bytes);
+/* Per-member total energy sum_i A_i h_i (K_i + g h_i / 2) of a group (M values, host),
+ * as total_energy (TRiSKShallowWater.jl:406-411) of every member. */
+int trisk_ensemble_energy(TriskEnsemble* ensemble, int32_t group, double* energies);
+
+/* ---- learned closure inside an ensemble (no reference counterpart) ---------------------
+ * With a closure, the network runs on all (edge, member) rows of the group's members (at
+ * stage 1 of each RK4 step, its output reused by the other stages, or at every stage), and
+ * every tendency adds, for members whose mask entry is 1, dF_e = sF y0 to the mass flux of
+ * the continuity equation only (dh_i/dt = -sum_k div[i,k] (F + dF); flux form, so mass is
+ * conserved; the PV flux keeps the resolved F) and du_e += sQ y1 to the momentum tendency. Features per row: u_e, u
+ * at the 10 TRiSK stencil edges, h at the two cells, q at the two vertices, K at the two
+ * cells, 7 geometry values (`geometry`, ne x 7 in file edge order); normalized as
+ * (x - mean) * scale with norm = [24 means, 24 scales, sF, sQ]. TRiSK PV flux only.
+ * net = NULL removes the group's closure. */
+int trisk_ensemble_set_closure(TriskEnsemble* ensemble, int32_t group, TriskClosure* net, const float* geometry,
+                               const double* norm, int32_t every_stage);
+int trisk_ensemble_closure_mask(TriskEnsemble* ensemble, int32_t group, const float* member_on);
+/* The features of the group's current member states into X (device, rows e * M + m in file
+ * edge order, 24 BF16 each), for training data. */
+int trisk_ensemble_features(TriskEnsemble* ensemble, int32_t group, void* X, const double* norm,
+                            const float* geometry);
+/* TRISK_ERR_TIMEOUT if a bounded tensor-core wait of a closure network gave up. */
+int trisk_ensemble_closure_check(TriskEnsemble* ensemble);
 
 /* ---- learned flux closure: the network ------------------------------------------------
  * No counterpart in the reference. An edge-local MLP 24 -> 64 -> 64 -> 2 (GELU) whose two
@@ -243,7 +267,6 @@ int trisk_ensemble_bytes(TriskEnsemble* ensemble, double* step_bytes);
  * 24), b1, W2 (64 x 64), b2, W3 (2 x 64), b3, row-major. Device arrays: X (n x 24, BF16),
  * targets and outputs (n x 2, FP32). A bounded wait on the tensor core that gives up
  * returns TRISK_ERR_TIMEOUT. */
-typedef struct TriskClosure TriskClosure;
 int trisk_closure_create(int32_t device, const float* params, TriskClosure** out); /* params: host, or NULL */
 void trisk_closure_destroy(TriskClosure* closure);
 int32_t trisk_closure_param_count(void);
