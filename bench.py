@@ -48,6 +48,8 @@ def parse():
     p.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble leg")
     p.add_argument("--no-closure", action="store_true", help="skip the learned-closure leg")
     p.add_argument("--level", type=int, default=LEVEL, help="mesh level (7 is the benchmark workload)")
+    p.add_argument("--block", default=None,
+                   help="fixed block sizes of the three phases, e.g. 128,128,64 (skips the autotuner)")
     args = p.parse_args()
     return args
 
@@ -346,8 +348,12 @@ def run_b200(args, rank, world, local_rank):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    # block shapes from the autotuner, then warm-up (also captures the CUDA graph)
-    tuned_ms = m.autotune(yd, DT, 20)
+    # block shapes from the autotuner (or given), then warm-up (also captures the CUDA graph)
+    if args.block:
+        m.set_block([int(b) for b in args.block.split(",")])
+        tuned_ms = None
+    else:
+        tuned_ms = m.autotune(yd, DT, 20)
     m.rk4_async(yd, DT, max(args.warmup, 3))
     m.synchronize()
     barrier()

@@ -145,6 +145,9 @@ def _load():
         "trisk_ensemble_features": (C.c_int, [_p, _i32, _p, _p, _p]),
         "trisk_ensemble_closure_check": (C.c_int, [_p]),
         "trisk_autotune": (C.c_int, [_p, _p, _f64, _i32, C.POINTER(_f64)]),
+        "trisk_model_set_block": (C.c_int, [_p, _p]),
+        "trisk_model_set_l2_residency": (C.c_int, [_p, _i64, _i32]),
+        "trisk_l2_info": (C.c_int, [_i32, _p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

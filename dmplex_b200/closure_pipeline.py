@@ -2,9 +2,11 @@
 
 1. Fine runs. Plain TRiSK runs on a fine hexagon mesh (a batched ensemble, one member per
    seed) are coarse-grained (coarsen.CoarseGrainer) to the coarse mesh at snapshot times t
-   and t + delta.
-2. Targets. One coarse RK4 step of length delta from the coarse-grained state at t gives
-   Y_hat; the missing tendency r = (Y_c(t + delta) - Y_hat) / delta splits into
+   (with their tendencies, or also at t + delta).
+2. Targets. The coarse model's missing tendency at the coarse-grained state, r =
+   C(f_fine(y)) - f_coarse(C(y)) (C: the linear coarse-graining; the default), or, over a
+   window, r = (Y_c(t + delta) - Y_hat) / delta with Y_hat the coarse run over delta from
+   Y_c(t). It splits into
      - the momentum correction dQ_e = r_u (edges), and
      - a mass-flux correction dF with -D dF = r_h (D: the coarse divergence), the minimum-
        norm solution dF = D^T psi, (D D^T) psi = -r_h, by batched conjugate gradients. The
@@ -47,11 +49,14 @@ def _torch_sparse(m, device):
 
 
 def fine_snapshots(gf, gc, seeds, days, snapshots_per_member, dt_fine=20.0, pair_steps=8, spinup_days=0.25,
-                   device=0, record_days=False):
+                   device=0, record_days=False, tendency_targets=False):
     """Coarse-grained pairs (Y0 at t, Y1 at t + pair_steps dt_fine) of fine runs, as CUDA
-    float64 tensors (state x snapshots); with record_days also the coarse state at every
-    whole day (days + 1 states per seed). Returns (Y0, Y1, delta, daily, seconds)."""
+    float64 tensors (state x snapshots); with tendency_targets, Y1 is instead the coarse-
+    grained fine tendency at t (the coarse-graining is linear, so this is the tendency of
+    the coarse-grained fine state) and delta is 0. With record_days also the coarse state at
+    every whole day (days + 1 states per seed). Returns (Y0, Y1, delta, daily, seconds)."""
     import torch
+    from .model import tendency
     si = w.si_parameters()
     mf = TRiSKShallowWater(gf, pv_flux=PV, kinetic_energy=KE, device=device, **si)
     total = int(round(days * 86400 / dt_fine))
@@ -67,6 +72,16 @@ def fine_snapshots(gf, gc, seeds, days, snapshots_per_member, dt_fine=20.0, pair
         for k in range(len(seeds)):
             ens.get_member(0, k, col)
             buf[:, k] = col
+        torch.cuda.synchronize()
+        return cg.torch_apply(buf)
+
+    dcol = torch.empty_like(col)
+
+    def coarse_tendency_now():
+        for k in range(len(seeds)):
+            ens.get_member(0, k, col)
+            tendency(dcol, col, mf)
+            buf[:, k] = dcol
         torch.cuda.synchronize()
         return cg.torch_apply(buf)
 
@@ -87,7 +102,10 @@ def fine_snapshots(gf, gc, seeds, days, snapshots_per_member, dt_fine=20.0, pair
         ens.run(stop - step)
         seconds += time.perf_counter() - t0
         step = stop
-        if step in marks:
+        if step in marks and tendency_targets:
+            Y0.append(coarse_now())
+            Y1.append(coarse_tendency_now())
+        elif step in marks:
             Y0.append(coarse_now())
             t0 = time.perf_counter()
             ens.run(pair_steps)
@@ -97,7 +115,7 @@ def fine_snapshots(gf, gc, seeds, days, snapshots_per_member, dt_fine=20.0, pair
         if record_days and step % day_steps == 0:
             daily.append(coarse_now())
     cat = (lambda a: torch.cat(a, dim=1)) if Y0 else (lambda a: None)
-    return cat(Y0), cat(Y1), pair_steps * dt_fine, daily, seconds
+    return cat(Y0), cat(Y1), 0.0 if tendency_targets else pair_steps * dt_fine, daily, seconds
 
 
 def cg_solve(DDt, rhs, null, iters=500, rtol=1e-9):
@@ -124,27 +142,40 @@ def cg_solve(DDt, rhs, null, iters=500, rtol=1e-9):
 
 
 def residual_targets(gc, Y0, Y1, delta, device=0, coarse_steps=1):
-    """(dF, dQ): edges x snapshots (CUDA float64). The coarse model covers delta in
-    `coarse_steps` RK4 steps; the residual is the mean missing tendency over the window."""
+    """(dF, dQ): edges x snapshots (CUDA float64). delta > 0: the coarse model covers delta
+    in `coarse_steps` RK4 steps from Y0 and the residual is the mean missing tendency over
+    the window, (Y1 - Y_coarse(delta)) / delta. delta = 0: Y1 holds the coarse-grained fine
+    tendency at Y0 and the residual is Y1 - f_coarse(Y0), the coarse model's missing
+    tendency at the same state."""
     import torch
+    from .model import tendency
     si = w.si_parameters()
     mc = TRiSKShallowWater(gc, pv_flux=PV, kinetic_energy=KE, device=device, **si)
     S = Y0.shape[1]
-    ens = Ensemble([(mc, S, delta / coarse_steps, coarse_steps)])
+    ens = Ensemble([(mc, S, max(delta, 1.0) / coarse_steps, coarse_steps)])
     col = torch.empty(mc.state_size, dtype=torch.float64, device=Y0.device)
-    for k in range(S):
-        col.copy_(Y0[:, k])
-        ens.set_member(0, k, col)
-    ens.run(coarse_steps)
-    ens.reset()
-    Yh = torch.empty_like(Y0)
-    for k in range(S):
-        ens.get_member(0, k, col)
-        Yh[:, k] = col
+    if delta > 0:
+        for k in range(S):
+            col.copy_(Y0[:, k])
+            ens.set_member(0, k, col)
+        ens.run(coarse_steps)
+        ens.reset()
+        Yh = torch.empty_like(Y0)
+        for k in range(S):
+            ens.get_member(0, k, col)
+            Yh[:, k] = col
+        r = (Y1 - Yh) / delta
+    else:
+        r = torch.empty_like(Y0)
+        dcol = torch.empty_like(col)
+        for k in range(S):
+            col.copy_(Y0[:, k])
+            tendency(dcol, col, mc)
+            r[:, k] = Y1[:, k] - dcol
+        torch.cuda.synchronize()
     for k in range(S):  # the features are those of the state at t
         col.copy_(Y0[:, k])
         ens.set_member(0, k, col)
-    r = (Y1 - Yh) / delta
     ne = gc.ne
     coeffs = model_tables(gc, pv_flux=PV, kinetic_energy=KE, **si)
     D = _torch_sparse(divergence_matrix(coeffs), Y0.device)
@@ -299,11 +330,14 @@ def run_coarse(gc, Y_init, days, dt, daily_truth, mlp=None, norm=None, drift_per
 
 def pipeline(fine_level=8, coarse_level=6, train_seeds=32, train_days=10, snapshots=2000, eval_seeds=4,
              eval_days=10, coarse_dt=150.0, window=1800.0, fine_dt=20.0, epochs=3, device=0, out_params=None,
-             log=print):
-    """The whole closure experiment; returns a JSON-able summary. The targets are mean missing
-    tendencies over `window` seconds (window / fine_dt fine steps, window / coarse_dt coarse
-    steps)."""
+             target="tendency", log=print):
+    """The whole closure experiment; returns a JSON-able summary. target "tendency": the
+    residual is the coarse model's missing tendency at the coarse-grained state; "window":
+    the mean missing tendency over `window` seconds (window / fine_dt fine steps, window /
+    coarse_dt coarse steps)."""
     import torch
+    if target not in ("tendency", "window"):
+        raise ValueError("target must be 'tendency' or 'window'")
     t_start = time.perf_counter()
     gf, gc = _grid(fine_level), _grid(coarse_level)
     log(f"meshes: fine {gf.nc} cells, coarse {gc.nc} cells ({time.perf_counter() - t_start:.1f} s)")
@@ -312,8 +346,8 @@ def pipeline(fine_level=8, coarse_level=6, train_seeds=32, train_days=10, snapsh
     coarse_steps = max(1, int(round(window / coarse_dt)))
     Y0, Y1, delta, _, fine_train_s = fine_snapshots(gf, gc, list(range(1, train_seeds + 1)), train_days,
                                                     per_member, dt_fine=fine_dt, pair_steps=pair_steps,
-                                                    device=device)
-    log(f"training snapshots: {Y0.shape[1]} pairs over {delta:.0f} s, fine GPU {fine_train_s:.1f} s")
+                                                    device=device, tendency_targets=target == "tendency")
+    log(f"training snapshots: {Y0.shape[1]} ({target} targets), fine GPU {fine_train_s:.1f} s")
     dF, dQ, mc, ens = residual_targets(gc, Y0, Y1, delta, device, coarse_steps=coarse_steps)
     X, T, norm = build_dataset(gc, Y0, dF, dQ, ens, device)
     del ens, Y1
@@ -326,13 +360,14 @@ def pipeline(fine_level=8, coarse_level=6, train_seeds=32, train_days=10, snapsh
         f"skill (mass flux, momentum) {skill}")
     if out_params:
         np.savez(out_params, params=mlp.params(), norm=norm, fine_level=fine_level, coarse_level=coarse_level,
-                 window=window)
+                 window=window if target == "window" else 0.0, target=target)
     del X, T
     torch.cuda.empty_cache()
     summary = {
         "fine_level": fine_level, "coarse_level": coarse_level, "train_seeds": train_seeds,
-        "train_days": train_days, "training_pairs": int(Y0.shape[1]), "window_seconds": delta,
-        "coarse_steps_per_window": coarse_steps, "epochs": epochs, "train_loss": history, "heldout_loss": held,
+        "train_days": train_days, "training_snapshots": int(Y0.shape[1]), "target": target,
+        "window_seconds": delta if target == "window" else None,
+        "coarse_steps_per_window": coarse_steps if target == "window" else None, "epochs": epochs, "train_loss": history, "heldout_loss": held,
         "heldout_loss_without_closure": zero, "output_skill": skill, "fine_training_gpu_seconds": fine_train_s,
     }
     summary.update(evaluate(gf, gc, mlp, norm, eval_seeds, eval_days, coarse_dt, fine_dt, device, log))
@@ -353,6 +388,8 @@ def evaluate(gf, gc, mlp, norm, eval_seeds=4, eval_days=10, coarse_dt=150.0, fin
     variants = {"plain_coarse": {},
                 "closure_coarse": {"mlp": mlp, "norm": norm},
                 "closure_coarse_no_fallback": {"mlp": mlp, "norm": norm, "drift_per_day": np.inf},
+                "closure_every_stage_no_fallback": {"mlp": mlp, "norm": norm, "drift_per_day": np.inf,
+                                                    "every_stage": True},
                 "closure_mass_flux_only_no_fallback": {"mlp": mlp, "norm": norm, "drift_per_day": np.inf,
                                                        "momentum_scale": 0.0}}
     for name, kw in variants.items():
@@ -377,6 +414,7 @@ def main():
     p.add_argument("--coarse-dt", type=float, default=150.0)
     p.add_argument("--fine-dt", type=float, default=20.0)
     p.add_argument("--window", type=float, default=1800.0)
+    p.add_argument("--target", default="tendency", choices=["tendency", "window"])
     p.add_argument("--epochs", type=int, default=3)
     p.add_argument("--out", default="closure_summary.json")
     p.add_argument("--params", default=None, help="where to save the trained network")
@@ -394,7 +432,7 @@ def main():
                           a.fine_dt))
     else:
         s = pipeline(a.fine, a.coarse, a.train_seeds, a.train_days, a.snapshots, a.eval_seeds, a.eval_days,
-                     a.coarse_dt, a.window, a.fine_dt, a.epochs, out_params=a.params)
+                     a.coarse_dt, a.window, a.fine_dt, a.epochs, out_params=a.params, target=a.target)
     with open(a.out, "w") as f:
         json.dump(s, f, indent=1)
     print(json.dumps({k: v for k, v in s.items() if not isinstance(v, dict)}))

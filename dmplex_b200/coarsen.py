@@ -8,7 +8,8 @@ counterpart; it produces the closure's training data and its error reference).
      averaged over the 3 generators nearest the coarse edge point; then the curl-free
      correction G phi (G the TRiSK gradient (phi_r - phi_l) / d_e, whose discrete curl is
      zero, so the vorticity is untouched) for which the coarse divergence equals the
-     area-weighted mean of the fine divergence. Interpolation alone leaves a divergence
+     area-weighted mean of the fine divergence (less its area-weighted global mean, which
+     a coarse divergence cannot have; it is zero up to the cells' area mismatch). Interpolation alone leaves a divergence
      made mostly of noise at the scale of the coarse cells; the correction removes it.
 
 The maps are linear: sparse matrices built once, and the symmetric positive semidefinite
@@ -77,8 +78,10 @@ class CoarseGrainer:
         u_f = y_fine[:f.ne]
         u = self.Ru @ u_f
         if divergence_fix:
-            b = c.cell_areas * (self.Rh @ (self.Df @ u_f) - self.Dc @ u)
-            b = b - b.mean()
+            r = self.Rh @ (self.Df @ u_f) - self.Dc @ u
+            r -= (c.cell_areas @ r) / c.cell_areas.sum()  # sum A D u = 0 for every u
+            b = c.cell_areas * r
+            b -= b.mean()
             phi = _cg_numpy(self.K, b)
             u = u - self.G @ phi  # D G (-phi) = -A^-1 K (-phi) = A^-1 b
         return np.concatenate([u, self.Rh @ y_fine[f.ne:]])
@@ -99,7 +102,10 @@ class CoarseGrainer:
         ne = self.fine.ne
         u = T["Ru"] @ Yf[:ne]
         if divergence_fix:
-            b = T["A"][:, None] * (T["Rh"] @ (T["Df"] @ Yf[:ne]) - T["Dc"] @ u)
+            A = T["A"][:, None]
+            r = T["Rh"] @ (T["Df"] @ Yf[:ne]) - T["Dc"] @ u
+            r = r - (A * r).sum(0, keepdim=True) / A.sum()
+            b = A * r
             b = b - b.mean(0, keepdim=True)
             phi = _cg_torch(lambda p: T["K"] @ p, b, iters, rtol)
             u = u - T["G"] @ phi

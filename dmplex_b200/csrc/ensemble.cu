@@ -202,6 +202,7 @@ struct ClosureSlot {
 struct TriskEnsemble {
   int device = 0;
   cudaStream_t stream = nullptr;
+  cudaEvent_t caller_ev = nullptr;  // for order_after_caller
   int pv = 0, ke = 0;
   int block = 128;
   int grid[3] = {0, 0, 0};
@@ -225,6 +226,7 @@ struct TriskEnsemble {
     cudaGetDevice(&prev);
     cudaSetDevice(device);
     if (graph) cudaGraphExecDestroy(graph);
+    if (caller_ev) cudaEventDestroy(caller_ev);
     if (stream) {
       cudaStreamSynchronize(stream);
       cudaStreamDestroy(stream);
@@ -391,6 +393,7 @@ int trisk_ensemble_create(TriskModel* const* models, const int32_t* members, con
   e->ke = m0->ke;
   DeviceGuard guard(e->device);
   CUDA_CHECK(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+  CUDA_CHECK(cudaEventCreateWithFlags(&e->caller_ev, cudaEventDisableTiming));
   int sV = 0, sF = 0, sT = 0;
   const int B = e->block;
   for (int g = 0; g < ngroups; ++g) {
@@ -476,6 +479,8 @@ int trisk_ensemble_set_member(TriskEnsemble* ens, int32_t group, int32_t member,
   if (!is_device_pointer(y)) {
     CUDA_CHECK(cudaMemcpyAsync(e.staging, y, m.N * sizeof(double), cudaMemcpyHostToDevice, e.stream));
     src = e.staging;
+  } else {
+    order_after_caller(e.stream, e.caller_ev);
   }
   kg_scatter_member<<<(unsigned)cdiv(m.N, 256), 256, 0, e.stream>>>(D.y, src, m.state_n2o, m.N, D.M, member);
   CUDA_CHECK(cudaGetLastError());
@@ -492,6 +497,7 @@ int trisk_ensemble_get_member(TriskEnsemble* ens, int32_t group, int32_t member,
   DeviceGuard guard(e.device);
   const bool dev = is_device_pointer(y);
   double* dst = dev ? y : e.staging;
+  if (dev) order_after_caller(e.stream, e.caller_ev);
   kg_gather_member<<<(unsigned)cdiv(m.N, 256), 256, 0, e.stream>>>(dst, D.y, m.state_o2n, m.N, D.M, member);
   CUDA_CHECK(cudaGetLastError());
   if (!dev) CUDA_CHECK(cudaMemcpyAsync(y, e.staging, m.N * sizeof(double), cudaMemcpyDeviceToHost, e.stream));
@@ -663,6 +669,7 @@ int trisk_ensemble_features(TriskEnsemble* ens, int32_t group, void* X, const do
     k_flux<PV, KE, true><<<(unsigned)(nbE + cdiv(m.nc * M, B)), B, 0, e.stream>>>(D.T, D.W, u, h, M, nbE, 1);
   });
   const int64_t rows = m.ne * (int64_t)M;
+  order_after_caller(e.stream, e.caller_ev);  // X may still be read by the caller
   kg_features<<<(unsigned)cdiv(rows, 256), 256, 0, e.stream>>>(D.T, D.W, D.y, M, geom, N,
                                                                 static_cast<__nv_bfloat16*>(X), map, rows);
   CUDA_CHECK(cudaGetLastError());

@@ -54,6 +54,9 @@ struct DevTables {
   int32_t nc, ne, nv;
   int32_t ldc, lde, ldv;  // padded entity counts of the [k][entity] tables
   double gravity;
+  // Table entries below keep_end (a prefix of the one packed table block) are loaded with
+  // an L2 evict-last policy, so they stay in L2 from one launch to the next; nullptr: none.
+  const char* keep_end;
   const int32_t* cell_edges;     // CW x ldc
   const double* divergence;      // CW x ldc
   const double* kinetic;         // CW x ldc (alpha != 0)
@@ -105,8 +108,31 @@ __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;"
 __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 template <typename T>
-__device__ __forceinline__ T ldt(const T* p) {  // streaming (evict-first) table load
+__device__ __forceinline__ T ldt_stream(const T* p) {  // streaming (evict-first) table load
   return __ldcs(p);
+}
+
+__device__ __forceinline__ uint64_t l2_keep_policy() {
+  uint64_t pol;
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+__device__ __forceinline__ double ld_keep(const double* p) {
+  double v;
+  asm("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(l2_keep_policy()));
+  return v;
+}
+__device__ __forceinline__ int32_t ld_keep(const int32_t* p) {
+  int32_t v;
+  asm("ld.global.nc.L2::cache_hint.s32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(l2_keep_policy()));
+  return v;
+}
+
+// Table load: L2-resident prefix (evict-last) or streaming (evict-first).
+template <class V>
+__device__ __forceinline__ V ldt(const DevTables& T, const V* p) {
+  if (reinterpret_cast<const char*>(p) < T.keep_end) return ld_keep(p);
+  return ldt_stream(p);
 }
 
 template <bool ENS>
@@ -136,14 +162,14 @@ __device__ __forceinline__ void vertex_body(const DevTables& T, const DevWork& W
   double cor = 0.0;
 #pragma unroll
   for (int k = 0; k < VW; ++k) {
-    ve[k] = ldt(T.vertex_edges + k * T.ldv + v);
-    cu[k] = ldt(T.curl + k * T.ldv + v);
-    vc[k] = ldt(T.vertex_cells + k * T.ldv + v);
-    vh[k] = ldt(T.vertex_height + k * T.ldv + v);
-    if (KE != KE_CELL) vkw[k] = ldt(T.vk_weights + k * T.ldv + v);
+    ve[k] = ldt(T, T.vertex_edges + k * T.ldv + v);
+    cu[k] = ldt(T, T.curl + k * T.ldv + v);
+    vc[k] = ldt(T, T.vertex_cells + k * T.ldv + v);
+    vh[k] = ldt(T, T.vertex_height + k * T.ldv + v);
+    if (KE != KE_CELL) vkw[k] = ldt(T, T.vk_weights + k * T.ldv + v);
   }
   const bool qv = PV == PVM_TRISK || want_qv;
-  if (qv) cor = ldt(T.coriolis + v);
+  if (qv) cor = ldt(T, T.coriolis + v);
   pdl_wait();
   double uu[VW], hh[VW];
 #pragma unroll
@@ -185,23 +211,23 @@ __device__ __forceinline__ void flux_body(const DevTables& T, const DevWork& W, 
     int e, mm;
     split<ENS>(vb * blockDim.x + threadIdx.x, M, e, mm);
     if (e >= T.ne) return;
-    const int ev0 = ldt(T.edge_vertices + e), ev1 = ldt(T.edge_vertices + T.lde + e);
+    const int ev0 = ldt(T, T.edge_vertices + e), ev1 = ldt(T, T.edge_vertices + T.lde + e);
     int ec0 = 0, ec1 = 0;
     double eh0 = 0, eh1 = 0, vk0 = 0, vk1 = 0, r0 = 0, r1 = 0, gc = 0;
     if (KE != KE_VERTEX) {
-      ec0 = ldt(T.edge_cells + e);
-      ec1 = ldt(T.edge_cells + T.lde + e);
-      eh0 = ldt(T.edge_height + e);
-      eh1 = ldt(T.edge_height + T.lde + e);
+      ec0 = ldt(T, T.edge_cells + e);
+      ec1 = ldt(T, T.edge_cells + T.lde + e);
+      eh0 = ldt(T, T.edge_height + e);
+      eh1 = ldt(T, T.edge_height + T.lde + e);
     }
     if (KE != KE_CELL) {
-      vk0 = ldt(T.vk_height + e);
-      vk1 = ldt(T.vk_height + T.lde + e);
+      vk0 = ldt(T, T.vk_height + e);
+      vk1 = ldt(T, T.vk_height + T.lde + e);
     }
     if (PV != PVM_TRISK) {
-      r0 = ldt(T.rhombus + e);
-      r1 = ldt(T.rhombus + T.lde + e);
-      gc = ldt(T.g_coriolis + e);
+      r0 = ldt(T, T.rhombus + e);
+      r1 = ldt(T, T.rhombus + T.lde + e);
+      gc = ldt(T, T.g_coriolis + e);
     }
     pdl_wait();
     const size_t o = (size_t)e * M + mm;
@@ -237,12 +263,12 @@ __device__ __forceinline__ void flux_body(const DevTables& T, const DevWork& W, 
 #pragma unroll
     for (int k = 0; k < CW; ++k) {
       if (KE != KE_VERTEX) {
-        ce[k] = ldt(T.cell_edges + k * T.ldc + i);
-        kin[k] = ldt(T.kinetic + k * T.ldc + i);
+        ce[k] = ldt(T, T.cell_edges + k * T.ldc + i);
+        kin[k] = ldt(T, T.kinetic + k * T.ldc + i);
       }
       if (KE != KE_CELL) {
-        cv[k] = ldt(T.cell_vertices + k * T.ldc + i);
-        kk[k] = ldt(T.vk_kites + k * T.ldc + i);
+        cv[k] = ldt(T, T.cell_vertices + k * T.ldc + i);
+        kk[k] = ldt(T, T.vk_kites + k * T.ldc + i);
       }
     }
     pdl_wait();
@@ -307,8 +333,8 @@ __device__ __forceinline__ void tend_body(const DevTables& T, const DevWork& W, 
     int e, mm;
     split<ENS>(vb * blockDim.x + threadIdx.x, M, e, mm);
     if (e >= T.ne) return;
-    const int ec0 = ldt(T.edge_cells + e), ec1 = ldt(T.edge_cells + T.lde + e);
-    const double invd = ldt(T.inverse_dual + e);
+    const int ec0 = ldt(T, T.edge_cells + e), ec1 = ldt(T, T.edge_cells + T.lde + e);
+    const double invd = ldt(T, T.inverse_dual + e);
     const size_t o = (size_t)e * M + mm;
     double du;
     if (PV == PVM_TRISK) {
@@ -316,8 +342,8 @@ __device__ __forceinline__ void tend_body(const DevTables& T, const DevWork& W, 
       double tr[TWD];
 #pragma unroll
       for (int k = 0; k < TWD; ++k) {
-        te[k] = ldt(T.trisk_edges + k * T.lde + e);
-        tr[k] = ldt(T.trisk + k * T.lde + e);
+        te[k] = ldt(T, T.trisk_edges + k * T.lde + e);
+        tr[k] = ldt(T, T.trisk + k * T.lde + e);
       }
       pdl_wait();
       const double qself = W.qe[o];
@@ -336,9 +362,9 @@ __device__ __forceinline__ void tend_body(const DevTables& T, const DevWork& W, 
       double gw[GW];
 #pragma unroll
       for (int k = 0; k < GW; ++k) {
-        ge[k] = ldt(T.g_edges + k * T.lde + e);
-        if (PV == PVM_GASSMANN) gp[k] = ldt(T.g_pv_edges + k * T.lde + e);
-        gw[k] = ldt(T.g_weights + k * T.lde + e);
+        ge[k] = ldt(T, T.g_edges + k * T.lde + e);
+        if (PV == PVM_GASSMANN) gp[k] = ldt(T, T.g_pv_edges + k * T.lde + e);
+        gw[k] = ldt(T, T.g_weights + k * T.lde + e);
       }
       pdl_wait();
       double f[GW], q[GW];
@@ -375,8 +401,8 @@ __device__ __forceinline__ void tend_body(const DevTables& T, const DevWork& W, 
     double dv[CW];
 #pragma unroll
     for (int k = 0; k < CW; ++k) {
-      ce[k] = ldt(T.cell_edges + k * T.ldc + i);
-      dv[k] = ldt(T.divergence + k * T.ldc + i);
+      ce[k] = ldt(T, T.cell_edges + k * T.ldc + i);
+      dv[k] = ldt(T, T.divergence + k * T.ldc + i);
     }
     pdl_wait();
     double f[CW];

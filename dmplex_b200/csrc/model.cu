@@ -69,6 +69,11 @@ __global__ void k_vertex_curl(DevTables T, const double* u, double* zeta) {  // 
   zeta[v] = s;
 }
 
+void order_after_caller(cudaStream_t stream, cudaEvent_t ev) {
+  CUDA_CHECK(cudaEventRecord(ev, cudaStreamLegacy));
+  CUDA_CHECK(cudaStreamWaitEvent(stream, ev, 0));
+}
+
 bool is_device_pointer(const void* p) {
   cudaPointerAttributes a;
   cudaError_t e = cudaPointerGetAttributes(&a, p);
@@ -117,11 +122,24 @@ void launch(TriskModel& m, void (*kernel)(KArgs...), int64_t grid, int block, cu
   cfg.blockDim = dim3((unsigned)block);
   cfg.dynamicSmemBytes = 0;
   cfg.stream = m.stream;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchAttribute attr[2];
+  unsigned na = 0;
+  if (m.use_pdl && !ev0) {
+    attr[na].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[na].val.programmaticStreamSerializationAllowed = 1;
+    ++na;
+  }
+  if (m.l2_window) {  // the resident table prefix as a persisting L2 window
+    attr[na].id = cudaLaunchAttributeAccessPolicyWindow;
+    attr[na].val.accessPolicyWindow.base_ptr = m.table_base;
+    attr[na].val.accessPolicyWindow.num_bytes = m.l2_keep_bytes;
+    attr[na].val.accessPolicyWindow.hitRatio = 1.0f;
+    attr[na].val.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+    attr[na].val.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+    ++na;
+  }
   cfg.attrs = attr;
-  cfg.numAttrs = (m.use_pdl && !ev0) ? 1 : 0;
+  cfg.numAttrs = na;
   CUDA_CHECK(cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...));
   if (ev1) CUDA_CHECK(cudaEventRecord(ev1, m.stream));
   m.launches++;
@@ -238,6 +256,7 @@ void gather(TriskModel& m, double* dst, const double* src, const int32_t* idx, i
 void state_in(TriskModel& m, const double* y_user, double* dst) {
   const size_t bytes = (size_t)m.N * sizeof(double);
   if (is_device_pointer(y_user)) {
+    order_after_caller(m.stream, m.caller_ev);
     if (m.identity)
       CUDA_CHECK(cudaMemcpyAsync(dst, y_user, bytes, cudaMemcpyDeviceToDevice, m.stream));
     else
@@ -256,6 +275,7 @@ void state_in(TriskModel& m, const double* y_user, double* dst) {
 void state_out(TriskModel& m, double* y_user, const double* src) {
   const size_t bytes = (size_t)m.N * sizeof(double);
   if (is_device_pointer(y_user)) {
+    order_after_caller(m.stream, m.caller_ev);
     if (m.identity)
       CUDA_CHECK(cudaMemcpyAsync(y_user, src, bytes, cudaMemcpyDeviceToDevice, m.stream));
     else
@@ -492,18 +512,6 @@ void upload(TriskModel& m, const Coefficients& C) {
   auto& cn = m.cell_n2o;
   auto& en = m.edge_n2o;
   auto& vn = m.vert_n2o;
-  o.ce = pack_index(P, C.cell_edges, C.cw, CW, nc, ldc, cn, m.edge_o2n);
-  o.dv = pack_weight(P, C.divergence, C.cw, CW, nc, ldc, cn);
-  if (cellK) o.kin = pack_weight(P, C.kinetic, C.cw, CW, nc, ldc, cn);
-  if (vertK) {
-    o.cv = pack_index(P, C.vk_cell_vertices, C.cw, CW, nc, ldc, cn, m.vert_o2n);
-    o.vkk = pack_weight(P, C.vk_kites, C.cw, CW, nc, ldc, cn);
-  }
-  o.ec = pack_index(P, C.edge_cells, 2, 2, ne, lde, en, m.cell_o2n);
-  if (cellK) o.eh = pack_weight(P, C.edge_height, 2, 2, ne, lde, en);
-  o.ev = pack_index(P, C.edge_vertices, 2, 2, ne, lde, en, m.vert_o2n);
-  o.invd = pack_weight(P, C.inverse_dual, 1, 1, ne, lde, en);
-  if (vertK) o.vkh = pack_weight(P, C.vk_height, 2, 2, ne, lde, en);
   // Gassmann PV edges follow from the flux edges whenever every edge has the block
   // structure gassmann_coefficients produces; then the kernel derives them (exact).
   bool derived = false;
@@ -517,9 +525,11 @@ void upload(TriskModel& m, const Coefficients& C) {
         }
     if (derived) m.pv = PVM_GASSMANN_DERIVED;
   }
+  // Pack order: the tendency phase's tables first (edge_cells, read by two phases, leads),
+  // then the flux phase's, then the vertex phase's, then the areas (diagnostics only). An
+  // L2-resident prefix of the block (trisk_model_set_l2_residency) covers them in this order.
+  o.ec = pack_index(P, C.edge_cells, 2, 2, ne, lde, en, m.cell_o2n);
   if (C.pv_flux != PV_TRISK) {
-    o.rh = pack_weight(P, C.rhombus, 2, 2, ne, lde, en);
-    o.gc = pack_weight(P, C.g_coriolis, 1, 1, ne, lde, en);
     o.ge = pack_index(P, C.g_edges, 12, GW, ne, lde, en, m.edge_o2n);
     if (C.pv_flux == PV_GASSMANN && !derived)
       o.gp = pack_index(P, C.g_pv_edges, 12, GW, ne, lde, en, m.edge_o2n);
@@ -527,6 +537,21 @@ void upload(TriskModel& m, const Coefficients& C) {
   } else {
     o.te = pack_index(P, C.trisk_edges, C.tw, TWD, ne, lde, en, m.edge_o2n);
     o.tr = pack_weight(P, C.trisk, C.tw, TWD, ne, lde, en);
+  }
+  o.invd = pack_weight(P, C.inverse_dual, 1, 1, ne, lde, en);
+  o.ce = pack_index(P, C.cell_edges, C.cw, CW, nc, ldc, cn, m.edge_o2n);
+  o.dv = pack_weight(P, C.divergence, C.cw, CW, nc, ldc, cn);
+  o.ev = pack_index(P, C.edge_vertices, 2, 2, ne, lde, en, m.vert_o2n);
+  if (cellK) o.eh = pack_weight(P, C.edge_height, 2, 2, ne, lde, en);
+  if (vertK) o.vkh = pack_weight(P, C.vk_height, 2, 2, ne, lde, en);
+  if (C.pv_flux != PV_TRISK) {
+    o.rh = pack_weight(P, C.rhombus, 2, 2, ne, lde, en);
+    o.gc = pack_weight(P, C.g_coriolis, 1, 1, ne, lde, en);
+  }
+  if (cellK) o.kin = pack_weight(P, C.kinetic, C.cw, CW, nc, ldc, cn);
+  if (vertK) {
+    o.cv = pack_index(P, C.vk_cell_vertices, C.cw, CW, nc, ldc, cn, m.vert_o2n);
+    o.vkk = pack_weight(P, C.vk_kites, C.cw, CW, nc, ldc, cn);
   }
   o.ve = pack_index(P, C.vertex_edges, C.vw, VW, nv, ldv, vn, m.edge_o2n);
   o.cu = pack_weight(P, C.curl, C.vw, VW, nv, ldv, vn);
@@ -536,9 +561,12 @@ void upload(TriskModel& m, const Coefficients& C) {
   if (vertK) o.vkw = pack_weight(P, C.vk_weights, C.vw, VW, nv, ldv, vn);
   o.ac = pack_weight(P, C.cell_areas, 1, 1, nc, ldc, cn);
   o.av = pack_weight(P, C.vertex_areas, 1, 1, nv, ldv, vn);
+  const size_t used_bytes = o.ac;  // the kernels' tables end where the areas begin
 
   char* base = m.alloc<char>(P.host.size());
   CUDA_CHECK(cudaMemcpy(base, P.host.data(), P.host.size(), cudaMemcpyHostToDevice));
+  m.table_base = base;
+  m.table_block_bytes = used_bytes;
   auto I = [&](size_t off, bool used) { return used ? reinterpret_cast<const int32_t*>(base + off) : nullptr; };
   auto D = [&](size_t off, bool used) { return used ? reinterpret_cast<const double*>(base + off) : nullptr; };
   const bool g = C.pv_flux != PV_TRISK;
@@ -550,6 +578,7 @@ void upload(TriskModel& m, const Coefficients& C) {
   T.lde = (int32_t)lde;
   T.ldv = (int32_t)ldv;
   T.gravity = C.gravity;
+  T.keep_end = nullptr;
   T.cell_edges = I(o.ce, true);
   T.divergence = D(o.dv, true);
   T.kinetic = D(o.kin, cellK);
@@ -627,6 +656,7 @@ void finish_create(TriskModel& m, const Coefficients& C, const std::vector<V3>* 
   if (m.device < 0 || m.device >= ndev) throw Error(TRISK_ERR_ARGUMENT, "device ordinal out of range");
   DeviceGuard guard(m.device);
   CUDA_CHECK(cudaStreamCreateWithFlags(&m.stream, cudaStreamNonBlocking));
+  CUDA_CHECK(cudaEventCreateWithFlags(&m.caller_ev, cudaEventDisableTiming));
   build_numbering(m, C, centroids);
   upload(m, C);
   m.W.K = m.alloc<double>(m.nc);
@@ -920,9 +950,10 @@ int trisk_relative_vorticity(TriskModel* model, const double* y, double* zeta) {
   m.launches++;
   // zeta_file[v] = zeta_int[o2n[v]]
   gather(m, m.st, m.W.zv, m.vertex_o2n, m.nv);
-  if (is_device_pointer(zeta))
+  if (is_device_pointer(zeta)) {
+    order_after_caller(m.stream, m.caller_ev);
     CUDA_CHECK(cudaMemcpyAsync(zeta, m.st, m.nv * sizeof(double), cudaMemcpyDeviceToDevice, m.stream));
-  else
+  } else
     CUDA_CHECK(cudaMemcpyAsync(zeta, m.st, m.nv * sizeof(double), cudaMemcpyDeviceToHost, m.stream));
   CUDA_CHECK(cudaStreamSynchronize(m.stream));
   TRISK_API_END
@@ -1015,6 +1046,72 @@ int trisk_autotune(TriskModel* model, double* y, double dt, int32_t steps, doubl
   CUDA_CHECK(cudaMemsetAsync(m.flag, 0, sizeof(int), m.stream));
   CUDA_CHECK(cudaStreamSynchronize(m.stream));
   if (best_ms) *best_ms = best_t / steps;
+  TRISK_API_END
+}
+
+int trisk_model_set_block(TriskModel* model, const int32_t block[3]) {
+  TRISK_API_BEGIN
+  TriskModel& m = *checked(model);
+  if (!block) throw Error(TRISK_ERR_ARGUMENT, "NULL argument");
+  for (int p = 0; p < 3; ++p)
+    if (block[p] < 64 || block[p] > 256 || block[p] % 32)
+      throw Error(TRISK_ERR_ARGUMENT, "block sizes must be multiples of 32 in [64, 256]");
+  DeviceGuard guard(m.device);
+  CUDA_CHECK(cudaStreamSynchronize(m.stream));
+  for (int p = 0; p < 3; ++p) m.block[p] = block[p];
+  if (m.graph) {  // recaptured with the new launch shapes at the next step
+    cudaGraphExecDestroy(m.graph);
+    m.graph = nullptr;
+  }
+  TRISK_API_END
+}
+
+int trisk_l2_info(int32_t device, int64_t info[4]) {
+  TRISK_API_BEGIN
+  if (!info) throw Error(TRISK_ERR_ARGUMENT, "NULL argument");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+    cudaGetLastError();
+    throw Error(TRISK_ERR_ARGUMENT, "no such CUDA device");
+  }
+  int l2 = 0, persist = 0, window = 0;
+  CUDA_CHECK(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, device));
+  CUDA_CHECK(cudaDeviceGetAttribute(&persist, cudaDevAttrMaxPersistingL2CacheSize, device));
+  CUDA_CHECK(cudaDeviceGetAttribute(&window, cudaDevAttrMaxAccessPolicyWindowSize, device));
+  size_t limit = 0;
+  DeviceGuard guard(device);
+  CUDA_CHECK(cudaDeviceGetLimit(&limit, cudaLimitPersistingL2CacheSize));
+  info[0] = l2;
+  info[1] = persist;
+  info[2] = window;
+  info[3] = (int64_t)limit;
+  TRISK_API_END
+}
+
+int trisk_model_set_l2_residency(TriskModel* model, int64_t bytes, int32_t window) {
+  TRISK_API_BEGIN
+  TriskModel& m = *checked(model);
+  if (bytes < 0) throw Error(TRISK_ERR_ARGUMENT, "negative size");
+  DeviceGuard guard(m.device);
+  CUDA_CHECK(cudaStreamSynchronize(m.stream));
+  size_t keep = std::min((size_t)bytes, m.table_block_bytes);
+  bool win = window != 0 && keep > 0;
+  if (win) {  // the persisting set-aside of this process's context (released with it)
+    int persist = 0, wmax = 0;
+    CUDA_CHECK(cudaDeviceGetAttribute(&persist, cudaDevAttrMaxPersistingL2CacheSize, m.device));
+    CUDA_CHECK(cudaDeviceGetAttribute(&wmax, cudaDevAttrMaxAccessPolicyWindowSize, m.device));
+    keep = std::min(keep, (size_t)std::min(persist, wmax));
+    size_t limit = 0;
+    CUDA_CHECK(cudaDeviceGetLimit(&limit, cudaLimitPersistingL2CacheSize));
+    if (limit < keep) CUDA_CHECK(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, keep));
+  }
+  m.l2_keep_bytes = keep;
+  m.l2_window = win && keep > 0;
+  m.T.keep_end = keep ? m.table_base + keep : nullptr;
+  if (m.graph) {  // recaptured with the new table pointers and launch attributes
+    cudaGraphExecDestroy(m.graph);
+    m.graph = nullptr;
+  }
   TRISK_API_END
 }
 

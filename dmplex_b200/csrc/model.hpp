@@ -37,6 +37,10 @@ struct DeviceGuard {
 
 // true for device or managed memory, false for host memory (pageable or pinned)
 bool is_device_pointer(const void* p);
+// Orders `stream` after all work queued so far on the legacy default stream (and, by its
+// semantics, on every blocking stream), so a caller's device buffer filled or still read on
+// those streams (PyTorch's default stream among them) is safe to use from `stream`.
+void order_after_caller(cudaStream_t stream, cudaEvent_t ev);
 
 // dst[j] = src[idx[j]], j < n, on `stream`
 void launch_gather(cudaStream_t stream, double* dst, const double* src, const int32_t* idx, int64_t n);
@@ -87,12 +91,18 @@ struct TriskModel {
   double table_bytes_unique = 0;
   double phase_bytes[3] = {0, 0, 0};
   double pv_table_bytes_saved = 0;  // k_tend bytes per launch the derived PV edges do not read
+  cudaEvent_t caller_ev = nullptr;  // for order_after_caller
+  char* table_base = nullptr;       // the packed table block (tendency phase's tables first)
+  size_t table_block_bytes = 0;     // its part the kernels read
+  size_t l2_keep_bytes = 0;         // prefix loaded with the L2 evict-last policy
+  bool l2_window = false;           // plus a persisting access-policy window on every launch
 
   ~TriskModel() {
     int prev = -1;
     cudaGetDevice(&prev);
     cudaSetDevice(device);
     if (graph) cudaGraphExecDestroy(graph);
+    if (caller_ev) cudaEventDestroy(caller_ev);
     if (stream) {
       cudaStreamSynchronize(stream);
       cudaStreamDestroy(stream);

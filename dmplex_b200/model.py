@@ -138,11 +138,31 @@ class TRiSKShallowWater:
         check(lib.trisk_autotune(self._h, ptr(y_device), float(dt), int(steps), C.byref(best)))
         return best.value
 
+    def set_block(self, block) -> None:
+        """Threads per block of the (vertex, flux, tend) phases, e.g. an autotune result."""
+        b = np.ascontiguousarray(block, dtype=np.int32)
+        if b.shape != (3,):
+            raise ValueError("three block sizes")
+        check(lib.trisk_model_set_block(self._h, b.ctypes.data))
+
+    def set_l2_residency(self, nbytes: int, window: bool = False) -> None:
+        """Keeps the first nbytes of the packed tables in L2 (evict-last loads; with window
+        also a persisting access-policy window). 0 streams every table."""
+        check(lib.trisk_model_set_l2_residency(self._h, int(nbytes), int(bool(window))))
+
     def rk4_async(self, y_device, dt: float, nsteps: int = 1) -> None:
         check(lib.trisk_rk4_step_async(self._h, ptr(y_device), float(dt), int(nsteps)))
 
     def synchronize(self) -> None:
         check(lib.trisk_synchronize(self._h))
+
+
+def l2_info(device: int = 0) -> dict:
+    """L2 size, largest persisting set-aside, largest access-policy window and the current
+    persisting limit of a CUDA device, in bytes."""
+    out = np.zeros(4, dtype=np.int64)
+    check(lib.trisk_l2_info(int(device), out.ctypes.data))
+    return dict(zip(("l2_bytes", "max_persisting_bytes", "max_window_bytes", "persisting_limit"), out.tolist()))
 
 
 def _coefficients_dict(c: _lib.TriskCoefficients) -> dict:

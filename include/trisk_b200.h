@@ -208,6 +208,20 @@ int trisk_model_info(TriskModel* model, int32_t* pv_mode, int32_t block[3], doub
  * unchanged) for every combination of the phase block sizes {64, 128, 256} and keeps the
  * fastest in the model; best_ms gets its time per step. */
 int trisk_autotune(TriskModel* model, double* y_device, double dt, int32_t steps, double* best_ms);
+/* Sets the threads per block of the three phases (vertex, flux, tend), each a multiple of 32
+ * in [64, 256], as an autotuner result found earlier (no reference counterpart). */
+int trisk_model_set_block(TriskModel* model, const int32_t block[3]);
+/* L2 residency of the tables (no reference counterpart). The first `bytes` of the model's
+ * packed table block (the tendency phase's tables first, then the flux phase's, then the
+ * vertex phase's) are loaded with an L2 evict-last policy, so they stay in L2 from one
+ * phase launch and one RK4 stage to the next instead of streaming from HBM; with window = 1
+ * also as a persisting access-policy window of that size on every launch (this sets the
+ * context's persisting-L2 limit, at most cudaDevAttrMaxPersistingL2CacheSize). bytes = 0:
+ * all tables stream (the default). Results are unchanged. */
+int trisk_model_set_l2_residency(TriskModel* model, int64_t bytes, int32_t window);
+/* L2 size, largest persisting-L2 set-aside, largest access-policy window and the current
+ * persisting-L2 limit of a device, in bytes. */
+int trisk_l2_info(int32_t device, int64_t info[4]);
 /* Runs nsteps RK4 steps on the device-resident state with a CUDA event pair around every
  * kernel launch and returns the mean duration in ms of each phase kernel in ms[3]. */
 int trisk_profile_phases(TriskModel* model, double* y_device, double dt, int64_t nsteps, double ms[3]);

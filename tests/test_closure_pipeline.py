@@ -13,11 +13,14 @@ from dmplex_b200.coarsen import divergence_matrix
 pytestmark = pytest.mark.gpu
 
 
-def test_closure_pipeline_small(require_gpu):
+@pytest.mark.parametrize("tendency_targets", [True, False])
+def test_closure_pipeline_small(require_gpu, tendency_targets):
     import torch
     gf, gc = cp._grid(5), cp._grid(3)
-    Y0, Y1, delta, _, _ = cp.fine_snapshots(gf, gc, [1, 2, 3, 4, 5, 6], 0.5, 24, dt_fine=60.0, pair_steps=4)
+    Y0, Y1, delta, _, _ = cp.fine_snapshots(gf, gc, [1, 2, 3, 4, 5, 6], 0.5, 24, dt_fine=60.0, pair_steps=4,
+                                            tendency_targets=tendency_targets)
     assert Y0.shape == (gc.ne + gc.nc, Y0.shape[1]) and Y0.shape[1] >= 100
+    assert (delta == 0) == tendency_targets
     dF, dQ, mc, ens = cp.residual_targets(gc, Y0, Y1, delta)
     # the flux part reproduces the height residual: -D dF = r_h minus its null-space part
     D = divergence_matrix(d.model_tables(gc, pv_flux="trisk", kinetic_energy="cell", **w.si_parameters()))

@@ -75,6 +75,28 @@ def test_ensemble_reset_and_launches(require_gpu):
     assert ens.steps_taken() == [0]
 
 
+def test_ensemble_member_copies_ordered_after_default_stream(require_gpu):
+    import torch
+    g = trisk_grid(3, True)
+    m = d.TRiSKShallowWater(g)
+    ens = d.Ensemble([(m, 2, 0.001, 1)])
+    states = member_states(g, 2, 5)
+    src = torch.from_numpy(states[1]).cuda()
+    col = torch.zeros_like(src)
+    torch.cuda.synchronize()
+    torch.cuda._sleep(20_000_000)
+    col.copy_(src)
+    ens.set_member(0, 1, col)                  # reads col after the copy
+    assert np.array_equal(ens.get_member(0, 1), states[1])
+    ens.set_member(0, 0, states[0])
+    out = torch.full_like(src, 3.0)
+    torch.cuda._sleep(20_000_000)
+    seen = out * 1.0                           # queued read of the old contents
+    ens.get_member(0, 0, out)                  # overwrites out after that read
+    assert bool((seen == 3.0).all())
+    assert np.array_equal(out.cpu().numpy(), states[0])
+
+
 def test_ensemble_nonfinite_member(require_gpu):
     g = trisk_grid(3, True)
     m = d.TRiSKShallowWater(g)

@@ -139,6 +139,27 @@ def test_device_pointers(require_gpu):
     assert np.array_equal(yd.cpu().numpy(), a)
 
 
+def test_device_inputs_ordered_after_default_stream(require_gpu):
+    """A device state written on PyTorch's (legacy default) stream just before the call is
+    read after that write; an output buffer still being read there is written after it."""
+    import torch
+    g = trisk_grid(4, True)
+    m = d.TRiSKShallowWater(g, pv_flux="gassmann", kinetic_energy="vertex")
+    y = perturbed_tc2(g)
+    expect = np.zeros_like(y)
+    d.tendency(expect, y, m)
+    src = torch.from_numpy(y).cuda()
+    yd = torch.zeros_like(src)
+    dyd = torch.full_like(src, 7.0)
+    torch.cuda.synchronize()
+    torch.cuda._sleep(20_000_000)  # keeps the default stream busy for several milliseconds
+    yd.copy_(src)
+    seen = dyd * 1.0               # queued read of the output buffer's old contents
+    d.tendency(dyd, yd, m)
+    assert np.array_equal(dyd.cpu().numpy(), expect)
+    assert bool((seen == 7.0).all())
+
+
 def test_nonfinite_state_is_reported(require_gpu):
     g = trisk_grid(3)
     m = d.TRiSKShallowWater(g)
@@ -210,6 +231,15 @@ def test_autotune_keeps_results(require_gpu):
     assert np.array_equal(yd.cpu().numpy(), y)  # the autotuner leaves the state alone
     d.rk4_step(yd, 0.002, d.tendency, d.RK4Cache(yd), m, nsteps=4)
     assert np.array_equal(yd.cpu().numpy(), ref)
+    # fixed block sizes: same numbers, and bad sizes are rejected
+    m.set_block([64, 256, 96])
+    assert m.info()["block"] == [64, 256, 96]
+    yd = torch.from_numpy(y).cuda()
+    d.rk4_step(yd, 0.002, d.tendency, d.RK4Cache(yd), m, nsteps=4)
+    assert np.array_equal(yd.cpu().numpy(), ref)
+    for bad in ([32, 128, 128], [128, 100, 128], [128, 128, 512]):
+        with pytest.raises(d.TriskError):
+            m.set_block(bad)
 
 
 @pytest.mark.slow
