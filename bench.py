@@ -50,6 +50,8 @@ def parse():
     p.add_argument("--level", type=int, default=LEVEL, help="mesh level (7 is the benchmark workload)")
     p.add_argument("--block", default=None,
                    help="fixed block sizes of the three phases, e.g. 128,128,64 (skips the autotuner)")
+    p.add_argument("--l2-keep-mb", type=int, default=0,
+                   help="with --block: L2-resident table prefix in MB (the autotuner's other choice)")
     args = p.parse_args()
     return args
 
@@ -215,8 +217,9 @@ CLOSURE_SUMMARY = os.path.join(ROOT, "dmplex_b200", "data", "closure_hexagon6.js
 
 def run_closure_leg(local_rank, members=128, seed=7):
     """GPU seconds per simulated day: hexagon 6 x `members` with the learned closure (dt 150
-    s, TRiSK, FP64 state), the same ensemble without it, and one plain hexagon-8 member
-    (dt 20 s); plus the errors of the committed closure experiment, when present."""
+    s, TRiSK, FP32 state with FP64 arithmetic and energy sums), the same ensemble without it
+    (FP32 and FP64 state), and one plain hexagon-8 member (dt 20 s); plus the errors of the
+    committed closure experiment, when present."""
     import torch
     import dmplex_b200 as d
     from dmplex_b200 import workloads as w
@@ -224,7 +227,8 @@ def run_closure_leg(local_rank, members=128, seed=7):
     from dmplex_b200.coarsen import edge_geometry
     from dmplex_b200._lib import TriskError
     si = w.si_parameters()
-    out = {"workload": f"hexagon6 x {members} members, TRiSK/cell, dt 150 s, FP64 state, 1 simulated day",
+    out = {"workload": f"hexagon6 x {members} members, TRiSK/cell, dt 150 s, FP32 state (FP64 arithmetic and "
+                       f"sums), 1 simulated day",
            "members": members}
     g6 = d.TRiSKGrid(d.create_hexagon_mesh(6, centroidal=True))
     m6 = d.TRiSKShallowWater(g6, pv_flux="trisk", kinetic_energy="cell", device=local_rank, **si)
@@ -240,8 +244,8 @@ def run_closure_leg(local_rank, members=128, seed=7):
         norm = np.concatenate([np.zeros(24), np.ones(24), [0.0, 0.0]])
         out["weights"] = "untrained, zero output scales (timing only)"
 
-    def timed(with_closure):
-        ens = d.Ensemble([(m6, members, 150.0, steps)])
+    def timed(with_closure, state_bits=32):
+        ens = d.Ensemble([(m6, members, 150.0, steps)], state_bits=state_bits)
         for k, y in enumerate(states):
             ens.set_member(0, k, y)
         if with_closure:
@@ -272,6 +276,7 @@ def run_closure_leg(local_rank, members=128, seed=7):
     out["closure_gpu_seconds_per_simulated_day"], out["closure_gpu_launches"], out["closure_max_energy_drift_day"] = \
         timed(True)
     out["plain_gpu_seconds_per_simulated_day"], _, out["plain_max_energy_drift_day"] = timed(False)
+    out["plain_fp64_gpu_seconds_per_simulated_day"], _, out["plain_fp64_max_energy_drift_day"] = timed(False, 64)
     out["closure_cell_steps_per_s"] = members * g6.nc * steps / out["closure_gpu_seconds_per_simulated_day"]
     # one plain hexagon-8 member at dt = 20 s: time 40 steps, scale to a day
     g8 = d.TRiSKGrid(d.create_hexagon_mesh(8, centroidal=True))
@@ -294,11 +299,12 @@ def run_closure_leg(local_rank, members=128, seed=7):
         with open(CLOSURE_SUMMARY) as f:
             s = json.load(f)
         out["errors_vs_coarse_grained_hexagon8"] = {
-            k: {"h_l2_last_day_m": float(np.mean(s[k]["h_l2"][-1])),
+            k: {"h_l2_per_day_m": [round(float(np.mean(x)), 3) for x in s[k]["h_l2"]],
                 "zeta_l2_last_day": float(np.mean(s[k]["zeta_l2"][-1])),
-                "fallback_members": s[k].get("fallback_members")}
-            for k in ("plain_coarse", "closure_coarse", "closure_coarse_no_fallback",
-                      "closure_mass_flux_only_no_fallback") if k in s}
+                "fallback_members": s[k].get("fallback_members"), "diverged_on_day": s[k].get("diverged_on_day"),
+                "state_bits": s[k].get("state_bits", 64)}
+            for k in ("plain_coarse", "plain_coarse_fp32", "closure_coarse", "closure_coarse_no_fallback",
+                      "closure_every_stage_no_fallback", "closure_mass_flux_only_no_fallback") if k in s}
         out["errors_source"] = "dmplex_b200/data/closure_hexagon6.json (python -m dmplex_b200.closure_pipeline)"
     return out
 
@@ -351,6 +357,7 @@ def run_b200(args, rank, world, local_rank):
     # block shapes from the autotuner (or given), then warm-up (also captures the CUDA graph)
     if args.block:
         m.set_block([int(b) for b in args.block.split(",")])
+        m.set_l2_residency(args.l2_keep_mb << 20)
         tuned_ms = None
     else:
         tuned_ms = m.autotune(yd, DT, 20)
@@ -402,7 +409,8 @@ def run_b200(args, rank, world, local_rank):
                 "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
                 "traffic": ncu_traffic("k_tend"), "algorithmic_bytes_per_launch": nbytes_phase["tend"],
                 "implementation_bytes_per_launch": nbytes_phase["tend"] - info["derived_pv_bytes_saved"],
-                "pv_mode": info["pv_mode"], "block": info["block"], "autotune_ms_per_step": tuned_ms,
+                "pv_mode": info["pv_mode"], "block": info["block"],
+                "l2_resident_table_bytes": info["l2_resident_table_bytes"], "autotune_ms_per_step": tuned_ms,
                 "launch_ms": phases["tend"], "phase_ms": phases,
                 "phase_bytes": {k: nbytes_phase[k] for k in ("vertex", "flux", "tend")},
                 "step_bytes": nbytes_phase["rk4_step"], "step_gbs": step_gbs, "step_frac": step_gbs / peak}

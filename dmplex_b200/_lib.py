@@ -129,6 +129,7 @@ def _load():
         "trisk_closure_synchronize": (C.c_int, [_p]),
         "trisk_closure_stream": (C.c_int, [_p, C.POINTER(_p)]),
         "trisk_ensemble_create": (C.c_int, [_p, _p, _p, _p, _i32, C.POINTER(_p)]),
+        "trisk_ensemble_create_precision": (C.c_int, [_p, _p, _p, _p, _i32, _i32, C.POINTER(_p)]),
         "trisk_ensemble_destroy": (None, [_p]),
         "trisk_ensemble_set_member": (C.c_int, [_p, _i32, _i32, _p]),
         "trisk_ensemble_get_member": (C.c_int, [_p, _i32, _i32, _p]),
@@ -147,6 +148,7 @@ def _load():
         "trisk_autotune": (C.c_int, [_p, _p, _f64, _i32, C.POINTER(_f64)]),
         "trisk_model_set_block": (C.c_int, [_p, _p]),
         "trisk_model_set_l2_residency": (C.c_int, [_p, _i64, _i32]),
+        "trisk_model_get_l2_residency": (C.c_int, [_p, C.POINTER(_i64), C.POINTER(_i32)]),
         "trisk_l2_info": (C.c_int, [_i32, _p]),
     }
     for name, (res, args) in sig.items():

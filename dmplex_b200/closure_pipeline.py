@@ -270,11 +270,11 @@ def l2_errors(gc, Vc, Y, Yt):
 
 
 def run_coarse(gc, Y_init, days, dt, daily_truth, mlp=None, norm=None, drift_per_day=1e-6, device=0,
-               every_stage=False, momentum_scale=1.0):
+               every_stage=False, momentum_scale=1.0, state_bits=64):
     """Coarse ensemble (members = columns of Y_init) for `days` days; h and vorticity errors
     against the daily truth, GPU seconds, and the members that fell back to the plain step.
     momentum_scale multiplies the closure's momentum correction (0 keeps only the mass-flux
-    correction)."""
+    correction); state_bits 32 stores the members' states as float."""
     if norm is not None:
         norm = np.array(norm, dtype=np.float64)
         norm[2 * NFEAT + 1] *= momentum_scale
@@ -283,7 +283,7 @@ def run_coarse(gc, Y_init, days, dt, daily_truth, mlp=None, norm=None, drift_per
     mc = TRiSKShallowWater(gc, pv_flux=PV, kinetic_energy=KE, device=device, **si)
     S = Y_init.shape[1]
     steps_day = int(round(86400 / dt))
-    ens = Ensemble([(mc, S, 86400 / steps_day, steps_day * days)])
+    ens = Ensemble([(mc, S, 86400 / steps_day, steps_day * days)], state_bits=state_bits)
     col = torch.empty(mc.state_size, dtype=torch.float64, device=Y_init.device)
     for k in range(S):
         col.copy_(Y_init[:, k])
@@ -325,7 +325,8 @@ def run_coarse(gc, Y_init, days, dt, daily_truth, mlp=None, norm=None, drift_per
     done = len(errs_h)
     return {"h_l2": errs_h, "zeta_l2": errs_z, "max_energy_drift_per_day": drifts, "diverged_on_day": diverged,
             "gpu_seconds": gpu_ms / 1e3, "gpu_seconds_per_member_day": gpu_ms / 1e3 / (S * max(done, 1)),
-            "fallback_members": int((on == 0).sum()) if mlp is not None else None, "members": S}
+            "fallback_members": int((on == 0).sum()) if mlp is not None else None, "members": S,
+            "state_bits": state_bits}
 
 
 def pipeline(fine_level=8, coarse_level=6, train_seeds=32, train_days=10, snapshots=2000, eval_seeds=4,
@@ -377,21 +378,24 @@ def pipeline(fine_level=8, coarse_level=6, train_seeds=32, train_days=10, snapsh
 
 def evaluate(gf, gc, mlp, norm, eval_seeds=4, eval_days=10, coarse_dt=150.0, fine_dt=20.0, device=0, log=print):
     """Coarse runs from the coarse-grained state of held-out seeds against the coarse-grained
-    fine run: plain, closure with the energy-drift fallback, closure without it, and the
-    mass-flux correction alone."""
+    fine run: plain (FP64 and FP32 state), and with FP32 state the closure with the energy-
+    drift fallback, without it, evaluated at every RK4 stage, and the mass-flux correction
+    alone."""
     eval_list = list(range(1001, 1001 + eval_seeds))
     _, _, _, daily, fine_eval_s = fine_snapshots(gf, gc, eval_list, eval_days, 0, dt_fine=fine_dt, device=device,
                                                  spinup_days=0.0, record_days=True)
     out = {"eval_seeds": eval_seeds, "eval_days": eval_days, "coarse_dt": coarse_dt, "fine_dt": fine_dt,
            "fine_gpu_seconds_per_member_day": fine_eval_s / (eval_seeds * eval_days)}
     init = daily[0]
+    f32 = {"state_bits": 32}
     variants = {"plain_coarse": {},
-                "closure_coarse": {"mlp": mlp, "norm": norm},
-                "closure_coarse_no_fallback": {"mlp": mlp, "norm": norm, "drift_per_day": np.inf},
+                "plain_coarse_fp32": dict(f32),
+                "closure_coarse": {"mlp": mlp, "norm": norm, **f32},
+                "closure_coarse_no_fallback": {"mlp": mlp, "norm": norm, "drift_per_day": np.inf, **f32},
                 "closure_every_stage_no_fallback": {"mlp": mlp, "norm": norm, "drift_per_day": np.inf,
-                                                    "every_stage": True},
+                                                    "every_stage": True, **f32},
                 "closure_mass_flux_only_no_fallback": {"mlp": mlp, "norm": norm, "drift_per_day": np.inf,
-                                                       "momentum_scale": 0.0}}
+                                                       "momentum_scale": 0.0, **f32}}
     for name, kw in variants.items():
         r = run_coarse(gc, init, eval_days, coarse_dt, daily, device=device, **kw)
         out[name] = r

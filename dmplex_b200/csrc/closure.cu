@@ -25,7 +25,8 @@
 //              DW += DD^T [H1 | X]   M=128 N=96 K=128 (A = DD MN-major, B = HX MN-major):
 //                   rows 0..63 x cols 0..63 = dW2, rows 64..127 x cols 64..87 = dW1
 //
-// Tensor memory (256 columns): Z1 at 0, Z2 (then G) at 64, DW at 128..224.
+// Tensor memory: Z1 at 0, Z2 (then G) at 64, DW at 128..224 (training: 256 columns, two
+// CTAs per SM; inference: 128 columns, four CTAs per SM).
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -47,7 +48,17 @@ constexpr int W1_BYTES = 4 * W_CHUNK;    // 64 x 32
 constexpr int W2_BYTES = 8 * W_CHUNK;    // 64 x 64
 // + 64 B (mbarrier, TMEM address) + H2 (128 x 64 BF16) and dY (128 x 2 FP32) for training
 constexpr int SMEM_BYTES = HX_BYTES + DD_BYTES + W1_BYTES + W2_BYTES + 64 + TILE * NH * 2 + TILE * NOUT * 4;
-constexpr uint32_t TMEM_COLS = 256;
+// Inference needs HX, W1, W2 and the barrier (36 KB) and 128 TMEM columns (Z1, Z2), so four
+// CTAs share an SM's 512 columns; its request is padded to 53 KB so that no fifth CTA, which
+// would wait in tcgen05.alloc for a whole CTA lifetime, becomes resident.
+constexpr int FWD_SMEM_BYTES = 53 * 1024;
+static_assert(HX_BYTES + W1_BYTES + W2_BYTES + 64 <= FWD_SMEM_BYTES, "inference shared memory");
+template <int TRAIN>
+struct MlpShape {
+  static constexpr uint32_t tmem_cols = TRAIN ? 256 : 128;
+  static constexpr int smem = TRAIN ? SMEM_BYTES : FWD_SMEM_BYTES;
+  static constexpr int ctas_per_sm = TRAIN ? 2 : 4;
+};
 constexpr int MBAR_SPIN_LIMIT = 1 << 20;
 
 // FP32 master parameters and their BF16 tensor-core copies (one contiguous block each).
@@ -151,15 +162,16 @@ struct Status {
 constexpr int ONES_COL = 64 + NIN;
 
 template <int TRAIN>
-__global__ void __launch_bounds__(TILE, 1) k_mlp(const __nv_bfloat16* __restrict__ X, int64_t n,
+__global__ void __launch_bounds__(TILE, MlpShape<TRAIN>::ctas_per_sm) k_mlp(const __nv_bfloat16* __restrict__ X, int64_t n,
                                                   const ParamsBF16* __restrict__ wbf, const Params* __restrict__ p,
                                                   const float* __restrict__ target, float* __restrict__ Y,
                                                   Params* __restrict__ grad, float* loss, float inv_n,
                                                   Status* status) {
   extern __shared__ __align__(1024) unsigned char smem[];
+  constexpr uint32_t TMEM_COLS = MlpShape<TRAIN>::tmem_cols;
   unsigned char* HX = smem;
-  unsigned char* DD = smem + HX_BYTES;
-  unsigned char* W1s = DD + DD_BYTES;
+  unsigned char* DD = smem + HX_BYTES;  // training only
+  unsigned char* W1s = DD + (TRAIN ? DD_BYTES : 0);
   unsigned char* W2s = W1s + W1_BYTES;
   uint64_t* mbar = reinterpret_cast<uint64_t*>(W2s + W2_BYTES);
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(W2s + W2_BYTES + 16);
@@ -450,7 +462,7 @@ struct TriskClosure {
   Status* status = nullptr;
   int64_t adam_step = 0;
   int64_t launches = 0;
-  int grid_limit = 0;
+  int sms = 0;  // the device's SM count (persistent grids)
   ~TriskClosure() {
     int prev = -1;
     cudaGetDevice(&prev);
@@ -479,16 +491,17 @@ void check_status(TriskClosure& c) {
   }
 }
 
-int mlp_grid(TriskClosure& c, int64_t n) {
+int mlp_grid(TriskClosure& c, int64_t n, int train) {
   const int64_t tiles = (n + TILE - 1) / TILE;
-  return (int)std::max<int64_t>(1, std::min<int64_t>(tiles, c.grid_limit));
+  const int64_t limit = (int64_t)c.sms * (train ? MlpShape<1>::ctas_per_sm : MlpShape<0>::ctas_per_sm);
+  return (int)std::max<int64_t>(1, std::min<int64_t>(tiles, limit));
 }
 
 template <int TRAIN>
 void launch_mlp(TriskClosure& c, const __nv_bfloat16* X, int64_t n, const float* target, float* Y, float inv_n) {
   if (n == 0) return;
-  k_mlp<TRAIN><<<mlp_grid(c, n), TILE, SMEM_BYTES, c.stream>>>(X, n, c.wbf, c.p, target, Y, c.g, c.loss, inv_n,
-                                                                 c.status);
+  k_mlp<TRAIN><<<mlp_grid(c, n, TRAIN), TILE, MlpShape<TRAIN>::smem, c.stream>>>(X, n, c.wbf, c.p, target, Y, c.g,
+                                                                                  c.loss, inv_n, c.status);
   CUDA_CHECK(cudaGetLastError());
   c.launches++;
 }
@@ -499,8 +512,9 @@ namespace trisk {
 
 void closure_forward_on(TriskClosure* c, const void* X, int64_t n, float* Y, cudaStream_t stream) {
   if (n == 0) return;
-  k_mlp<0><<<mlp_grid(*c, n), TILE, SMEM_BYTES, stream>>>(static_cast<const __nv_bfloat16*>(X), n, c->wbf, c->p,
-                                                           nullptr, Y, nullptr, nullptr, 0.0f, c->status);
+  k_mlp<0><<<mlp_grid(*c, n, 0), TILE, MlpShape<0>::smem, stream>>>(static_cast<const __nv_bfloat16*>(X), n, c->wbf,
+                                                                     c->p, nullptr, Y, nullptr, nullptr, 0.0f,
+                                                                     c->status);
   CUDA_CHECK(cudaGetLastError());
   c->launches++;
 }
@@ -534,11 +548,11 @@ int trisk_closure_create(int32_t device, const float* params, TriskClosure** out
   else CUDA_CHECK(cudaMemset(c->p, 0, sizeof(Params)));
   k_refresh_bf16<<<(NH * NH + 255) / 256, 256, 0, c->stream>>>(c->p, c->wbf);
   CUDA_CHECK(cudaGetLastError());
-  CUDA_CHECK(cudaFuncSetAttribute(k_mlp<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
-  CUDA_CHECK(cudaFuncSetAttribute(k_mlp<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+  CUDA_CHECK(cudaFuncSetAttribute(k_mlp<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, MlpShape<0>::smem));
+  CUDA_CHECK(cudaFuncSetAttribute(k_mlp<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, MlpShape<1>::smem));
   int sms = 0;
   CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-  c->grid_limit = sms * 2;  // two CTAs of 256 TMEM columns fit an SM's 512
+  c->sms = sms;
   CUDA_CHECK(cudaStreamSynchronize(c->stream));
   *out = c.release();
   TRISK_API_END

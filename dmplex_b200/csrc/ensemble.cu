@@ -48,48 +48,60 @@ __device__ __forceinline__ int group_of(const GroupSet& G, int vb, int phase) {
   return gi;
 }
 
-template <int PV, int KE>
+// The group descriptors keep every buffer as double*; an FP32-state ensemble (R = float)
+// reinterprets them, its buffers having been allocated with 4-byte elements.
+template <class R>
+__device__ __forceinline__ const R* as_r(const double* p) {
+  return reinterpret_cast<const R*>(p);
+}
+template <class R>
+__device__ __forceinline__ R* as_r(double* p) {
+  return reinterpret_cast<R*>(p);
+}
+
+template <int PV, int KE, class R>
 __global__ void __launch_bounds__(256) kg_vertex(const GroupSet G, int first_stage) {
   pdl_trigger();
   for (int vb = blockIdx.x; vb < G.totalV; vb += gridDim.x) {
     const int gi = group_of(G, vb, 0);
     const GroupDesc& D = G.g[gi];
     if (G.counters[gi] >= D.nsteps) continue;
-    const double* u = first_stage ? D.y : D.st;
-    vertex_body<PV, KE, true>(D.T, D.W, u, u + (size_t)D.T.ne * D.M, D.M, 0, vb - D.startV);
+    const R* u = as_r<R>(first_stage ? D.y : D.st);
+    vertex_body<PV, KE, true, R>(D.T, work_as<R>(D.W), u, u + (size_t)D.T.ne * D.M, D.M, 0, vb - D.startV);
   }
 }
 
-template <int PV, int KE>
+template <int PV, int KE, class R>
 __global__ void __launch_bounds__(256) kg_flux(const GroupSet G, int first_stage, int want_K) {
   pdl_trigger();
   for (int vb = blockIdx.x; vb < G.totalF; vb += gridDim.x) {
     const int gi = group_of(G, vb, 1);
     const GroupDesc& D = G.g[gi];
     if (G.counters[gi] >= D.nsteps) continue;
-    const double* u = first_stage ? D.y : D.st;
-    flux_body<PV, KE, true>(D.T, D.W, u, u + (size_t)D.T.ne * D.M, D.M, D.nEF, want_K, vb - D.startF);
+    const R* u = as_r<R>(first_stage ? D.y : D.st);
+    flux_body<PV, KE, true, R>(D.T, work_as<R>(D.W), u, u + (size_t)D.T.ne * D.M, D.M, D.nEF, want_K,
+                               vb - D.startF);
   }
 }
 
-template <int PV, int EPI>
+template <int PV, int EPI, class R>
 __global__ void __launch_bounds__(256) kg_tend(const GroupSet G) {
   pdl_trigger();
   for (int vb = blockIdx.x; vb < G.totalT; vb += gridDim.x) {
     const int gi = group_of(G, vb, 2);
     const GroupDesc& D = G.g[gi];
     if (G.counters[gi] >= D.nsteps) continue;
-    DevStage S{};
-    S.y = D.y;
-    S.acc = D.acc;
-    S.st = D.st;
+    DevStageT<R> S{};
+    S.y = as_r<R>(D.y);
+    S.acc = as_r<R>(D.acc);
+    S.st = as_r<R>(D.st);
     S.flag = G.flag;
     S.c = EPI == EPI_STAGE3 ? D.dt : D.dt / 2;
     S.sixth = D.dt / 6;
     if (D.W.dq)
-      tend_body<PV, EPI, true, true>(D.T, D.W, S, D.M, D.nET, vb - D.startT);
+      tend_body<PV, EPI, true, true, R>(D.T, work_as<R>(D.W), S, D.M, D.nET, vb - D.startT);
     else
-      tend_body<PV, EPI, true, false>(D.T, D.W, S, D.M, D.nET, vb - D.startT);
+      tend_body<PV, EPI, true, false, R>(D.T, work_as<R>(D.W), S, D.M, D.nET, vb - D.startT);
   }
 }
 
@@ -104,33 +116,40 @@ struct FeatureNorm {
   double out_scale[2];
 };
 
-// The network's 24 inputs of (edge, member) rows e * M + m: u_e, u at the 10 TRiSK stencil
-// edges (0 for padded entries), h at the two cells, q at the two vertices, K = B - g h at
-// the two cells, and 7 geometry values of the edge. Output row: row_map ? row_map[e] * M + m
-// (file edge numbering) : the internal row.
-__global__ void kg_features(DevTables T, DevWork W, const double* y, int M, const float* geom,
+// The network's 24 inputs of (edge, member) rows e * M + m, formed in FP64 as the stencil's
+// mean and differences so that their BF16 rounding keeps the local gradients: u_e; u at the
+// 10 TRiSK stencil edges minus u_e (0 for padded entries); the mean and the difference
+// (second cell minus first) of h at the two cells, of q at the two vertices and of K = B - g h
+// at the two cells; and 7 geometry values of the edge. Output row: row_map ? row_map[e] * M
+// + m (file edge numbering) : the internal row.
+template <class R>
+__global__ void kg_features(DevTables T, DevWorkT<R> W, const R* y, int M, const float* geom,
                             const FeatureNorm N, __nv_bfloat16* X, const int32_t* row_map, int64_t rows) {
   const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (r >= rows) return;
   const int e = (int)(r / M), m = (int)(r - (int64_t)e * M);
-  const double* u = y;
-  const double* h = y + (size_t)T.ne * M;
+  const R* u = y;
+  const R* h = y + (size_t)T.ne * M;
   double f[NFEAT];
-  f[0] = u[(size_t)e * M + m];
+  const double ue = u[(size_t)e * M + m];
+  f[0] = ue;
 #pragma unroll
   for (int k = 0; k < TWD; ++k) {
     const int ep = T.trisk_edges[k * T.lde + e];
-    f[1 + k] = T.trisk[k * T.lde + e] != 0.0 ? u[(size_t)ep * M + m] : 0.0;
+    f[1 + k] = T.trisk[k * T.lde + e] != 0.0 ? (double)u[(size_t)ep * M + m] - ue : 0.0;
   }
   const int c0 = T.edge_cells[e], c1 = T.edge_cells[T.lde + e];
   const int v0 = T.edge_vertices[e], v1 = T.edge_vertices[T.lde + e];
   const double h0 = h[(size_t)c0 * M + m], h1 = h[(size_t)c1 * M + m];
-  f[11] = h0;
-  f[12] = h1;
-  f[13] = W.qv[(size_t)v0 * M + m];
-  f[14] = W.qv[(size_t)v1 * M + m];
-  f[15] = W.B[(size_t)c0 * M + m] - T.gravity * h0;
-  f[16] = W.B[(size_t)c1 * M + m] - T.gravity * h1;
+  const double q0 = W.qv[(size_t)v0 * M + m], q1 = W.qv[(size_t)v1 * M + m];
+  const double K0 = (double)W.B[(size_t)c0 * M + m] - T.gravity * h0;
+  const double K1 = (double)W.B[(size_t)c1 * M + m] - T.gravity * h1;
+  f[11] = (h0 + h1) / 2;
+  f[12] = h1 - h0;
+  f[13] = (q0 + q1) / 2;
+  f[14] = q1 - q0;
+  f[15] = (K0 + K1) / 2;
+  f[16] = K1 - K0;
 #pragma unroll
   for (int k = 0; k < NGEOM; ++k) f[17 + k] = geom[(size_t)e * NGEOM + k];
   const int64_t out = row_map ? (int64_t)row_map[e] * M + m : r;
@@ -141,17 +160,19 @@ __global__ void kg_features(DevTables T, DevWork W, const double* y, int M, cons
 // dF = on[m] sF y0 (mass flux: added to F in the flux-form continuity equation only, so
 // mass stays conserved and the PV flux keeps the resolved F); dq = on[m] sQ y1 (momentum
 // tendency).
-__global__ void kg_closure_apply(double* dF, double* dq, const float* Y, const float* member_on, int64_t rows, int M,
+template <class R>
+__global__ void kg_closure_apply(R* dF, R* dq, const float* Y, const float* member_on, int64_t rows, int M,
                                  double sF, double sQ) {
   const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (r >= rows) return;
   const double on = member_on[r % M];
-  dF[r] = on * sF * (double)Y[2 * r];
-  dq[r] = on * sQ * (double)Y[2 * r + 1];
+  dF[r] = (R)(on * sF * (double)Y[2 * r]);
+  dq[r] = (R)(on * sQ * (double)Y[2 * r + 1]);
 }
 
 // energy[m] += sum_i A_i h_i (K_i + g h_i / 2) over this block's cells (TRiSKShallowWater.jl:406-411)
-__global__ void kg_energy(const double* y, const double* K, const double* area, int nc, int ne, int M, double g,
+template <class R>
+__global__ void kg_energy(const R* y, const R* K, const double* area, int nc, int ne, int M, double g,
                           double* energy) {
   __shared__ double sm[256];
   const int m = blockIdx.y;
@@ -159,7 +180,8 @@ __global__ void kg_energy(const double* y, const double* K, const double* area, 
   double s = 0.0;
   if (i < nc) {
     const double hi = y[(size_t)ne * M + (size_t)i * M + m];
-    s = area[i] * hi * (K[(size_t)i * M + m] + g * hi / 2);
+    const double Ki = K[(size_t)i * M + m];
+    s = area[i] * hi * (Ki + g * hi / 2);
   }
   sm[threadIdx.x] = s;
   __syncthreads();
@@ -175,13 +197,15 @@ __global__ void kg_advance(int* counters, int n) {
 }
 
 // y_group[j M + m] = y_file[n2o[j]]  and back
-__global__ void kg_scatter_member(double* dst, const double* src, const int32_t* n2o, int64_t N, int M, int m) {
+template <class R>
+__global__ void kg_scatter_member(R* dst, const double* src, const int32_t* n2o, int64_t N, int M, int m) {
   const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (j < N) dst[j * M + m] = src[n2o[j]];
+  if (j < N) dst[j * M + m] = (R)src[n2o[j]];
 }
-__global__ void kg_gather_member(double* dst, const double* src, const int32_t* o2n, int64_t N, int M, int m) {
+template <class R>
+__global__ void kg_gather_member(double* dst, const R* src, const int32_t* o2n, int64_t N, int M, int m) {
   const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (j < N) dst[j] = src[(int64_t)o2n[j] * M + m];
+  if (j < N) dst[j] = (double)src[(int64_t)o2n[j] * M + m];
 }
 
 }  // namespace trisk
@@ -193,8 +217,8 @@ struct ClosureSlot {
   float* Y = nullptr;          // rows x 2 corrections
   float* geom = nullptr;       // ne x 7, internal edge order
   float* member_on = nullptr;  // M flags (1: closure on, 0: plain step)
-  double* dF = nullptr;        // rows: mass-flux correction (continuity equation only)
-  double* dq = nullptr;        // rows: momentum-tendency correction
+  double* dF = nullptr;        // rows: mass-flux correction (continuity equation only), storage type
+  double* dq = nullptr;        // rows: momentum-tendency correction, storage type
   trisk::FeatureNorm norm{};
   bool every_stage = false;    // false: the network runs at stage 1 and its output is reused
 };
@@ -203,6 +227,7 @@ struct TriskEnsemble {
   int device = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t caller_ev = nullptr;  // for order_after_caller
+  bool fp32 = false;                // state and work vectors stored as float (arithmetic FP64)
   int pv = 0, ke = 0;
   int block = 128;
   int grid[3] = {0, 0, 0};
@@ -241,6 +266,9 @@ struct TriskEnsemble {
     allocations.push_back(p);
     return static_cast<T*>(p);
   }
+  size_t esize() const { return fp32 ? sizeof(float) : sizeof(double); }
+  // a state or work vector of `count` elements of the storage type, kept as double*
+  double* alloc_state(size_t count) { return reinterpret_cast<double*>(alloc<char>(count * esize())); }
 };
 
 namespace {
@@ -263,6 +291,15 @@ void with_modes_e(int pv, int ke, F&& f) {
     case 11: f(integral_constant<int, 3>{}, integral_constant<int, 2>{}); break;
     default: throw Error(TRISK_ERR_ARGUMENT, "bad scheme");
   }
+}
+
+// f(R{}) with R the ensemble's storage type.
+template <class F>
+void with_real(const TriskEnsemble& e, F&& f) {
+  if (e.fp32)
+    f(float{});
+  else
+    f(double{});
 }
 
 template <typename... KArgs, typename... Args>
@@ -292,19 +329,20 @@ void enqueue_closure(TriskEnsemble& e, int stage) {
     const GroupDesc& D = e.G.g[g];
     const int64_t rows = (int64_t)D.T.ne * D.M;
     const unsigned nb = (unsigned)cdiv(rows, 256);
-    if (stage == 1 || c.every_stage) {
-      kg_features<<<nb, 256, 0, e.stream>>>(D.T, D.W, stage == 1 ? D.y : D.st, D.M, c.geom, c.norm, c.X, nullptr,
-                                            rows);
+    if (stage != 1 && !c.every_stage) continue;
+    with_real(e, [&](auto r) {
+      using R = decltype(r);
+      kg_features<R><<<nb, 256, 0, e.stream>>>(D.T, work_as<R>(D.W),
+                                               reinterpret_cast<const R*>(stage == 1 ? D.y : D.st), D.M, c.geom,
+                                               c.norm, c.X, nullptr, rows);
       CUDA_CHECK(cudaGetLastError());
       closure_forward_on(c.net, c.X, rows, c.Y, e.stream);
-      e.launches += 2;
-    }
-    if (stage == 1 || c.every_stage) {
-      kg_closure_apply<<<nb, 256, 0, e.stream>>>(c.dF, c.dq, c.Y, c.member_on, rows, D.M, c.norm.out_scale[0],
-                                                 c.norm.out_scale[1]);
+      kg_closure_apply<R><<<nb, 256, 0, e.stream>>>(reinterpret_cast<R*>(c.dF), reinterpret_cast<R*>(c.dq), c.Y,
+                                                    c.member_on, rows, D.M, c.norm.out_scale[0],
+                                                    c.norm.out_scale[1]);
       CUDA_CHECK(cudaGetLastError());
-      e.launches++;
-    }
+    });
+    e.launches += 3;
   }
 }
 
@@ -319,15 +357,18 @@ void enqueue_ensemble_step(TriskEnsemble& e) {
   with_modes_e(e.pv, e.ke, [&](auto pvc, auto kec) {
     constexpr int PV = decltype(pvc)::value, KE = decltype(kec)::value;
     for (int stage = 1; stage <= 4; ++stage) {
-      elaunch(e, kg_vertex<PV, KE>, e.grid[0], stage != 1, e.G, stage == 1 ? 1 : 0);
-      elaunch(e, kg_flux<PV, KE>, e.grid[1], true, e.G, stage == 1 ? 1 : 0, 0);
-      if (closure) enqueue_closure(e, stage);
-      switch (stage) {
-        case 1: elaunch(e, kg_tend<PV, EPI_STAGE1>, e.grid[2], true, e.G); break;
-        case 2: elaunch(e, kg_tend<PV, EPI_STAGE2>, e.grid[2], true, e.G); break;
-        case 3: elaunch(e, kg_tend<PV, EPI_STAGE3>, e.grid[2], true, e.G); break;
-        default: elaunch(e, kg_tend<PV, EPI_STAGE4>, e.grid[2], true, e.G); break;
-      }
+      with_real(e, [&](auto r) {
+        using R = decltype(r);
+        elaunch(e, kg_vertex<PV, KE, R>, e.grid[0], stage != 1, e.G, stage == 1 ? 1 : 0);
+        elaunch(e, kg_flux<PV, KE, R>, e.grid[1], true, e.G, stage == 1 ? 1 : 0, 0);
+        if (closure) enqueue_closure(e, stage);
+        switch (stage) {
+          case 1: elaunch(e, kg_tend<PV, EPI_STAGE1, R>, e.grid[2], true, e.G); break;
+          case 2: elaunch(e, kg_tend<PV, EPI_STAGE2, R>, e.grid[2], true, e.G); break;
+          case 3: elaunch(e, kg_tend<PV, EPI_STAGE3, R>, e.grid[2], true, e.G); break;
+          default: elaunch(e, kg_tend<PV, EPI_STAGE4, R>, e.grid[2], true, e.G); break;
+        }
+      });
     }
   });
   kg_advance<<<1, 32, 0, e.stream>>>(e.counters, e.G.n);
@@ -380,12 +421,20 @@ extern "C" {
 
 int trisk_ensemble_create(TriskModel* const* models, const int32_t* members, const double* dt,
                           const int64_t* nsteps, int32_t ngroups, TriskEnsemble** out) {
+  return trisk_ensemble_create_precision(models, members, dt, nsteps, ngroups, 64, out);
+}
+
+int trisk_ensemble_create_precision(TriskModel* const* models, const int32_t* members, const double* dt,
+                                    const int64_t* nsteps, int32_t ngroups, int32_t state_bits,
+                                    TriskEnsemble** out) {
   TRISK_API_BEGIN
   if (!models || !members || !dt || !nsteps || !out) throw Error(TRISK_ERR_ARGUMENT, "NULL argument");
   *out = nullptr;
   if (ngroups < 1 || ngroups > MAX_GROUPS)
     throw Error(TRISK_ERR_ARGUMENT, "an ensemble has 1.." + std::to_string(MAX_GROUPS) + " groups");
+  if (state_bits != 64 && state_bits != 32) throw Error(TRISK_ERR_ARGUMENT, "state_bits must be 64 or 32");
   auto e = std::make_unique<TriskEnsemble>();
+  e->fp32 = state_bits == 32;
   const TriskModel* m0 = models[0];
   if (!m0) throw Error(TRISK_ERR_ARGUMENT, "model is NULL");
   e->device = m0->device;
@@ -411,18 +460,18 @@ int trisk_ensemble_create(TriskModel* const* models, const int32_t* members, con
     D.M = (int)M;
     D.dt = dt[g];
     D.nsteps = (int)nsteps[g];
-    D.W.K = e->alloc<double>(m->nc * M);
-    D.W.B = e->alloc<double>(m->nc * M);
-    D.W.F = e->alloc<double>(m->ne * M);
-    D.W.qe = e->alloc<double>(m->ne * M);
-    D.W.zv = e->alloc<double>(m->nv * M);
-    D.W.hv = e->alloc<double>(m->nv * M);
-    D.W.qv = e->alloc<double>(m->nv * M);
-    D.W.Kv = e->alloc<double>(m->nv * M);
-    D.y = e->alloc<double>(m->N * M);
-    D.acc = e->alloc<double>(m->N * M);
-    D.st = e->alloc<double>(m->N * M);
-    CUDA_CHECK(cudaMemset(D.y, 0, m->N * M * sizeof(double)));
+    D.W.K = e->alloc_state(m->nc * M);
+    D.W.B = e->alloc_state(m->nc * M);
+    D.W.F = e->alloc_state(m->ne * M);
+    D.W.qe = e->alloc_state(m->ne * M);
+    D.W.zv = e->alloc_state(m->nv * M);
+    D.W.hv = e->alloc_state(m->nv * M);
+    D.W.qv = e->alloc_state(m->nv * M);
+    D.W.Kv = e->alloc_state(m->nv * M);
+    D.y = e->alloc_state(m->N * M);
+    D.acc = e->alloc_state(m->N * M);
+    D.st = e->alloc_state(m->N * M);
+    CUDA_CHECK(cudaMemset(D.y, 0, m->N * M * e->esize()));
     D.nV = (int)cdiv(m->nv * M, B);
     D.nEF = D.nET = (int)cdiv(m->ne * M, B);
     D.nCF = D.nCT = (int)cdiv(m->nc * M, B);
@@ -435,7 +484,7 @@ int trisk_ensemble_create(TriskModel* const* models, const int32_t* members, con
     e->models.push_back(m);
     e->max_state = std::max(e->max_state, m->N);
     e->max_members = std::max(e->max_members, (int)M);
-    const double Nb = 8.0 * (double)m->N * M;
+    const double Nb = (double)e->esize() * (double)m->N * M;
     e->step_bytes += 4 * (m->table_bytes_unique + 2 * Nb) + 15 * Nb;
   }
   e->G.n = ngroups;
@@ -455,9 +504,12 @@ int trisk_ensemble_create(TriskModel* const* models, const int32_t* members, con
   int occ[3] = {1, 1, 1};
   with_modes_e(e->pv, e->ke, [&](auto pvc, auto kec) {
     constexpr int PV = decltype(pvc)::value, KE = decltype(kec)::value;
-    CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[0], kg_vertex<PV, KE>, B, 0));
-    CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[1], kg_flux<PV, KE>, B, 0));
-    CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[2], kg_tend<PV, EPI_STAGE2>, B, 0));
+    with_real(*e, [&](auto r) {
+      using R = decltype(r);
+      CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[0], kg_vertex<PV, KE, R>, B, 0));
+      CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[1], kg_flux<PV, KE, R>, B, 0));
+      CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[2], kg_tend<PV, EPI_STAGE2, R>, B, 0));
+    });
   });
   const int total[3] = {sV, sF, sT};
   for (int p = 0; p < 3; ++p) e->grid[p] = std::max(1, std::min(total[p], dev_sms * std::max(occ[p], 1)));
@@ -482,7 +534,11 @@ int trisk_ensemble_set_member(TriskEnsemble* ens, int32_t group, int32_t member,
   } else {
     order_after_caller(e.stream, e.caller_ev);
   }
-  kg_scatter_member<<<(unsigned)cdiv(m.N, 256), 256, 0, e.stream>>>(D.y, src, m.state_n2o, m.N, D.M, member);
+  with_real(e, [&](auto r) {
+    using R = decltype(r);
+    kg_scatter_member<R><<<(unsigned)cdiv(m.N, 256), 256, 0, e.stream>>>(reinterpret_cast<R*>(D.y), src,
+                                                                         m.state_n2o, m.N, D.M, member);
+  });
   CUDA_CHECK(cudaGetLastError());
   CUDA_CHECK(cudaStreamSynchronize(e.stream));
   TRISK_API_END
@@ -498,7 +554,11 @@ int trisk_ensemble_get_member(TriskEnsemble* ens, int32_t group, int32_t member,
   const bool dev = is_device_pointer(y);
   double* dst = dev ? y : e.staging;
   if (dev) order_after_caller(e.stream, e.caller_ev);
-  kg_gather_member<<<(unsigned)cdiv(m.N, 256), 256, 0, e.stream>>>(dst, D.y, m.state_o2n, m.N, D.M, member);
+  with_real(e, [&](auto r) {
+    using R = decltype(r);
+    kg_gather_member<R><<<(unsigned)cdiv(m.N, 256), 256, 0, e.stream>>>(dst, reinterpret_cast<const R*>(D.y),
+                                                                        m.state_o2n, m.N, D.M, member);
+  });
   CUDA_CHECK(cudaGetLastError());
   if (!dev) CUDA_CHECK(cudaMemcpyAsync(y, e.staging, m.N * sizeof(double), cudaMemcpyDeviceToHost, e.stream));
   CUDA_CHECK(cudaStreamSynchronize(e.stream));
@@ -595,13 +655,13 @@ int trisk_ensemble_set_closure(TriskEnsemble* ens, int32_t group, TriskClosure* 
     c.Y = e.alloc<float>(rows * 2);
     c.geom = e.alloc<float>(m.ne * NGEOM);
     c.member_on = e.alloc<float>(D.M);
-    c.dF = e.alloc<double>(rows);
-    c.dq = e.alloc<double>(rows);
+    c.dF = e.alloc_state(rows);
+    c.dq = e.alloc_state(rows);
     std::vector<float> on(D.M, 1.0f);
     CUDA_CHECK(cudaMemcpy(c.member_on, on.data(), D.M * sizeof(float), cudaMemcpyHostToDevice));
     CUDA_CHECK(cudaMemset(c.Y, 0, rows * 2 * sizeof(float)));
-    CUDA_CHECK(cudaMemset(c.dF, 0, rows * sizeof(double)));
-    CUDA_CHECK(cudaMemset(c.dq, 0, rows * sizeof(double)));
+    CUDA_CHECK(cudaMemset(c.dF, 0, rows * e.esize()));
+    CUDA_CHECK(cudaMemset(c.dq, 0, rows * e.esize()));
   }
   D.W.dq = c.dq;
   D.W.dF = c.dF;
@@ -660,18 +720,22 @@ int trisk_ensemble_features(TriskEnsemble* ens, int32_t group, void* X, const do
   CUDA_CHECK(cudaMemcpyAsync(geom, g.data(), g.size() * sizeof(float), cudaMemcpyHostToDevice, e.stream));
   CUDA_CHECK(cudaMemcpyAsync(map, m.edge_n2o.data(), m.ne * sizeof(int32_t), cudaMemcpyHostToDevice, e.stream));
   const int B = 128;
-  with_modes_e(e.pv, e.ke, [&](auto pvc, auto kec) {
-    constexpr int PV = decltype(pvc)::value, KE = decltype(kec)::value;
-    const double* u = D.y;
-    const double* h = D.y + (size_t)m.ne * M;
-    k_vertex<PV, KE, true><<<(unsigned)cdiv(m.nv * M, B), B, 0, e.stream>>>(D.T, D.W, u, h, M, 0);
-    const int nbE = (int)cdiv(m.ne * M, B);
-    k_flux<PV, KE, true><<<(unsigned)(nbE + cdiv(m.nc * M, B)), B, 0, e.stream>>>(D.T, D.W, u, h, M, nbE, 1);
-  });
   const int64_t rows = m.ne * (int64_t)M;
   order_after_caller(e.stream, e.caller_ev);  // X may still be read by the caller
-  kg_features<<<(unsigned)cdiv(rows, 256), 256, 0, e.stream>>>(D.T, D.W, D.y, M, geom, N,
-                                                                static_cast<__nv_bfloat16*>(X), map, rows);
+  with_modes_e(e.pv, e.ke, [&](auto pvc, auto kec) {
+    constexpr int PV = decltype(pvc)::value, KE = decltype(kec)::value;
+    with_real(e, [&](auto r) {
+      using R = decltype(r);
+      const R* u = reinterpret_cast<const R*>(D.y);
+      const R* h = u + (size_t)m.ne * M;
+      const DevWorkT<R> W = work_as<R>(D.W);
+      k_vertex<PV, KE, true, R><<<(unsigned)cdiv(m.nv * M, B), B, 0, e.stream>>>(D.T, W, u, h, M, 0);
+      const int nbE = (int)cdiv(m.ne * M, B);
+      k_flux<PV, KE, true, R><<<(unsigned)(nbE + cdiv(m.nc * M, B)), B, 0, e.stream>>>(D.T, W, u, h, M, nbE, 1);
+      kg_features<R><<<(unsigned)cdiv(rows, 256), 256, 0, e.stream>>>(D.T, W, u, M, geom, N,
+                                                                       static_cast<__nv_bfloat16*>(X), map, rows);
+    });
+  });
   CUDA_CHECK(cudaGetLastError());
   CUDA_CHECK(cudaFreeAsync(geom, e.stream));
   CUDA_CHECK(cudaFreeAsync(map, e.stream));
@@ -694,14 +758,18 @@ int trisk_ensemble_energy(TriskEnsemble* ens, int32_t group, double* energies) {
   const int B = 128;
   with_modes_e(e.pv, e.ke, [&](auto pvc, auto kec) {
     constexpr int PV = decltype(pvc)::value, KE = decltype(kec)::value;
-    const double* u = D.y;
-    const double* h = D.y + (size_t)m.ne * M;
-    k_vertex<PV, KE, true><<<(unsigned)cdiv(m.nv * M, B), B, 0, e.stream>>>(D.T, D.W, u, h, M, 0);
-    const int nbE = (int)cdiv(m.ne * M, B);
-    k_flux<PV, KE, true><<<(unsigned)(nbE + cdiv(m.nc * M, B)), B, 0, e.stream>>>(D.T, D.W, u, h, M, nbE, 1);
+    with_real(e, [&](auto r) {
+      using R = decltype(r);
+      const R* u = reinterpret_cast<const R*>(D.y);
+      const R* h = u + (size_t)m.ne * M;
+      const DevWorkT<R> W = work_as<R>(D.W);
+      k_vertex<PV, KE, true, R><<<(unsigned)cdiv(m.nv * M, B), B, 0, e.stream>>>(D.T, W, u, h, M, 0);
+      const int nbE = (int)cdiv(m.ne * M, B);
+      k_flux<PV, KE, true, R><<<(unsigned)(nbE + cdiv(m.nc * M, B)), B, 0, e.stream>>>(D.T, W, u, h, M, nbE, 1);
+      kg_energy<R><<<dim3((unsigned)cdiv(m.nc, 256), (unsigned)M), 256, 0, e.stream>>>(
+          u, W.K, m.area_c, (int)m.nc, (int)m.ne, M, m.gravity, e.energy);
+    });
   });
-  kg_energy<<<dim3((unsigned)cdiv(m.nc, 256), (unsigned)M), 256, 0, e.stream>>>(D.y, D.W.K, m.area_c, (int)m.nc,
-                                                                                (int)m.ne, M, m.gravity, e.energy);
   CUDA_CHECK(cudaGetLastError());
   CUDA_CHECK(cudaMemcpyAsync(energies, e.energy, M * sizeof(double), cudaMemcpyDeviceToHost, e.stream));
   CUDA_CHECK(cudaStreamSynchronize(e.stream));

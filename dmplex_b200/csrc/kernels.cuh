@@ -82,27 +82,49 @@ struct DevTables {
   const double* vk_weights;      // VW x ldv (alpha != 1)
 };
 
-// Work vectors of one member group, [entity][member]. dq, dF: the closure's momentum-
+// Work vectors of one member group, [entity][member], stored as R (double; float for an
+// FP32-state ensemble, whose arithmetic stays FP64). dq, dF: the closure's momentum-
 // tendency and mass-flux corrections per edge (only read by the closure variant of the
 // tendency phase).
-struct DevWork {
-  double *K, *B, *F, *qe, *zv, *hv, *qv, *Kv;
-  double* dq = nullptr;
-  double* dF = nullptr;
+template <class R>
+struct DevWorkT {
+  R *K, *B, *F, *qe, *zv, *hv, *qv, *Kv;
+  R* dq = nullptr;
+  R* dF = nullptr;
 };
+using DevWork = DevWorkT<double>;
 
 // State pointers of one stage. y = [u (ne x M); h (nc x M)].
-struct DevStage {
-  const double* u;  // stage state read by the phases
-  const double* h;
-  double* y;    // base state (RK4) / unused for a plain tendency
-  double* acc;  // k1 + 2 k2 + 2 k3 accumulator
-  double* st;   // next stage state
-  double* dy;   // plain tendency output
+template <class R>
+struct DevStageT {
+  const R* u;   // stage state read by the phases
+  const R* h;
+  R* y;         // base state (RK4) / unused for a plain tendency
+  R* acc;       // k1 + 2 k2 + 2 k3 accumulator
+  R* st;        // next stage state
+  R* dy;        // plain tendency output
   double c;     // dt/2 (stages 1, 2) or dt (stage 3)
   double sixth; // dt/6
   int* flag;    // set to 1 when a non-finite state appears
 };
+using DevStage = DevStageT<double>;
+
+// The same buffers seen with storage type R (the ensemble keeps its pointers as double*).
+template <class R>
+__host__ __device__ __forceinline__ DevWorkT<R> work_as(const DevWork& W) {
+  DevWorkT<R> o;
+  o.K = reinterpret_cast<R*>(W.K);
+  o.B = reinterpret_cast<R*>(W.B);
+  o.F = reinterpret_cast<R*>(W.F);
+  o.qe = reinterpret_cast<R*>(W.qe);
+  o.zv = reinterpret_cast<R*>(W.zv);
+  o.hv = reinterpret_cast<R*>(W.hv);
+  o.qv = reinterpret_cast<R*>(W.qv);
+  o.Kv = reinterpret_cast<R*>(W.Kv);
+  o.dq = reinterpret_cast<R*>(W.dq);
+  o.dF = reinterpret_cast<R*>(W.dF);
+  return o;
+}
 
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
@@ -112,27 +134,35 @@ __device__ __forceinline__ T ldt_stream(const T* p) {  // streaming (evict-first
   return __ldcs(p);
 }
 
-__device__ __forceinline__ uint64_t l2_keep_policy() {
+__device__ __forceinline__ uint64_t l2_policy(bool keep) {
   uint64_t pol;
-  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+  if (keep)
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+  else
+    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
   return pol;
 }
-__device__ __forceinline__ double ld_keep(const double* p) {
+__device__ __forceinline__ double ld_hint(const double* p, uint64_t pol) {
   double v;
-  asm("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(l2_keep_policy()));
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
   return v;
 }
-__device__ __forceinline__ int32_t ld_keep(const int32_t* p) {
+__device__ __forceinline__ int32_t ld_hint(const int32_t* p, uint64_t pol) {
   int32_t v;
-  asm("ld.global.nc.L2::cache_hint.s32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(l2_keep_policy()));
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.s32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
   return v;
 }
 
-// Table load: L2-resident prefix (evict-last) or streaming (evict-first).
-template <class V>
-__device__ __forceinline__ V ldt(const DevTables& T, const V* p) {
-  if (reinterpret_cast<const char*>(p) < T.keep_end) return ld_keep(p);
-  return ldt_stream(p);
+// Table entry base[i]. KEEP = false: streaming load (evict-first). KEEP = true: tables that
+// start below T.keep_end (the L2-resident prefix of the packed block) load with an L2
+// evict-last policy, the others with evict-first; the choice is per table, uniform.
+template <bool KEEP, class V>
+__device__ __forceinline__ V ldt(const DevTables& T, const V* base, int i) {
+  if constexpr (KEEP) {
+    return ld_hint(base + i, l2_policy(reinterpret_cast<const char*>(base) < T.keep_end));
+  } else {
+    return ldt_stream(base + i);
+  }
 }
 
 template <bool ENS>
@@ -151,8 +181,8 @@ __device__ __forceinline__ void split(int t, int M, int& ent, int& mem) {
 // Each phase is a __device__ body over one block's worth of entities (block index vb),
 // called by the one-model kernels with vb = blockIdx.x and by the persistent ensemble
 // kernels (ensemble.cu) for every block of work they take.
-template <int PV, int KE, bool ENS>
-__device__ __forceinline__ void vertex_body(const DevTables& T, const DevWork& W, const double* u, const double* h,
+template <int PV, int KE, bool ENS, class R = double, bool KEEP = false>
+__device__ __forceinline__ void vertex_body(const DevTables& T, const DevWorkT<R>& W, const R* u, const R* h,
                                             int M, int want_qv, int vb) {
   int v, mm;
   split<ENS>(vb * blockDim.x + threadIdx.x, M, v, mm);
@@ -162,14 +192,14 @@ __device__ __forceinline__ void vertex_body(const DevTables& T, const DevWork& W
   double cor = 0.0;
 #pragma unroll
   for (int k = 0; k < VW; ++k) {
-    ve[k] = ldt(T, T.vertex_edges + k * T.ldv + v);
-    cu[k] = ldt(T, T.curl + k * T.ldv + v);
-    vc[k] = ldt(T, T.vertex_cells + k * T.ldv + v);
-    vh[k] = ldt(T, T.vertex_height + k * T.ldv + v);
-    if (KE != KE_CELL) vkw[k] = ldt(T, T.vk_weights + k * T.ldv + v);
+    ve[k] = ldt<KEEP>(T, T.vertex_edges, k * T.ldv + v);
+    cu[k] = ldt<KEEP>(T, T.curl, k * T.ldv + v);
+    vc[k] = ldt<KEEP>(T, T.vertex_cells, k * T.ldv + v);
+    vh[k] = ldt<KEEP>(T, T.vertex_height, k * T.ldv + v);
+    if (KE != KE_CELL) vkw[k] = ldt<KEEP>(T, T.vk_weights, k * T.ldv + v);
   }
   const bool qv = PV == PVM_TRISK || want_qv;
-  if (qv) cor = ldt(T, T.coriolis + v);
+  if (qv) cor = ldt<KEEP>(T, T.coriolis, v);
   pdl_wait();
   double uu[VW], hh[VW];
 #pragma unroll
@@ -183,51 +213,51 @@ __device__ __forceinline__ void vertex_body(const DevTables& T, const DevWork& W
 #pragma unroll
   for (int k = 0; k < VW; ++k) eta += vh[k] * hh[k];
   const size_t o = (size_t)v * M + mm;
-  W.zv[o] = z;
-  W.hv[o] = eta;
-  if (qv) W.qv[o] = (z + cor) / eta;
+  W.zv[o] = (R)z;
+  W.hv[o] = (R)eta;
+  if (qv) W.qv[o] = (R)((z + cor) / eta);
   if (KE != KE_CELL) {
     double s = 0.0;
 #pragma unroll
     for (int k = 0; k < VW; ++k) s += vkw[k] * (uu[k] * uu[k]);
-    W.Kv[o] = s;
+    W.Kv[o] = (R)s;
   }
 }
 
-template <int PV, int KE, bool ENS>
-__global__ void __launch_bounds__(256) k_vertex(DevTables T, DevWork W, const double* u, const double* h, int M,
+template <int PV, int KE, bool ENS, class R = double, bool KEEP = false>
+__global__ void __launch_bounds__(256) k_vertex(DevTables T, DevWorkT<R> W, const R* u, const R* h, int M,
                                                 int want_qv) {
   pdl_trigger();
-  vertex_body<PV, KE, ENS>(T, W, u, h, M, want_qv, blockIdx.x);
+  vertex_body<PV, KE, ENS, R, KEEP>(T, W, u, h, M, want_qv, blockIdx.x);
 }
 
 // ------------------------------------------------------------------------------------
 // phase 2: edges (mass flux, edge PV) and cells (Bernoulli function); blocks [0, nbE)
 // take edges, the rest cells
-template <int PV, int KE, bool ENS>
-__device__ __forceinline__ void flux_body(const DevTables& T, const DevWork& W, const double* u, const double* h,
+template <int PV, int KE, bool ENS, class R = double, bool KEEP = false>
+__device__ __forceinline__ void flux_body(const DevTables& T, const DevWorkT<R>& W, const R* u, const R* h,
                                           int M, int nbE, int want_K, int vb) {
   if (vb < nbE) {
     int e, mm;
     split<ENS>(vb * blockDim.x + threadIdx.x, M, e, mm);
     if (e >= T.ne) return;
-    const int ev0 = ldt(T, T.edge_vertices + e), ev1 = ldt(T, T.edge_vertices + T.lde + e);
+    const int ev0 = ldt<KEEP>(T, T.edge_vertices, e), ev1 = ldt<KEEP>(T, T.edge_vertices, T.lde + e);
     int ec0 = 0, ec1 = 0;
     double eh0 = 0, eh1 = 0, vk0 = 0, vk1 = 0, r0 = 0, r1 = 0, gc = 0;
     if (KE != KE_VERTEX) {
-      ec0 = ldt(T, T.edge_cells + e);
-      ec1 = ldt(T, T.edge_cells + T.lde + e);
-      eh0 = ldt(T, T.edge_height + e);
-      eh1 = ldt(T, T.edge_height + T.lde + e);
+      ec0 = ldt<KEEP>(T, T.edge_cells, e);
+      ec1 = ldt<KEEP>(T, T.edge_cells, T.lde + e);
+      eh0 = ldt<KEEP>(T, T.edge_height, e);
+      eh1 = ldt<KEEP>(T, T.edge_height, T.lde + e);
     }
     if (KE != KE_CELL) {
-      vk0 = ldt(T, T.vk_height + e);
-      vk1 = ldt(T, T.vk_height + T.lde + e);
+      vk0 = ldt<KEEP>(T, T.vk_height, e);
+      vk1 = ldt<KEEP>(T, T.vk_height, T.lde + e);
     }
     if (PV != PVM_TRISK) {
-      r0 = ldt(T, T.rhombus + e);
-      r1 = ldt(T, T.rhombus + T.lde + e);
-      gc = ldt(T, T.g_coriolis + e);
+      r0 = ldt<KEEP>(T, T.rhombus, e);
+      r1 = ldt<KEEP>(T, T.rhombus, T.lde + e);
+      gc = ldt<KEEP>(T, T.g_coriolis, e);
     }
     pdl_wait();
     const size_t o = (size_t)e * M + mm;
@@ -246,13 +276,15 @@ __device__ __forceinline__ void flux_body(const DevTables& T, const DevWork& W, 
     } else {
       he = eh0 * h[(size_t)ec0 * M + mm] + eh1 * h[(size_t)ec1 * M + mm] + vk0 * hv0 + vk1 * hv1;
     }
-    W.F[o] = he * ue;
+    W.F[o] = (R)(he * ue);
     if (PV == PVM_TRISK) {
-      W.qe[o] = (W.qv[o0] + W.qv[o1]) / 2;
+      const double qa = W.qv[o0], qb = W.qv[o1];
+      W.qe[o] = (R)((qa + qb) / 2);
     } else {
-      const double z = r0 * W.zv[o0] + r1 * W.zv[o1];
+      const double za = W.zv[o0], zb = W.zv[o1];
+      const double z = r0 * za + r1 * zb;
       const double eta = r0 * hv0 + r1 * hv1;
-      W.qe[o] = (z + gc) / eta;
+      W.qe[o] = (R)((z + gc) / eta);
     }
   } else {
     int i, mm;
@@ -263,12 +295,12 @@ __device__ __forceinline__ void flux_body(const DevTables& T, const DevWork& W, 
 #pragma unroll
     for (int k = 0; k < CW; ++k) {
       if (KE != KE_VERTEX) {
-        ce[k] = ldt(T, T.cell_edges + k * T.ldc + i);
-        kin[k] = ldt(T, T.kinetic + k * T.ldc + i);
+        ce[k] = ldt<KEEP>(T, T.cell_edges, k * T.ldc + i);
+        kin[k] = ldt<KEEP>(T, T.kinetic, k * T.ldc + i);
       }
       if (KE != KE_CELL) {
-        cv[k] = ldt(T, T.cell_vertices + k * T.ldc + i);
-        kk[k] = ldt(T, T.vk_kites + k * T.ldc + i);
+        cv[k] = ldt<KEEP>(T, T.cell_vertices, k * T.ldc + i);
+        kk[k] = ldt<KEEP>(T, T.vk_kites, k * T.ldc + i);
       }
     }
     pdl_wait();
@@ -295,46 +327,49 @@ __device__ __forceinline__ void flux_body(const DevTables& T, const DevWork& W, 
       K += s;
       B += s;
     }
-    W.B[o] = B;
-    if (want_K) W.K[o] = K;
+    W.B[o] = (R)B;
+    if (want_K) W.K[o] = (R)K;
   }
 }
 
-template <int PV, int KE, bool ENS>
-__global__ void __launch_bounds__(256) k_flux(DevTables T, DevWork W, const double* u, const double* h, int M,
+template <int PV, int KE, bool ENS, class R = double, bool KEEP = false>
+__global__ void __launch_bounds__(256) k_flux(DevTables T, DevWorkT<R> W, const R* u, const R* h, int M,
                                               int nbE, int want_K) {
   pdl_trigger();
-  flux_body<PV, KE, ENS>(T, W, u, h, M, nbE, want_K, blockIdx.x);
+  flux_body<PV, KE, ENS, R, KEEP>(T, W, u, h, M, nbE, want_K, blockIdx.x);
 }
 
 // ------------------------------------------------------------------------------------
 // phase 3: tendencies and the RK4 stage update
-template <int EPI>
-__device__ __forceinline__ void epilogue(const DevStage& S, size_t j, double kv) {
+template <int EPI, class R = double>
+__device__ __forceinline__ void epilogue(const DevStageT<R>& S, size_t j, double kv) {
   if (EPI == EPI_TENDENCY) {
-    S.dy[j] = kv;
+    S.dy[j] = (R)kv;
   } else if (EPI == EPI_STAGE1) {
-    S.acc[j] = kv;
-    S.st[j] = S.y[j] + S.c * kv;
+    const double y = S.y[j];
+    S.acc[j] = (R)kv;
+    S.st[j] = (R)(y + S.c * kv);
   } else if (EPI == EPI_STAGE2 || EPI == EPI_STAGE3) {
-    S.acc[j] = S.acc[j] + 2 * kv;
-    S.st[j] = S.y[j] + S.c * kv;
+    const double y = S.y[j], a = S.acc[j];
+    S.acc[j] = (R)(a + 2 * kv);
+    S.st[j] = (R)(y + S.c * kv);
   } else {
-    const double yn = S.y[j] + S.sixth * (S.acc[j] + kv);
+    const double y = S.y[j], a = S.acc[j];
+    const R yn = (R)(y + S.sixth * (a + kv));
     S.y[j] = yn;
     if (!isfinite(yn)) atomicOr(S.flag, 1);
   }
 }
 
-template <int PV, int EPI, bool ENS, bool CL = false>
-__device__ __forceinline__ void tend_body(const DevTables& T, const DevWork& W, const DevStage& S, int M, int nbE,
-                                          int vb) {
+template <int PV, int EPI, bool ENS, bool CL = false, class R = double, bool KEEP = false>
+__device__ __forceinline__ void tend_body(const DevTables& T, const DevWorkT<R>& W, const DevStageT<R>& S, int M,
+                                          int nbE, int vb) {
   if (vb < nbE) {
     int e, mm;
     split<ENS>(vb * blockDim.x + threadIdx.x, M, e, mm);
     if (e >= T.ne) return;
-    const int ec0 = ldt(T, T.edge_cells + e), ec1 = ldt(T, T.edge_cells + T.lde + e);
-    const double invd = ldt(T, T.inverse_dual + e);
+    const int ec0 = ldt<KEEP>(T, T.edge_cells, e), ec1 = ldt<KEEP>(T, T.edge_cells, T.lde + e);
+    const double invd = ldt<KEEP>(T, T.inverse_dual, e);
     const size_t o = (size_t)e * M + mm;
     double du;
     if (PV == PVM_TRISK) {
@@ -342,8 +377,8 @@ __device__ __forceinline__ void tend_body(const DevTables& T, const DevWork& W, 
       double tr[TWD];
 #pragma unroll
       for (int k = 0; k < TWD; ++k) {
-        te[k] = ldt(T, T.trisk_edges + k * T.lde + e);
-        tr[k] = ldt(T, T.trisk + k * T.lde + e);
+        te[k] = ldt<KEEP>(T, T.trisk_edges, k * T.lde + e);
+        tr[k] = ldt<KEEP>(T, T.trisk, k * T.lde + e);
       }
       pdl_wait();
       const double qself = W.qe[o];
@@ -356,15 +391,15 @@ __device__ __forceinline__ void tend_body(const DevTables& T, const DevWork& W, 
       double s = 0.0;
 #pragma unroll
       for (int k = 0; k < TWD; ++k) s += tr[k] * f[k] * (qself + q[k]);
-      du = s / 2 - (W.B[(size_t)ec1 * M + mm] - W.B[(size_t)ec0 * M + mm]) * invd;
+      du = s / 2 - ((double)W.B[(size_t)ec1 * M + mm] - (double)W.B[(size_t)ec0 * M + mm]) * invd;
     } else {
       int ge[GW], gp[GW];
       double gw[GW];
 #pragma unroll
       for (int k = 0; k < GW; ++k) {
-        ge[k] = ldt(T, T.g_edges + k * T.lde + e);
-        if (PV == PVM_GASSMANN) gp[k] = ldt(T, T.g_pv_edges + k * T.lde + e);
-        gw[k] = ldt(T, T.g_weights + k * T.lde + e);
+        ge[k] = ldt<KEEP>(T, T.g_edges, k * T.lde + e);
+        if (PV == PVM_GASSMANN) gp[k] = ldt<KEEP>(T, T.g_pv_edges, k * T.lde + e);
+        gw[k] = ldt<KEEP>(T, T.g_weights, k * T.lde + e);
       }
       pdl_wait();
       double f[GW], q[GW];
@@ -389,10 +424,10 @@ __device__ __forceinline__ void tend_body(const DevTables& T, const DevWork& W, 
       double s = 0.0;
 #pragma unroll
       for (int k = 0; k < GW; ++k) s += gw[k] * f[k] * q[k];
-      du = s - (W.B[(size_t)ec1 * M + mm] - W.B[(size_t)ec0 * M + mm]) * invd;
+      du = s - ((double)W.B[(size_t)ec1 * M + mm] - (double)W.B[(size_t)ec0 * M + mm]) * invd;
     }
-    if (CL) du += W.dq[o];  // learned momentum correction
-    epilogue<EPI>(S, o, du);
+    if (CL) du += (double)W.dq[o];  // learned momentum correction
+    epilogue<EPI, R>(S, o, du);
   } else {
     int i, mm;
     split<ENS>((vb - nbE) * blockDim.x + threadIdx.x, M, i, mm);
@@ -401,28 +436,28 @@ __device__ __forceinline__ void tend_body(const DevTables& T, const DevWork& W, 
     double dv[CW];
 #pragma unroll
     for (int k = 0; k < CW; ++k) {
-      ce[k] = ldt(T, T.cell_edges + k * T.ldc + i);
-      dv[k] = ldt(T, T.divergence + k * T.ldc + i);
+      ce[k] = ldt<KEEP>(T, T.cell_edges, k * T.ldc + i);
+      dv[k] = ldt<KEEP>(T, T.divergence, k * T.ldc + i);
     }
     pdl_wait();
     double f[CW];
 #pragma unroll
     for (int k = 0; k < CW; ++k) {
       f[k] = W.F[(size_t)ce[k] * M + mm];
-      if (CL) f[k] += W.dF[(size_t)ce[k] * M + mm];  // learned mass-flux correction
+      if (CL) f[k] += (double)W.dF[(size_t)ce[k] * M + mm];  // learned mass-flux correction
     }
     double s = 0.0;
 #pragma unroll
     for (int k = 0; k < CW; ++k) s += dv[k] * f[k];
     const size_t o = (size_t)i * M + mm;
-    epilogue<EPI>(S, (size_t)T.ne * M + o, -s);
+    epilogue<EPI, R>(S, (size_t)T.ne * M + o, -s);
   }
 }
 
-template <int PV, int EPI, bool ENS>
+template <int PV, int EPI, bool ENS, bool KEEP = false>
 __global__ void __launch_bounds__(256) k_tend(DevTables T, DevWork W, DevStage S, int M, int nbE) {
   pdl_trigger();
-  tend_body<PV, EPI, ENS>(T, W, S, M, nbE, blockIdx.x);
+  tend_body<PV, EPI, ENS, false, double, KEEP>(T, W, S, M, nbE, blockIdx.x);
 }
 
 }  // namespace trisk

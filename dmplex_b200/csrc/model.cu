@@ -166,27 +166,35 @@ void with_modes(int pv, int ke, F&& f) {
 }
 
 // One tendency: three phase launches. ev: optional 6 events (pairs around each launch).
+// With an L2-resident table prefix the kernels' KEEP variants run (per-table L2 policies).
 void enqueue_tendency(TriskModel& m, const DevStage& S, int epi, cudaEvent_t* ev = nullptr) {
   const int bV = m.block[0], bF = m.block[1], bT = m.block[2];
   const int64_t nbV = cdiv(m.nv, bV);
   const int64_t nbEF = cdiv(m.ne, bF), nbCF = cdiv(m.nc, bF);
   const int64_t nbET = cdiv(m.ne, bT), nbCT = cdiv(m.nc, bT);
-  with_modes(m.pv, m.ke, [&](auto pvc, auto kec) {
+  auto body = [&](auto pvc, auto kec, auto keepc) {
     constexpr int PV = decltype(pvc)::value, KE = decltype(kec)::value;
-    launch(m, k_vertex<PV, KE, false>, nbV, bV, ev ? ev[0] : nullptr, ev ? ev[1] : nullptr, m.T, m.W, S.u, S.h, 1,
-           0);
-    launch(m, k_flux<PV, KE, false>, nbEF + nbCF, bF, ev ? ev[2] : nullptr, ev ? ev[3] : nullptr, m.T, m.W, S.u,
-           S.h, 1, (int)nbEF, 0);
+    constexpr bool K = decltype(keepc)::value;
+    launch(m, k_vertex<PV, KE, false, double, K>, nbV, bV, ev ? ev[0] : nullptr, ev ? ev[1] : nullptr, m.T, m.W, S.u,
+           S.h, 1, 0);
+    launch(m, k_flux<PV, KE, false, double, K>, nbEF + nbCF, bF, ev ? ev[2] : nullptr, ev ? ev[3] : nullptr, m.T,
+           m.W, S.u, S.h, 1, (int)nbEF, 0);
     cudaEvent_t e0 = ev ? ev[4] : nullptr, e1 = ev ? ev[5] : nullptr;
     const int64_t g = nbET + nbCT;
     const int nbE = (int)nbET;
     switch (epi) {
-      case EPI_TENDENCY: launch(m, k_tend<PV, EPI_TENDENCY, false>, g, bT, e0, e1, m.T, m.W, S, 1, nbE); break;
-      case EPI_STAGE1: launch(m, k_tend<PV, EPI_STAGE1, false>, g, bT, e0, e1, m.T, m.W, S, 1, nbE); break;
-      case EPI_STAGE2: launch(m, k_tend<PV, EPI_STAGE2, false>, g, bT, e0, e1, m.T, m.W, S, 1, nbE); break;
-      case EPI_STAGE3: launch(m, k_tend<PV, EPI_STAGE3, false>, g, bT, e0, e1, m.T, m.W, S, 1, nbE); break;
-      default: launch(m, k_tend<PV, EPI_STAGE4, false>, g, bT, e0, e1, m.T, m.W, S, 1, nbE); break;
+      case EPI_TENDENCY: launch(m, k_tend<PV, EPI_TENDENCY, false, K>, g, bT, e0, e1, m.T, m.W, S, 1, nbE); break;
+      case EPI_STAGE1: launch(m, k_tend<PV, EPI_STAGE1, false, K>, g, bT, e0, e1, m.T, m.W, S, 1, nbE); break;
+      case EPI_STAGE2: launch(m, k_tend<PV, EPI_STAGE2, false, K>, g, bT, e0, e1, m.T, m.W, S, 1, nbE); break;
+      case EPI_STAGE3: launch(m, k_tend<PV, EPI_STAGE3, false, K>, g, bT, e0, e1, m.T, m.W, S, 1, nbE); break;
+      default: launch(m, k_tend<PV, EPI_STAGE4, false, K>, g, bT, e0, e1, m.T, m.W, S, 1, nbE); break;
     }
+  };
+  with_modes(m.pv, m.ke, [&](auto pvc, auto kec) {
+    if (m.l2_keep_bytes > 0)
+      body(pvc, kec, std::true_type{});
+    else
+      body(pvc, kec, std::false_type{});
   });
 }
 
@@ -996,41 +1004,62 @@ int trisk_autotune(TriskModel* model, double* y, double dt, int32_t steps, doubl
   if (!y || steps <= 0) throw Error(TRISK_ERR_ARGUMENT, "bad argument");
   DeviceGuard guard(m.device);
   if (!is_device_pointer(y)) throw Error(TRISK_ERR_ARGUMENT, "trisk_autotune needs a device state");
-  // Times `steps` RK4 steps (graph + PDL as configured) for every combination of the
-  // three phase block sizes and keeps the fastest. Every candidate computes the same
-  // numbers; the state is restored from the caller's copy before each trial.
+  // Times `steps` RK4 steps (graph + PDL as configured) for every combination of the three
+  // phase block sizes, then for L2-resident table prefixes of several sizes with the best
+  // blocks, then the blocks again with the best prefix, and keeps the fastest. Every
+  // candidate computes the same numbers; the state is restored from the caller's copy
+  // before each trial. A persisting window, if one was set, is left off.
   static const int choices[] = {64, 128, 256};
+  static const int keep_mb[] = {0, 8, 16, 24, 32, 40, 48, 64};
   cudaEvent_t e0, e1;
   CUDA_CHECK(cudaEventCreate(&e0));
   CUDA_CHECK(cudaEventCreate(&e1));
+  int l2 = 0;
+  CUDA_CHECK(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, m.device));
   int best[3] = {m.block[0], m.block[1], m.block[2]};
+  size_t best_keep = 0;
   double best_t = INFINITY;
-  try {
+  auto trial = [&](int a, int b, int c, size_t keep) {
+    m.block[0] = a;
+    m.block[1] = b;
+    m.block[2] = c;
+    m.l2_keep_bytes = keep;
+    m.l2_window = false;
+    m.T.keep_end = keep ? m.table_base + keep : nullptr;
+    if (m.graph) {
+      cudaGraphExecDestroy(m.graph);
+      m.graph = nullptr;
+    }
+    state_in(m, y, m.y);
+    run_steps(m, dt, 2);  // warm-up (and graph capture)
+    CUDA_CHECK(cudaEventRecord(e0, m.stream));
+    run_steps(m, dt, steps);
+    CUDA_CHECK(cudaEventRecord(e1, m.stream));
+    CUDA_CHECK(cudaEventSynchronize(e1));
+    float ms = 0;
+    CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+    if (ms < best_t) {
+      best_t = ms;
+      best[0] = a;
+      best[1] = b;
+      best[2] = c;
+      best_keep = keep;
+    }
+  };
+  auto blocks_pass = [&](size_t keep) {
     for (int a : choices)
       for (int b : choices)
-        for (int c : choices) {
-          m.block[0] = a;
-          m.block[1] = b;
-          m.block[2] = c;
-          if (m.graph) {
-            cudaGraphExecDestroy(m.graph);
-            m.graph = nullptr;
-          }
-          state_in(m, y, m.y);
-          run_steps(m, dt, 2);  // warm-up (and graph capture)
-          CUDA_CHECK(cudaEventRecord(e0, m.stream));
-          run_steps(m, dt, steps);
-          CUDA_CHECK(cudaEventRecord(e1, m.stream));
-          CUDA_CHECK(cudaEventSynchronize(e1));
-          float ms = 0;
-          CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
-          if (ms < best_t) {
-            best_t = ms;
-            best[0] = a;
-            best[1] = b;
-            best[2] = c;
-          }
-        }
+        for (int c : choices) trial(a, b, c, keep);
+  };
+  try {
+    blocks_pass(0);
+    const int b0 = best[0], b1 = best[1], b2 = best[2];
+    for (int mb : keep_mb) {
+      const size_t keep = (size_t)mb << 20;
+      if (mb == 0 || keep >= m.table_block_bytes || keep > (size_t)l2 / 2) continue;
+      trial(b0, b1, b2, keep);
+    }
+    if (best_keep) blocks_pass(best_keep);
   } catch (...) {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -1039,6 +1068,9 @@ int trisk_autotune(TriskModel* model, double* y, double dt, int32_t steps, doubl
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   for (int p = 0; p < 3; ++p) m.block[p] = best[p];
+  m.l2_keep_bytes = best_keep;
+  m.l2_window = false;
+  m.T.keep_end = best_keep ? m.table_base + best_keep : nullptr;
   if (m.graph) {
     cudaGraphExecDestroy(m.graph);
     m.graph = nullptr;
@@ -1046,6 +1078,15 @@ int trisk_autotune(TriskModel* model, double* y, double dt, int32_t steps, doubl
   CUDA_CHECK(cudaMemsetAsync(m.flag, 0, sizeof(int), m.stream));
   CUDA_CHECK(cudaStreamSynchronize(m.stream));
   if (best_ms) *best_ms = best_t / steps;
+  TRISK_API_END
+}
+
+int trisk_model_get_l2_residency(TriskModel* model, int64_t* bytes, int32_t* window) {
+  TRISK_API_BEGIN
+  TriskModel& m = *checked(model);
+  if (!bytes || !window) throw Error(TRISK_ERR_ARGUMENT, "NULL argument");
+  *bytes = (int64_t)m.l2_keep_bytes;
+  *window = m.l2_window ? 1 : 0;
   TRISK_API_END
 }
 

@@ -15,18 +15,20 @@ from .model import TRiSKShallowWater, _state
 
 class Ensemble:
     """groups: a list of (model, members, dt, nsteps). Members of a group share the model's
-    tables; every group has its own time step and number of RK4 steps."""
+    tables; every group has its own time step and number of RK4 steps. state_bits = 32
+    stores the members' states and work vectors as float (the arithmetic stays FP64)."""
 
-    def __init__(self, groups):
+    def __init__(self, groups, state_bits: int = 64):
         self.groups = list(groups)
+        self.state_bits = int(state_bits)
         n = len(self.groups)
         models = (C.c_void_p * n)(*[g[0].handle.value for g in self.groups])
         members = np.array([g[1] for g in self.groups], dtype=np.int32)
         dts = np.array([g[2] for g in self.groups], dtype=np.float64)
         steps = np.array([g[3] for g in self.groups], dtype=np.int64)
         handle = C.c_void_p()
-        check(lib.trisk_ensemble_create(models, members.ctypes.data, dts.ctypes.data, steps.ctypes.data, n,
-                                        C.byref(handle)))
+        check(lib.trisk_ensemble_create_precision(models, members.ctypes.data, dts.ctypes.data, steps.ctypes.data,
+                                                  n, self.state_bits, C.byref(handle)))
         self._h = handle
         self._models = [g[0] for g in self.groups]  # the ensemble uses their device tables
 

@@ -130,10 +130,14 @@ class TRiSKShallowWater:
         block = np.zeros(3, dtype=np.int32)
         saved = C.c_double()
         check(lib.trisk_model_info(self._h, C.byref(pv), block.ctypes.data, C.byref(saved)))
-        return {"pv_mode": pv.value, "block": block.tolist(), "derived_pv_bytes_saved": saved.value}
+        keep, window = C.c_int64(), C.c_int32()
+        check(lib.trisk_model_get_l2_residency(self._h, C.byref(keep), C.byref(window)))
+        return {"pv_mode": pv.value, "block": block.tolist(), "derived_pv_bytes_saved": saved.value,
+                "l2_resident_table_bytes": keep.value, "l2_window": bool(window.value)}
 
     def autotune(self, y_device, dt: float, steps: int = 20) -> float:
-        """Picks the fastest phase block sizes for this mesh and scheme; returns ms/step."""
+        """Picks the fastest phase block sizes and L2-resident table prefix for this mesh and
+        scheme; returns ms/step."""
         best = C.c_double()
         check(lib.trisk_autotune(self._h, ptr(y_device), float(dt), int(steps), C.byref(best)))
         return best.value

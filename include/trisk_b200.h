@@ -205,8 +205,10 @@ int trisk_model_bytes(TriskModel* model, double out[4]);
  * the derived PV edges save. No reference counterpart (implementation detail). */
 int trisk_model_info(TriskModel* model, int32_t* pv_mode, int32_t block[3], double* derived_saving);
 /* Autotuner (no reference counterpart): times `steps` RK4 steps of the device state y (left
- * unchanged) for every combination of the phase block sizes {64, 128, 256} and keeps the
- * fastest in the model; best_ms gets its time per step. */
+ * unchanged) for every combination of the phase block sizes {64, 128, 256}, then L2-resident
+ * table prefixes of 8..64 MB (trisk_model_set_l2_residency, no window) with the best blocks,
+ * then the blocks again with the best prefix, and keeps the fastest in the model; best_ms
+ * gets its time per step. */
 int trisk_autotune(TriskModel* model, double* y_device, double dt, int32_t steps, double* best_ms);
 /* Sets the threads per block of the three phases (vertex, flux, tend), each a multiple of 32
  * in [64, 256], as an autotuner result found earlier (no reference counterpart). */
@@ -219,6 +221,7 @@ int trisk_model_set_block(TriskModel* model, const int32_t block[3]);
  * context's persisting-L2 limit, at most cudaDevAttrMaxPersistingL2CacheSize). bytes = 0:
  * all tables stream (the default). Results are unchanged. */
 int trisk_model_set_l2_residency(TriskModel* model, int64_t bytes, int32_t window);
+int trisk_model_get_l2_residency(TriskModel* model, int64_t* bytes, int32_t* window);
 /* L2 size, largest persisting-L2 set-aside, largest access-policy window and the current
  * persisting-L2 limit of a device, in bytes. */
 int trisk_l2_info(int32_t device, int64_t info[4]);
@@ -237,6 +240,13 @@ int trisk_profile_phases(TriskModel* model, double* y_device, double dt, int64_t
 typedef struct TriskEnsemble TriskEnsemble;
 int trisk_ensemble_create(TriskModel* const* models, const int32_t* members, const double* dt,
                           const int64_t* nsteps, int32_t ngroups, TriskEnsemble** out);
+/* As trisk_ensemble_create with the members' state, RK4 stage vectors and work vectors
+ * stored in state_bits = 64 (FP64, bit for bit rk4_step!) or 32 (FP32 storage: every value
+ * is rounded to float when stored, the arithmetic stays FP64, the tables stay FP64, and the
+ * energy sums are FP64). set/get_member still exchange FP64 states. */
+int trisk_ensemble_create_precision(TriskModel* const* models, const int32_t* members, const double* dt,
+                                    const int64_t* nsteps, int32_t ngroups, int32_t state_bits,
+                                    TriskEnsemble** out);
 void trisk_ensemble_destroy(TriskEnsemble* ensemble);
 /* Member state y = [u; h] in file numbering, host or device memory. */
 int trisk_ensemble_set_member(TriskEnsemble* ensemble, int32_t group, int32_t member, const double* y);
@@ -259,10 +269,12 @@ int trisk_ensemble_energy(TriskEnsemble* ensemble, int32_t group, double* energi
  * stage 1 of each RK4 step, its output reused by the other stages, or at every stage), and
  * every tendency adds, for members whose mask entry is 1, dF_e = sF y0 to the mass flux of
  * the continuity equation only (dh_i/dt = -sum_k div[i,k] (F + dF); flux form, so mass is
- * conserved; the PV flux keeps the resolved F) and du_e += sQ y1 to the momentum tendency. Features per row: u_e, u
- * at the 10 TRiSK stencil edges, h at the two cells, q at the two vertices, K at the two
- * cells, 7 geometry values (`geometry`, ne x 7 in file edge order); normalized as
- * (x - mean) * scale with norm = [24 means, 24 scales, sF, sQ]. TRiSK PV flux only.
+ * conserved; the PV flux keeps the resolved F) and du_e += sQ y1 to the momentum tendency.
+ * Features per row, formed in FP64: u_e; u at the 10 TRiSK stencil edges minus u_e; mean and
+ * difference (second minus first) of h at the two cells, of q at the two vertices and of K
+ * at the two cells; 7 geometry values (`geometry`, ne x 7 in file edge order); normalized
+ * as (x - mean) * scale with norm = [24 means, 24 scales, sF, sQ], then rounded to BF16.
+ * TRiSK PV flux only.
  * net = NULL removes the group's closure. */
 int trisk_ensemble_set_closure(TriskEnsemble* ensemble, int32_t group, TriskClosure* net, const float* geometry,
                                const double* norm, int32_t every_stage);

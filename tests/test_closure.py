@@ -79,3 +79,53 @@ def test_training_reduces_loss(require_gpu):
     for _ in range(300):
         last = mlp.train_step(Xd, Td, 3e-3)
     assert np.isfinite(last) and last < 0.1 * first
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("state_bits", [64, 32])
+def test_ensemble_features_match_oracle(require_gpu, state_bits):
+    """The closure's 24 inputs from an ensemble's member states against the same quantities
+    built from the CPU oracle's work vectors (K via B - g h, q at the vertices), rounded to
+    BF16 like the kernel; exact."""
+    import torch
+    import dmplex_b200 as d
+    from dmplex_b200 import workloads as w
+    from dmplex_b200.coarsen import edge_geometry
+    from oracle.oracle import Oracle
+    from conftest import tables, trisk_grid
+    si = w.si_parameters()
+    g = trisk_grid(3, True)
+    t = tables(3, "trisk", "cell", True, None, **si)
+    m = d.TRiSKShallowWater(g, pv_flux="trisk", kinetic_energy="cell", **si)
+    o = Oracle(t)
+    states = w.ensemble_members(g, 2, 3, degree=6)
+    if state_bits == 32:  # the ensemble stores float: the oracle sees the rounded states
+        states = [y.astype(np.float32).astype(np.float64) for y in states]
+    ens = d.Ensemble([(m, 2, 100.0, 1)], state_bits=state_bits)
+    for k, y in enumerate(states):
+        ens.set_member(0, k, y)
+    geom = edge_geometry(g)
+    norm = np.concatenate([np.zeros(24), np.ones(24), [1.0, 1.0]])
+    X = torch.empty((g.ne * 2, 24), dtype=torch.bfloat16, device="cuda")
+    ens.features(0, X, norm, geom)
+    got = X.float().cpu().numpy().astype(np.float64).reshape(g.ne, 2, 24)
+    ne = g.ne
+    te, tw = t["trisk_edges"] - 1, t["trisk"]
+    ec, ev = t["edge_cells"] - 1, t["edge_vertices"] - 1
+    for k, y in enumerate(states):
+        o.tendency(y)
+        wk = o.work()
+        if state_bits == 32:  # the ensemble stores its work vectors as float too
+            wk = {key: v.astype(np.float32).astype(np.float64) for key, v in wk.items()}
+        u, h = y[:ne], y[ne:]
+        h0, h1 = h[ec[:, 0]], h[ec[:, 1]]
+        q0, q1 = wk["qv"][ev[:, 0]], wk["qv"][ev[:, 1]]
+        K0, K1 = wk["B"][ec[:, 0]] - t["gravity"] * h0, wk["B"][ec[:, 1]] - t["gravity"] * h1
+        f = np.zeros((ne, 24))
+        f[:, 0] = u
+        f[:, 1:11] = np.where(tw != 0, u[te] - u[:, None], 0.0)
+        f[:, 11], f[:, 12] = (h0 + h1) / 2, h1 - h0
+        f[:, 13], f[:, 14] = (q0 + q1) / 2, q1 - q0
+        f[:, 15], f[:, 16] = (K0 + K1) / 2, K1 - K0
+        f[:, 17:] = geom
+        assert np.array_equal(got[:, k, :], co.bf16(f))

@@ -111,3 +111,40 @@ def test_ensemble_nonfinite_member(require_gpu):
     ref = ys[0].copy()
     d.rk4_step(ref, 0.001, d.tendency, d.RK4Cache(ref), m, nsteps=2)
     assert np.array_equal(ens.get_member(0, 0), ref)  # the other member is unaffected
+
+
+@pytest.mark.parametrize("pv,ke", [("trisk", "cell"), ("gassmann", "vertex")])
+def test_fp32_state_ensemble(require_gpu, pv, ke):
+    """FP32 storage of state and work vectors (FP64 arithmetic and tables): set/get round to
+    float exactly, 20 steps stay within float rounding of the FP64 ensemble, mass is
+    conserved to float rounding, and a non-finite member is still reported."""
+    si = w.si_parameters()
+    g = trisk_grid(4, True)
+    m = d.TRiSKShallowWater(g, pv_flux=pv, kinetic_energy=ke, **si)
+    dt = w.courant_dt(g)
+    states = member_states(g, 3, 11)
+    e64 = d.Ensemble([(m, 3, dt, 20)])
+    e32 = d.Ensemble([(m, 3, dt, 20)], state_bits=32)
+    for k, y in enumerate(states):
+        e64.set_member(0, k, y)
+        e32.set_member(0, k, y)
+        assert np.array_equal(e32.get_member(0, k), y.astype(np.float32).astype(np.float64))
+    e64.run(20)
+    e32.run(20)
+    ne = g.ne
+    for k in range(3):
+        a, b = e64.get_member(0, k), e32.get_member(0, k)
+        assert np.isfinite(b).all()
+        assert np.linalg.norm(b[ne:] - a[ne:]) <= 1e-6 * np.linalg.norm(a[ne:])
+        assert np.linalg.norm(b[:ne] - a[:ne]) <= 1e-4 * np.linalg.norm(a[:ne])
+        mass_a, mass_b = g.cell_areas @ a[ne:], g.cell_areas @ b[ne:]
+        assert abs(mass_b - mass_a) <= 1e-7 * abs(mass_a)
+    energy = e32.energy(0)
+    assert np.all(np.abs(energy - e64.energy(0)) <= 1e-5 * np.abs(energy))
+    bad = states[0].copy()
+    bad[5] = np.nan
+    e32.reset()
+    e32.set_member(0, 2, bad)
+    with pytest.raises(d.TriskError) as err:
+        e32.run(1)
+    assert err.value.status == 4

@@ -242,6 +242,32 @@ def test_autotune_keeps_results(require_gpu):
             m.set_block(bad)
 
 
+def test_l2_residency_keeps_results(require_gpu):
+    """The L2-resident table prefix (evict-last loads, with or without a persisting window)
+    changes only where tables are cached: results stay bit-identical."""
+    import torch
+    from dmplex_b200.model import l2_info
+    g = trisk_grid(5, True)
+    si = w.si_parameters()
+    m = d.TRiSKShallowWater(g, pv_flux="gassmann", kinetic_energy="vertex", **si)
+    y = w.synthetic_state(g, seed=4)
+    ref = y.copy()
+    d.rk4_step(ref, 300.0, d.tendency, d.RK4Cache(ref), m, nsteps=3)
+    info = l2_info(0)
+    assert info["l2_bytes"] > 0 and info["max_window_bytes"] >= 0
+    for keep, window in ((1 << 20, False), (8 << 20, True), (1 << 40, False)):
+        m.set_l2_residency(keep, window)
+        got = m.info()
+        assert 0 < got["l2_resident_table_bytes"] <= keep and got["l2_window"] == window
+        yd = torch.from_numpy(y).cuda()
+        d.rk4_step(yd, 300.0, d.tendency, d.RK4Cache(yd), m, nsteps=3)
+        assert np.array_equal(yd.cpu().numpy(), ref)
+    m.set_l2_residency(0)
+    assert m.info()["l2_resident_table_bytes"] == 0
+    with pytest.raises(d.TriskError):
+        m.set_l2_residency(-1)
+
+
 @pytest.mark.slow
 def test_config_level7_gassmann_vertex(require_gpu):
     """The drop-in configuration at full size (hexagon 7, Gassmann PV flux, vertex kinetic
