@@ -47,6 +47,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble leg")
     p.add_argument("--no-closure", action="store_true", help="skip the learned-closure leg")
+    p.add_argument("--no-hexagon5", action="store_true", help="skip the hexagon-5 CPU/GPU leg")
+    p.add_argument("--ensemble-days", type=float, default=1.0, help="simulated days of the ensemble leg")
     p.add_argument("--level", type=int, default=LEVEL, help="mesh level (7 is the benchmark workload)")
     p.add_argument("--block", default=None,
                    help="fixed block sizes of the three phases, e.g. 128,128,64 (skips the autotuner)")
@@ -89,6 +91,50 @@ def oracle_baseline(g, y, seconds, threads):
         if el >= seconds or steps >= 1000:
             break
     return g.nc * steps / el, steps, el
+
+
+def run_hexagon5_leg(local_rank, threads, cpu=True):
+    """The reference's CPU-runnable case: hexagon 5, TRiSK PV flux, cell K, dt 300 s, 100 RK4
+    steps from a seeded degree-8, 100 m rms state. The CPU restatement on `threads` host
+    threads (median of 5 repeats) and the B200 path (device-resident state)."""
+    import torch
+    import dmplex_b200 as d
+    from dmplex_b200 import workloads as w
+    from oracle.oracle import Oracle
+    si = w.si_parameters()
+    g = d.TRiSKGrid(d.create_hexagon_mesh(5, centroidal=True))
+    y = w.synthetic_state(g, seed=0)
+    out = {"workload": "hexagon5-trisk-cell-fp64-rk4, dt 300 s, 100 steps", "cells": g.nc}
+    if cpu:
+        o = Oracle(d.model_tables(g, pv_flux="trisk", kinetic_energy="cell", **si), threads=threads)
+        times = []
+        for _ in range(5):
+            z = y.copy()
+            o.rk4_step(z, 300.0, 1)
+            t0 = time.perf_counter()
+            o.rk4_step(z, 300.0, 100)
+            times.append(time.perf_counter() - t0)
+        out["cpu_cell_steps_per_s"] = g.nc * 100 / float(np.median(times))
+        out["cpu_cores"] = threads
+        out["cpu_kind"] = "CPU restatement of the reference kernels in C with OpenMP (not Julia)"
+    m = d.TRiSKShallowWater(g, pv_flux="trisk", kinetic_energy="cell", device=local_rank, **si)
+    yd = torch.from_numpy(y).to(f"cuda:{local_rank}")
+    m.autotune(yd, 300.0, 20)
+    stream = torch.cuda.ExternalStream(m.stream(), device=local_rank)
+    m.rk4_async(yd, 300.0, 10)
+    m.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    m.rk4_async(yd, 300.0, 1000)
+    b.record(stream)
+    m.synchronize()
+    sec = a.elapsed_time(b) / 1e3
+    out["gpu_cell_steps_per_s"] = g.nc * 1000 / sec
+    out["gpu_us_per_step"] = sec / 1000 * 1e6
+    out["gpu_step_bytes"] = m.algorithmic_bytes()["rk4_step"]
+    out["gpu_step_gbs"] = out["gpu_step_bytes"] / (sec / 1000) / 1e9
+    out["note"] = "tables and state (39 MB per step) stay in the 126 MB L2"
+    return out
 
 
 class ClockSampler:
@@ -165,10 +211,11 @@ def ncu_traffic(kernel):
 ENSEMBLE_GROUPS = ((5, 64), (6, 32), (7, 8))  # (mesh level, members), one simulated day, FP64
 
 
-def run_ensemble_leg(local_rank, seed):
+def run_ensemble_leg(local_rank, seed, days=1.0, state_bits=64):
     """Batched ensemble of three mesh levels in one persistent CUDA-graph launch per phase:
     every member has its own seed, harmonic degree <= 12 and height rms in 50-300 m; each
-    level has its own dt (Courant 0.5) and runs one simulated day."""
+    level has its own dt (Courant 0.5) and runs `days` simulated days (state_bits 32: the
+    states and work vectors are stored as float, the arithmetic stays FP64)."""
     import torch
     import dmplex_b200 as d
     from dmplex_b200 import workloads as w
@@ -178,9 +225,10 @@ def run_ensemble_leg(local_rank, seed):
         g = d.TRiSKGrid(d.create_hexagon_mesh(level, centroidal=True))
         m = d.TRiSKShallowWater(g, pv_flux=PV, kinetic_energy=KE, device=local_rank, **si)
         nsteps, dt = w.day_steps(g)
+        nsteps = max(1, int(round(nsteps * days)))
         groups.append((m, members, dt, nsteps))
         info.append((g, m, members, nsteps, dt))
-    ens = d.Ensemble(groups)
+    ens = d.Ensemble(groups, state_bits=state_bits)
     for gi, (g, m, members, nsteps, dt) in enumerate(info):
         for k, y in enumerate(w.ensemble_members(g, members, seed=seed + gi)):
             ens.set_member(gi, k, y)
@@ -201,11 +249,14 @@ def run_ensemble_leg(local_rank, seed):
     for (g, m, members, _, _), s in zip(info, taken):
         n_b = 8.0 * m.state_size
         T = (m.algorithmic_bytes()["rk4_step"] - 23 * n_b) / 4
+        n_b *= state_bits / 64  # the state in its storage precision
         nbytes += s * (4 * (T + 2 * members * n_b) + 15 * members * n_b)
     peak, _ = measured_peak()
     return {"workload": "ensemble " + " + ".join(f"{k}x hexagon{l}" for l, k in ENSEMBLE_GROUPS) +
-                        f", {PV}/{KE}, FP64, 1 simulated day each",
-            "value": cell_steps / (ms * 1e-3), "unit": "cell-steps/s", "gpu_seconds_per_simulated_day": ms * 1e-3,
+                        f", {PV}/{KE}, {'FP64' if state_bits == 64 else 'FP32 state, FP64 arithmetic'}, "
+                        f"{days:g} simulated day each",
+            "value": cell_steps / (ms * 1e-3), "unit": "cell-steps/s",
+            "gpu_seconds_per_simulated_day": ms * 1e-3 / days,
             "steps": taken, "dt_s": [round(x[4], 3) for x in info], "members": [x[2] for x in info],
             "gpu_launches": ens.launch_count() - launches0, "gbs": nbytes / (ms * 1e-3) / 1e9,
             "frac": nbytes / (ms * 1e-3) / 1e9 / peak}
@@ -417,12 +468,17 @@ def run_b200(args, rank, world, local_rank):
 
     ensemble = None
     if not args.no_ensemble:
-        ensemble = run_ensemble_leg(local_rank, seed=1000 * (rank + 1))
+        ensemble = run_ensemble_leg(local_rank, seed=1000 * (rank + 1), days=args.ensemble_days)
+        f32 = run_ensemble_leg(local_rank, seed=1000 * (rank + 1), days=args.ensemble_days, state_bits=32)
+        ensemble["fp32_state"] = {k: f32[k] for k in ("value", "gpu_seconds_per_simulated_day", "gbs", "frac")}
         if world > 1:
             ensemble["value_all_ranks"] = world * ensemble["value"]
     closure = None
     if not args.no_closure:
         closure = run_closure_leg(local_rank)
+    hexagon5 = None
+    if rank == 0 and not args.no_hexagon5:
+        hexagon5 = run_hexagon5_leg(local_rank, os.cpu_count() or 1, cpu=world == 1 and not args.no_cpu_baseline)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -436,7 +492,7 @@ def run_b200(args, rank, world, local_rank):
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": config_dict(g, world, args.level), "clocks": clocks.summary(), "e2e": e2e,
                 "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu, "ensemble": ensemble,
-                "closure": closure}
+                "closure": closure, "hexagon5": hexagon5}
         print(json.dumps(line), flush=True)
     del m
 
