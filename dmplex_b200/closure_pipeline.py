@@ -13,7 +13,8 @@
        continuity equation stays in flux form, so the corrected model conserves mass to
        round-off.
 3. Training: the edge-local MLP (closure.ClosureMLP, tensor cores) on normalized features
-   and targets, Adam, batches of 65536 edges.
+   and targets, Adam, batches of 65536 edges; then the momentum output's scale is chosen
+   a posteriori by 2-day coarse runs from separate validation seeds (calibrate).
 4. Evaluation: coarse ensembles with and without the closure, started from the coarse-
    grained fine state, against the coarse-grained fine run; h and relative-vorticity L2
    errors per day; the closure is switched off for a member whose energy drifts by more
@@ -270,9 +271,10 @@ def l2_errors(gc, Vc, Y, Yt):
 
 
 def run_coarse(gc, Y_init, days, dt, daily_truth, mlp=None, norm=None, drift_per_day=1e-6, device=0,
-               every_stage=False, momentum_scale=1.0, state_bits=64):
+               every_stage=False, momentum_scale=1.0, state_bits=64, checks_per_day=8):
     """Coarse ensemble (members = columns of Y_init) for `days` days; h and vorticity errors
-    against the daily truth, GPU seconds, and the members that fell back to the plain step.
+    against the daily truth, GPU seconds, and the members that fell back to the plain step
+    (energy drift per elapsed day above drift_per_day, checked checks_per_day times a day).
     momentum_scale multiplies the closure's momentum correction (0 keeps only the mass-flux
     correction); state_bits 32 stores the members' states as float."""
     if norm is not None:
@@ -297,27 +299,33 @@ def run_coarse(gc, Y_init, days, dt, daily_truth, mlp=None, norm=None, drift_per
     from ._lib import TriskError
     errs_h, errs_z, drifts, gpu_ms = [], [], [], 0.0
     diverged = None
+    checks = max(1, min(int(checks_per_day), steps_day))
+    bounds = [round(steps_day * c / checks) for c in range(checks + 1)]
     for day in range(1, days + 1):
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        ens.run_async(steps_day)
-        b.record(stream)
-        try:
-            ens.synchronize()
-        except TriskError as err:
-            if err.status != 4:
-                raise
-            diverged = day  # a member's state became non-finite during this day
+        for c in range(checks):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            ens.run_async(bounds[c + 1] - bounds[c])
+            b.record(stream)
+            try:
+                ens.synchronize()
+            except TriskError as err:
+                if err.status != 4:
+                    raise
+                diverged = day  # a member's state became non-finite during this day
+                break
+            gpu_ms += a.elapsed_time(b)
+            elapsed = day - 1 + (c + 1) / checks
+            drift = np.abs(ens.energy(0) - e0) / np.abs(e0) / elapsed
+            if mlp is not None:
+                ens.closure_check()
+                newly = (drift > drift_per_day) & (on > 0)
+                if newly.any():
+                    on[newly] = 0.0
+                    ens.closure_mask(0, on)
+        if diverged:
             break
-        gpu_ms += a.elapsed_time(b)
-        drift = np.abs(ens.energy(0) - e0) / np.abs(e0) / day
         drifts.append(float(drift.max()))
-        if mlp is not None:
-            ens.closure_check()
-            newly = (drift > drift_per_day) & (on > 0)
-            if newly.any():
-                on[newly] = 0.0
-                ens.closure_mask(0, on)
         Y = np.stack([ens.get_member(0, k) for k in range(S)], axis=1)
         eh, ez = l2_errors(gc, Vc, Y, daily_truth[day].cpu().numpy())
         errs_h.append(eh.tolist())
@@ -327,6 +335,25 @@ def run_coarse(gc, Y_init, days, dt, daily_truth, mlp=None, norm=None, drift_per
             "gpu_seconds": gpu_ms / 1e3, "gpu_seconds_per_member_day": gpu_ms / 1e3 / (S * max(done, 1)),
             "fallback_members": int((on == 0).sum()) if mlp is not None else None, "members": S,
             "state_bits": state_bits}
+
+
+def calibrate(gf, gc, mlp, norm, seeds=(501, 502), days=2, coarse_dt=150.0, fine_dt=20.0,
+              scales=(0.0, 0.05, 0.1, 0.2, 0.4, 1.0), device=0, log=print):
+    """A-posteriori choice of the momentum correction's scale: coarse runs with the closure
+    (no fallback, mass-flux part unscaled) from validation seeds, none of them a training or
+    evaluation seed, against their coarse-grained fine runs; the scale with the smallest mean
+    h error over the days wins (a run that turns non-finite loses). Returns (scale, table)."""
+    _, _, _, daily, _ = fine_snapshots(gf, gc, list(seeds), days, 0, dt_fine=fine_dt, device=device,
+                                       spinup_days=0.0, record_days=True)
+    table = {}
+    for sc in scales:
+        r = run_coarse(gc, daily[0], days, coarse_dt, daily, mlp, norm, drift_per_day=np.inf, device=device,
+                       momentum_scale=sc, state_bits=32)
+        err = float(np.mean(r["h_l2"])) if r["diverged_on_day"] is None else float("inf")
+        table[str(sc)] = err
+        log(f"calibration: momentum scale {sc}: mean h L2 over {days} days {err:.3f} m")
+    best = min(scales, key=lambda sc: table[str(sc)])
+    return best, table
 
 
 def pipeline(fine_level=8, coarse_level=6, train_seeds=32, train_days=10, snapshots=2000, eval_seeds=4,
@@ -359,6 +386,9 @@ def pipeline(fine_level=8, coarse_level=6, train_seeds=32, train_days=10, snapsh
     skill = output_skill(mlp, X, T)
     log(f"training loss per epoch {history}, held-out {held:.4f} (without the closure {zero:.4f}), "
         f"skill (mass flux, momentum) {skill}")
+    scale, table = calibrate(gf, gc, mlp, norm, coarse_dt=coarse_dt, fine_dt=fine_dt, device=device, log=log)
+    norm = np.array(norm, dtype=np.float64)
+    norm[2 * NFEAT + 1] *= scale  # the calibrated momentum scale is part of the saved closure
     if out_params:
         np.savez(out_params, params=mlp.params(), norm=norm, fine_level=fine_level, coarse_level=coarse_level,
                  window=window if target == "window" else 0.0, target=target)
@@ -370,6 +400,7 @@ def pipeline(fine_level=8, coarse_level=6, train_seeds=32, train_days=10, snapsh
         "window_seconds": delta if target == "window" else None,
         "coarse_steps_per_window": coarse_steps if target == "window" else None, "epochs": epochs, "train_loss": history, "heldout_loss": held,
         "heldout_loss_without_closure": zero, "output_skill": skill, "fine_training_gpu_seconds": fine_train_s,
+        "calibrated_momentum_scale": scale, "calibration_mean_h_l2": table,
     }
     summary.update(evaluate(gf, gc, mlp, norm, eval_seeds, eval_days, coarse_dt, fine_dt, device, log))
     summary["wall_seconds"] = time.perf_counter() - t_start

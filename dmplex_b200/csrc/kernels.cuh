@@ -213,8 +213,11 @@ __device__ __forceinline__ void vertex_body(const DevTables& T, const DevWorkT<R
 #pragma unroll
   for (int k = 0; k < VW; ++k) eta += vh[k] * hh[k];
   const size_t o = (size_t)v * M + mm;
-  W.zv[o] = (R)z;
-  W.hv[o] = (R)eta;
+  // only what a later phase reads: zeta_v for the Gassmann rhombus PV, h_v for it and for
+  // the vertex part of the mass flux, q_v for the TRiSK edge PV; all three for a diagnostic
+  // call (want_qv)
+  if (want_qv || PV != PVM_TRISK) W.zv[o] = (R)z;
+  if (want_qv || PV != PVM_TRISK || KE != KE_CELL) W.hv[o] = (R)eta;
   if (qv) W.qv[o] = (R)((z + cor) / eta);
   if (KE != KE_CELL) {
     double s = 0.0;
