@@ -85,7 +85,7 @@ __global__ void __launch_bounds__(256) kg_flux(const GroupSet G, int first_stage
 }
 
 template <int PV, int EPI, class R>
-__global__ void __launch_bounds__(256) kg_tend(const GroupSet G) {
+__global__ void __launch_bounds__(256, 4) kg_tend(const GroupSet G) {  // <= 64 registers: 8 blocks of 128
   pdl_trigger();
   for (int vb = blockIdx.x; vb < G.totalT; vb += gridDim.x) {
     const int gi = group_of(G, vb, 2);

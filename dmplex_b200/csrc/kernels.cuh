@@ -168,8 +168,13 @@ __device__ __forceinline__ V ldt(const DevTables& T, const V* base, int i) {
 template <bool ENS>
 __device__ __forceinline__ void split(int t, int M, int& ent, int& mem) {
   if (ENS) {
-    ent = t / M;
-    mem = t - ent * M;
+    if ((M & (M - 1)) == 0) {  // power-of-two member counts (uniform): a shift, no division
+      ent = t >> (__ffs(M) - 1);
+      mem = t & (M - 1);
+    } else {
+      ent = t / M;
+      mem = t - ent * M;
+    }
   } else {
     ent = t;
     mem = 0;
