@@ -391,7 +391,7 @@ def pipeline(fine_level=8, coarse_level=6, train_seeds=32, train_days=10, snapsh
     norm[2 * NFEAT + 1] *= scale  # the calibrated momentum scale is part of the saved closure
     if out_params:
         np.savez(out_params, params=mlp.params(), norm=norm, fine_level=fine_level, coarse_level=coarse_level,
-                 window=window if target == "window" else 0.0, target=target)
+                 window=window if target == "window" else 0.0, target=target, momentum_scale=scale)
     del X, T
     torch.cuda.empty_cache()
     summary = {
@@ -455,7 +455,13 @@ def main():
     p.add_argument("--params", default=None, help="where to save the trained network")
     p.add_argument("--evaluate", default=None, help="skip training: evaluate this saved network (.npz)")
     p.add_argument("--training-summary", default=None, help="JSON of the training run to merge (with --evaluate)")
+    p.add_argument("--momentum-scale", type=float, default=None,
+                   help="with --evaluate: the scale the saved closure's momentum output had at training "
+                        "(when the file does not record it); the closure is then re-calibrated")
+    p.add_argument("--calibrate-days", type=int, default=2)
+    p.add_argument("--scales", default="0,0.05,0.1,0.2,0.4,1", help="momentum scales the calibration tries")
     a = p.parse_args()
+    scales = tuple(float(x) for x in a.scales.split(","))
     if a.evaluate:
         z = np.load(a.evaluate)
         gf, gc = _grid(int(z["fine_level"])), _grid(int(z["coarse_level"]))
@@ -463,8 +469,21 @@ def main():
         if a.training_summary:
             with open(a.training_summary) as f:
                 s.update(json.load(f))
-        s.update(evaluate(gf, gc, ClosureMLP(z["params"]), z["norm"], a.eval_seeds, a.eval_days, a.coarse_dt,
-                          a.fine_dt))
+        mlp, norm = ClosureMLP(z["params"]), np.array(z["norm"], dtype=np.float64)
+        old = float(z["momentum_scale"]) if "momentum_scale" in z.files else a.momentum_scale
+        if old is not None:  # back to the trained output scale, then calibrate again
+            if old <= 0:
+                raise SystemExit("the saved closure's momentum output is off; nothing to re-calibrate")
+            norm[2 * NFEAT + 1] /= old
+            scale, table = calibrate(gf, gc, mlp, norm, days=a.calibrate_days, coarse_dt=a.coarse_dt,
+                                     fine_dt=a.fine_dt, scales=scales)
+            norm[2 * NFEAT + 1] *= scale
+            s.update({"calibrated_momentum_scale": scale, "calibration_mean_h_l2": table,
+                      "calibration_days": a.calibrate_days})
+            if a.params:
+                np.savez(a.params, **{k: z[k] for k in z.files if k not in ("norm", "momentum_scale")}, norm=norm,
+                         momentum_scale=scale)
+        s.update(evaluate(gf, gc, mlp, norm, a.eval_seeds, a.eval_days, a.coarse_dt, a.fine_dt))
     else:
         s = pipeline(a.fine, a.coarse, a.train_seeds, a.train_days, a.snapshots, a.eval_seeds, a.eval_days,
                      a.coarse_dt, a.window, a.fine_dt, a.epochs, out_params=a.params, target=a.target)
