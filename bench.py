@@ -58,6 +58,33 @@ def parse():
     return args
 
 
+def rank_barrier(world, cuda=True):
+    """All ranks meet here (after their GPU work has finished, with cuda)."""
+    import torch
+    if cuda:
+        torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks_of(x, world, device=None):
+    """The largest x over all ranks (device None: a CPU tensor, for gloo)."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_value(world, cells, steps, ms):
+    """cell-steps/s of the whole job: every rank advances its own replica of `cells` cells
+    by `steps` RK4 steps; ms is the slowest rank's time."""
+    return world * cells * steps / (ms * 1e-3)
+
+
 def build_workload(seed, level=LEVEL):
     import dmplex_b200 as d
     from dmplex_b200 import workloads as w
@@ -393,17 +420,13 @@ def run_b200(args, rank, world, local_rank):
     stream = torch.cuda.ExternalStream(m.stream(), device=local_rank)
     yd = torch.from_numpy(y_host).to(f"cuda:{local_rank}")
 
+    dev = f"cuda:{local_rank}"
+
     def barrier():
-        torch.cuda.synchronize()
-        if world > 1:
-            dist.barrier()
+        rank_barrier(world, cuda=True)
 
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local_rank}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks_of(x, world, dev)
 
     # block shapes from the autotuner (or given), then warm-up (also captures the CUDA graph)
     if args.block:
@@ -427,7 +450,7 @@ def run_b200(args, rank, world, local_rank):
     ms = start.elapsed_time(end)
     launches = m.launch_count() - launches0
     ms = max_over_ranks(ms)
-    value = world * g.nc * args.steps / (ms * 1e-3)
+    value = whole_job_value(world, g.nc, args.steps, ms)
 
     # e2e: the public synchronous call with a pinned host state, one step per call
     pinned = torch.from_numpy(y_host.copy()).pin_memory()
@@ -444,7 +467,7 @@ def run_b200(args, rank, world, local_rank):
     e1.record(stream)
     torch.cuda.synchronize()
     e_ms = max_over_ranks(e0.elapsed_time(e1))
-    e2e = {"value": world * g.nc * e_steps / (e_ms * 1e-3), "unit": "cell-steps/s", "h2d_bytes_per_step": nbytes,
+    e2e = {"value": whole_job_value(world, g.nc, e_steps, e_ms), "unit": "cell-steps/s", "h2d_bytes_per_step": nbytes,
            "d2h_bytes_per_step": nbytes, "steps": e_steps}
 
     # roofline of the dominant kernel: a second, instrumented pass with events around
