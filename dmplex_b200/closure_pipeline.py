@@ -271,7 +271,7 @@ def l2_errors(gc, Vc, Y, Yt):
 
 
 def run_coarse(gc, Y_init, days, dt, daily_truth, mlp=None, norm=None, drift_per_day=1e-6, device=0,
-               every_stage=False, momentum_scale=1.0, state_bits=64, checks_per_day=8):
+               every_stage=False, momentum_scale=1.0, state_bits=64, checks_per_day=8, work_free=False):
     """Coarse ensemble (members = columns of Y_init) for `days` days; h and vorticity errors
     against the daily truth, GPU seconds, and the members that fell back to the plain step
     (energy drift per elapsed day above drift_per_day, checked checks_per_day times a day).
@@ -291,7 +291,7 @@ def run_coarse(gc, Y_init, days, dt, daily_truth, mlp=None, norm=None, drift_per
         col.copy_(Y_init[:, k])
         ens.set_member(0, k, col)
     if mlp is not None:
-        ens.set_closure(0, mlp, edge_geometry(gc), norm, every_stage)
+        ens.set_closure(0, mlp, edge_geometry(gc), norm, every_stage, work_free)
     on = np.ones(S, dtype=np.float32)
     e0 = ens.energy(0)
     Vc = relative_vorticity_matrix(model_tables(gc, pv_flux=PV, kinetic_energy=KE, **si))
@@ -338,7 +338,7 @@ def run_coarse(gc, Y_init, days, dt, daily_truth, mlp=None, norm=None, drift_per
 
 
 def calibrate(gf, gc, mlp, norm, seeds=(501, 502), days=2, coarse_dt=150.0, fine_dt=20.0,
-              scales=(0.0, 0.05, 0.1, 0.2, 0.4, 1.0), device=0, log=print):
+              scales=(0.0, 0.05, 0.1, 0.2, 0.4, 1.0), device=0, log=print, work_free=False):
     """A-posteriori choice of the momentum correction's scale: coarse runs with the closure
     (no fallback, mass-flux part unscaled) from validation seeds, none of them a training or
     evaluation seed, against their coarse-grained fine runs; the scale with the smallest mean
@@ -348,7 +348,7 @@ def calibrate(gf, gc, mlp, norm, seeds=(501, 502), days=2, coarse_dt=150.0, fine
     table = {}
     for sc in scales:
         r = run_coarse(gc, daily[0], days, coarse_dt, daily, mlp, norm, drift_per_day=np.inf, device=device,
-                       momentum_scale=sc, state_bits=32)
+                       momentum_scale=sc, state_bits=32, work_free=work_free)
         err = float(np.mean(r["h_l2"])) if r["diverged_on_day"] is None else float("inf")
         table[str(sc)] = err
         log(f"calibration: momentum scale {sc}: mean h L2 over {days} days {err:.3f} m")
@@ -407,7 +407,8 @@ def pipeline(fine_level=8, coarse_level=6, train_seeds=32, train_days=10, snapsh
     return summary
 
 
-def evaluate(gf, gc, mlp, norm, eval_seeds=4, eval_days=10, coarse_dt=150.0, fine_dt=20.0, device=0, log=print):
+def evaluate(gf, gc, mlp, norm, eval_seeds=4, eval_days=10, coarse_dt=150.0, fine_dt=20.0, device=0, log=print,
+             work_free=False):
     """Coarse runs from the coarse-grained state of held-out seeds against the coarse-grained
     fine run: plain (FP64 and FP32 state), and with FP32 state the closure with the energy-
     drift fallback, without it, evaluated at every RK4 stage, and the mass-flux correction
@@ -419,6 +420,7 @@ def evaluate(gf, gc, mlp, norm, eval_seeds=4, eval_days=10, coarse_dt=150.0, fin
            "fine_gpu_seconds_per_member_day": fine_eval_s / (eval_seeds * eval_days)}
     init = daily[0]
     f32 = {"state_bits": 32}
+    out["work_free_momentum_correction"] = bool(work_free)
     variants = {"plain_coarse": {},
                 "plain_coarse_fp32": dict(f32),
                 "closure_coarse": {"mlp": mlp, "norm": norm, **f32},
@@ -428,6 +430,8 @@ def evaluate(gf, gc, mlp, norm, eval_seeds=4, eval_days=10, coarse_dt=150.0, fin
                 "closure_mass_flux_only_no_fallback": {"mlp": mlp, "norm": norm, "drift_per_day": np.inf,
                                                        "momentum_scale": 0.0, **f32}}
     for name, kw in variants.items():
+        if "mlp" in kw:
+            kw["work_free"] = work_free
         r = run_coarse(gc, init, eval_days, coarse_dt, daily, device=device, **kw)
         out[name] = r
         log(f"{name}: h L2 per day {[round(float(np.mean(x)), 2) for x in r['h_l2']]}, vorticity "
@@ -459,6 +463,8 @@ def main():
                    help="with --evaluate: the scale the saved closure's momentum output had at training "
                         "(when the file does not record it); the closure is then re-calibrated")
     p.add_argument("--calibrate-days", type=int, default=2)
+    p.add_argument("--work-free", action="store_true",
+                   help="with --evaluate: the momentum correction does no work on each member's flow")
     p.add_argument("--scales", default="0,0.05,0.1,0.2,0.4,1", help="momentum scales the calibration tries")
     a = p.parse_args()
     scales = tuple(float(x) for x in a.scales.split(","))
@@ -476,14 +482,15 @@ def main():
                 raise SystemExit("the saved closure's momentum output is off; nothing to re-calibrate")
             norm[2 * NFEAT + 1] /= old
             scale, table = calibrate(gf, gc, mlp, norm, days=a.calibrate_days, coarse_dt=a.coarse_dt,
-                                     fine_dt=a.fine_dt, scales=scales)
+                                     fine_dt=a.fine_dt, scales=scales, work_free=a.work_free)
             norm[2 * NFEAT + 1] *= scale
             s.update({"calibrated_momentum_scale": scale, "calibration_mean_h_l2": table,
                       "calibration_days": a.calibrate_days})
             if a.params:
-                np.savez(a.params, **{k: z[k] for k in z.files if k not in ("norm", "momentum_scale")}, norm=norm,
-                         momentum_scale=scale)
-        s.update(evaluate(gf, gc, mlp, norm, a.eval_seeds, a.eval_days, a.coarse_dt, a.fine_dt))
+                np.savez(a.params, **{k: z[k] for k in z.files if k not in ("norm", "momentum_scale", "work_free")},
+                         norm=norm, momentum_scale=scale, work_free=a.work_free)
+        s.update(evaluate(gf, gc, mlp, norm, a.eval_seeds, a.eval_days, a.coarse_dt, a.fine_dt,
+                          work_free=a.work_free))
     else:
         s = pipeline(a.fine, a.coarse, a.train_seeds, a.train_days, a.snapshots, a.eval_seeds, a.eval_days,
                      a.coarse_dt, a.window, a.fine_dt, a.epochs, out_params=a.params, target=a.target)

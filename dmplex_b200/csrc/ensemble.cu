@@ -29,6 +29,7 @@ struct GroupDesc {
   int startV, nV;
   int startF, nEF, nCF;
   int startT, nET, nCT;
+  int P;  // members per thread in the vertex and flux phases (2 when M is even, else 1)
 };
 
 struct GroupSet {
@@ -67,7 +68,11 @@ __global__ void __launch_bounds__(256) kg_vertex(const GroupSet G, int first_sta
     const GroupDesc& D = G.g[gi];
     if (G.counters[gi] >= D.nsteps) continue;
     const R* u = as_r<R>(first_stage ? D.y : D.st);
-    vertex_body<PV, KE, true, R>(D.T, work_as<R>(D.W), u, u + (size_t)D.T.ne * D.M, D.M, 0, vb - D.startV);
+    if (D.P == 2)
+      vertex_body<PV, KE, true, R, false, 2>(D.T, work_as<R>(D.W), u, u + (size_t)D.T.ne * D.M, D.M, 0,
+                                             vb - D.startV);
+    else
+      vertex_body<PV, KE, true, R>(D.T, work_as<R>(D.W), u, u + (size_t)D.T.ne * D.M, D.M, 0, vb - D.startV);
   }
 }
 
@@ -79,8 +84,12 @@ __global__ void __launch_bounds__(256) kg_flux(const GroupSet G, int first_stage
     const GroupDesc& D = G.g[gi];
     if (G.counters[gi] >= D.nsteps) continue;
     const R* u = as_r<R>(first_stage ? D.y : D.st);
-    flux_body<PV, KE, true, R>(D.T, work_as<R>(D.W), u, u + (size_t)D.T.ne * D.M, D.M, D.nEF, want_K,
-                               vb - D.startF);
+    if (D.P == 2)
+      flux_body<PV, KE, true, R, false, 2>(D.T, work_as<R>(D.W), u, u + (size_t)D.T.ne * D.M, D.M, D.nEF, want_K,
+                                           vb - D.startF);
+    else
+      flux_body<PV, KE, true, R>(D.T, work_as<R>(D.W), u, u + (size_t)D.T.ne * D.M, D.M, D.nEF, want_K,
+                                 vb - D.startF);
   }
 }
 
@@ -170,6 +179,62 @@ __global__ void kg_closure_apply(R* dF, R* dq, const float* Y, const float* memb
   dq[r] = (R)(on * sQ * (double)Y[2 * r + 1]);
 }
 
+// Work-free momentum correction. With the cell kinetic energy K_i = sum_k kinetic[i,k] u_k^2,
+// kinetic[i,k] = l_e d_(e,i) / (2 A_i) (the TRiSK coefficient, alpha = 1), the energy's
+// gradient is g_e = dE/du_e = u_e l_e (h_c0 d_(e,c0) + h_c1 d_(e,c1)). Removing from each
+// member's correction dq its component along g (dq -= (<g, dq> / <g, g>) g) leaves a
+// correction that does no work on that member's flow to first order. geom: l_e, d_e and the
+// two cell distances in columns 0..3 of the closure geometry (internal edge order).
+__device__ __forceinline__ double energy_gradient(const DevTables& T, double ue, double h0, double h1,
+                                                  const float* geom, int e) {
+  const float* gm = geom + (size_t)e * NGEOM;
+  return ue * (double)gm[0] * (h0 * (double)gm[2] + h1 * (double)gm[3]);
+}
+
+// sums[2m] += <g, dq>, sums[2m + 1] += <g, g> for member m; block (32, 8): x members, y edges
+template <class R>
+__global__ void kg_work_sums(DevTables T, const R* y, const R* dq, const float* geom, int M, double* sums) {
+  __shared__ double s1[8][32], s2[8][32];
+  const int m = blockIdx.y * 32 + threadIdx.x;
+  double a = 0.0, b = 0.0;
+  if (m < M) {
+    const R* h = y + (size_t)T.ne * M;
+    for (int e = blockIdx.x * 8 + threadIdx.y; e < T.ne; e += gridDim.x * 8) {
+      const int c0 = T.edge_cells[e], c1 = T.edge_cells[T.lde + e];
+      const double g = energy_gradient(T, (double)y[(size_t)e * M + m], (double)h[(size_t)c0 * M + m],
+                                       (double)h[(size_t)c1 * M + m], geom, e);
+      a += g * (double)dq[(size_t)e * M + m];
+      b += g * g;
+    }
+  }
+  s1[threadIdx.y][threadIdx.x] = a;
+  s2[threadIdx.y][threadIdx.x] = b;
+  __syncthreads();
+  if (threadIdx.y == 0 && m < M) {
+    for (int k = 1; k < 8; ++k) {
+      a += s1[k][threadIdx.x];
+      b += s2[k][threadIdx.x];
+    }
+    atomicAdd(&sums[2 * m], a);
+    atomicAdd(&sums[2 * m + 1], b);
+  }
+}
+
+template <class R>
+__global__ void kg_work_project(DevTables T, const R* y, R* dq, const float* geom, int M, int64_t rows,
+                                const double* sums) {
+  const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (r >= rows) return;
+  const int e = (int)(r / M), m = (int)(r - (int64_t)e * M);
+  const double gg = sums[2 * m + 1];
+  if (!(gg > 0.0)) return;
+  const R* h = y + (size_t)T.ne * M;
+  const int c0 = T.edge_cells[e], c1 = T.edge_cells[T.lde + e];
+  const double g = energy_gradient(T, (double)y[r], (double)h[(size_t)c0 * M + m], (double)h[(size_t)c1 * M + m],
+                                   geom, e);
+  dq[r] = (R)((double)dq[r] - sums[2 * m] / gg * g);
+}
+
 // energy[m] += sum_i A_i h_i (K_i + g h_i / 2) over this block's cells (TRiSKShallowWater.jl:406-411)
 template <class R>
 __global__ void kg_energy(const R* y, const R* K, const double* area, int nc, int ne, int M, double g,
@@ -221,6 +286,8 @@ struct ClosureSlot {
   double* dq = nullptr;        // rows: momentum-tendency correction, storage type
   trisk::FeatureNorm norm{};
   bool every_stage = false;    // false: the network runs at stage 1 and its output is reused
+  bool work_free = false;      // project the momentum correction to do no work (per member)
+  double* sums = nullptr;      // 2 M: <g, dq>, <g, g> per member
 };
 
 struct TriskEnsemble {
@@ -341,6 +408,16 @@ void enqueue_closure(TriskEnsemble& e, int stage) {
                                                     c.member_on, rows, D.M, c.norm.out_scale[0],
                                                     c.norm.out_scale[1]);
       CUDA_CHECK(cudaGetLastError());
+      if (c.work_free) {
+        const R* ys = reinterpret_cast<const R*>(stage == 1 ? D.y : D.st);
+        CUDA_CHECK(cudaMemsetAsync(c.sums, 0, 2 * D.M * sizeof(double), e.stream));
+        const dim3 grid((unsigned)std::min<int64_t>(cdiv(D.T.ne, 8), 1024), (unsigned)cdiv(D.M, 32));
+        kg_work_sums<R><<<grid, dim3(32, 8), 0, e.stream>>>(D.T, ys, reinterpret_cast<const R*>(c.dq), c.geom, D.M,
+                                                             c.sums);
+        kg_work_project<R><<<nb, 256, 0, e.stream>>>(D.T, ys, reinterpret_cast<R*>(c.dq), c.geom, D.M, rows, c.sums);
+        CUDA_CHECK(cudaGetLastError());
+        e.launches += 2;
+      }
     });
     e.launches += 3;
   }
@@ -472,9 +549,12 @@ int trisk_ensemble_create_precision(TriskModel* const* models, const int32_t* me
     D.acc = e->alloc_state(m->N * M);
     D.st = e->alloc_state(m->N * M);
     CUDA_CHECK(cudaMemset(D.y, 0, m->N * M * e->esize()));
-    D.nV = (int)cdiv(m->nv * M, B);
-    D.nEF = D.nET = (int)cdiv(m->ne * M, B);
-    D.nCF = D.nCT = (int)cdiv(m->nc * M, B);
+    D.P = M % 2 == 0 ? 2 : 1;
+    D.nV = (int)cdiv(m->nv * M / D.P, B);
+    D.nEF = (int)cdiv(m->ne * M / D.P, B);
+    D.nCF = (int)cdiv(m->nc * M / D.P, B);
+    D.nET = (int)cdiv(m->ne * M, B);
+    D.nCT = (int)cdiv(m->nc * M, B);
     D.startV = sV;
     D.startF = sF;
     D.startT = sT;
@@ -632,7 +712,7 @@ int trisk_ensemble_bytes(TriskEnsemble* ens, double* step_bytes) {
 }
 
 int trisk_ensemble_set_closure(TriskEnsemble* ens, int32_t group, TriskClosure* net, const float* geometry,
-                               const double* norm, int32_t every_stage) {
+                               const double* norm, int32_t flags) {
   TRISK_API_BEGIN
   TriskEnsemble& e = *checked_e(ens);
   if (group < 0 || group >= e.G.n) throw Error(TRISK_ERR_ARGUMENT, "group out of range");
@@ -675,7 +755,9 @@ int trisk_ensemble_set_closure(TriskEnsemble* ens, int32_t group, TriskClosure* 
   }
   c.norm.out_scale[0] = norm[2 * NFEAT];
   c.norm.out_scale[1] = norm[2 * NFEAT + 1];
-  c.every_stage = every_stage != 0;
+  c.every_stage = (flags & 1) != 0;
+  c.work_free = (flags & 2) != 0;
+  if (c.work_free && !c.sums) c.sums = e.alloc<double>(2 * (size_t)D.M);
   c.net = net;
   TRISK_API_END
 }

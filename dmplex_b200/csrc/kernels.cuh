@@ -181,16 +181,56 @@ __device__ __forceinline__ void split(int t, int M, int& ent, int& mem) {
   }
 }
 
+// P members per thread (P = 1 or 2, M a multiple of P): the thread's members are mm ..
+// mm + P - 1, read and written as one P-wide vector; the arithmetic per member is that of
+// P = 1, so results are the same bit for bit.
+template <bool ENS, int P>
+__device__ __forceinline__ void split_p(int t, int M, int& ent, int& mm) {
+  if (P == 1) {
+    split<ENS>(t, M, ent, mm);
+  } else {
+    int g;
+    split<ENS>(t, M / P, ent, g);
+    mm = g * P;
+  }
+}
+
+template <class R, int P>
+__device__ __forceinline__ void ld_members(const R* p, double (&x)[P]) {
+  if constexpr (P == 1) {
+    x[0] = p[0];
+  } else if constexpr (sizeof(R) == 8) {
+    const double2 v = *reinterpret_cast<const double2*>(p);
+    x[0] = v.x;
+    x[1] = v.y;
+  } else {
+    const float2 v = *reinterpret_cast<const float2*>(p);
+    x[0] = v.x;
+    x[1] = v.y;
+  }
+}
+
+template <class R, int P>
+__device__ __forceinline__ void st_members(R* p, const double (&x)[P]) {
+  if constexpr (P == 1) {
+    p[0] = (R)x[0];
+  } else if constexpr (sizeof(R) == 8) {
+    *reinterpret_cast<double2*>(p) = make_double2(x[0], x[1]);
+  } else {
+    *reinterpret_cast<float2*>(p) = make_float2((float)x[0], (float)x[1]);
+  }
+}
+
 // ------------------------------------------------------------------------------------
 // phase 1: vertices
 // Each phase is a __device__ body over one block's worth of entities (block index vb),
 // called by the one-model kernels with vb = blockIdx.x and by the persistent ensemble
 // kernels (ensemble.cu) for every block of work they take.
-template <int PV, int KE, bool ENS, class R = double, bool KEEP = false>
+template <int PV, int KE, bool ENS, class R = double, bool KEEP = false, int P = 1>
 __device__ __forceinline__ void vertex_body(const DevTables& T, const DevWorkT<R>& W, const R* u, const R* h,
                                             int M, int want_qv, int vb) {
   int v, mm;
-  split<ENS>(vb * blockDim.x + threadIdx.x, M, v, mm);
+  split_p<ENS, P>(vb * blockDim.x + threadIdx.x, M, v, mm);
   if (v >= T.nv) return;
   int ve[VW], vc[VW];
   double cu[VW], vh[VW], vkw[VW];
@@ -206,30 +246,36 @@ __device__ __forceinline__ void vertex_body(const DevTables& T, const DevWorkT<R
   const bool qv = PV == PVM_TRISK || want_qv;
   if (qv) cor = ldt<KEEP>(T, T.coriolis, v);
   pdl_wait();
-  double uu[VW], hh[VW];
+  double uu[VW][P], hh[VW][P];
 #pragma unroll
   for (int k = 0; k < VW; ++k) {
-    uu[k] = u[(size_t)ve[k] * M + mm];
-    hh[k] = h[(size_t)vc[k] * M + mm];
+    ld_members<R, P>(u + (size_t)ve[k] * M + mm, uu[k]);
+    ld_members<R, P>(h + (size_t)vc[k] * M + mm, hh[k]);
   }
-  double z = 0.0, eta = 0.0;
+  double z[P], eta[P], q[P], kv[P];
 #pragma unroll
-  for (int k = 0; k < VW; ++k) z += cu[k] * uu[k];
+  for (int p = 0; p < P; ++p) {
+    z[p] = 0.0;
+    eta[p] = 0.0;
 #pragma unroll
-  for (int k = 0; k < VW; ++k) eta += vh[k] * hh[k];
+    for (int k = 0; k < VW; ++k) z[p] += cu[k] * uu[k][p];
+#pragma unroll
+    for (int k = 0; k < VW; ++k) eta[p] += vh[k] * hh[k][p];
+    if (qv) q[p] = (z[p] + cor) / eta[p];
+    kv[p] = 0.0;
+    if (KE != KE_CELL) {
+#pragma unroll
+      for (int k = 0; k < VW; ++k) kv[p] += vkw[k] * (uu[k][p] * uu[k][p]);
+    }
+  }
   const size_t o = (size_t)v * M + mm;
   // only what a later phase reads: zeta_v for the Gassmann rhombus PV, h_v for it and for
   // the vertex part of the mass flux, q_v for the TRiSK edge PV; all three for a diagnostic
   // call (want_qv)
-  if (want_qv || PV != PVM_TRISK) W.zv[o] = (R)z;
-  if (want_qv || PV != PVM_TRISK || KE != KE_CELL) W.hv[o] = (R)eta;
-  if (qv) W.qv[o] = (R)((z + cor) / eta);
-  if (KE != KE_CELL) {
-    double s = 0.0;
-#pragma unroll
-    for (int k = 0; k < VW; ++k) s += vkw[k] * (uu[k] * uu[k]);
-    W.Kv[o] = (R)s;
-  }
+  if (want_qv || PV != PVM_TRISK) st_members<R, P>(W.zv + o, z);
+  if (want_qv || PV != PVM_TRISK || KE != KE_CELL) st_members<R, P>(W.hv + o, eta);
+  if (qv) st_members<R, P>(W.qv + o, q);
+  if (KE != KE_CELL) st_members<R, P>(W.Kv + o, kv);
 }
 
 template <int PV, int KE, bool ENS, class R = double, bool KEEP = false>
@@ -242,12 +288,12 @@ __global__ void __launch_bounds__(256) k_vertex(DevTables T, DevWorkT<R> W, cons
 // ------------------------------------------------------------------------------------
 // phase 2: edges (mass flux, edge PV) and cells (Bernoulli function); blocks [0, nbE)
 // take edges, the rest cells
-template <int PV, int KE, bool ENS, class R = double, bool KEEP = false>
+template <int PV, int KE, bool ENS, class R = double, bool KEEP = false, int P = 1>
 __device__ __forceinline__ void flux_body(const DevTables& T, const DevWorkT<R>& W, const R* u, const R* h,
                                           int M, int nbE, int want_K, int vb) {
   if (vb < nbE) {
     int e, mm;
-    split<ENS>(vb * blockDim.x + threadIdx.x, M, e, mm);
+    split_p<ENS, P>(vb * blockDim.x + threadIdx.x, M, e, mm);
     if (e >= T.ne) return;
     const int ev0 = ldt<KEEP>(T, T.edge_vertices, e), ev1 = ldt<KEEP>(T, T.edge_vertices, T.lde + e);
     int ec0 = 0, ec1 = 0;
@@ -270,33 +316,48 @@ __device__ __forceinline__ void flux_body(const DevTables& T, const DevWorkT<R>&
     pdl_wait();
     const size_t o = (size_t)e * M + mm;
     const size_t o0 = (size_t)ev0 * M + mm, o1 = (size_t)ev1 * M + mm;
-    const double ue = u[o];
-    double hv0 = 0, hv1 = 0;
+    double ue[P], hv0[P], hv1[P], hc0[P], hc1[P], a0[P], a1[P];
+    ld_members<R, P>(u + o, ue);
     if (KE != KE_CELL || PV != PVM_TRISK) {
-      hv0 = W.hv[o0];
-      hv1 = W.hv[o1];
+      ld_members<R, P>(W.hv + o0, hv0);
+      ld_members<R, P>(W.hv + o1, hv1);
     }
-    double he;
-    if (KE == KE_CELL) {
-      he = eh0 * h[(size_t)ec0 * M + mm] + eh1 * h[(size_t)ec1 * M + mm];
-    } else if (KE == KE_VERTEX) {
-      he = vk0 * hv0 + vk1 * hv1;  // the reference's zero cell part adds exactly 0
-    } else {
-      he = eh0 * h[(size_t)ec0 * M + mm] + eh1 * h[(size_t)ec1 * M + mm] + vk0 * hv0 + vk1 * hv1;
+    if (KE != KE_VERTEX) {
+      ld_members<R, P>(h + (size_t)ec0 * M + mm, hc0);
+      ld_members<R, P>(h + (size_t)ec1 * M + mm, hc1);
     }
-    W.F[o] = (R)(he * ue);
     if (PV == PVM_TRISK) {
-      const double qa = W.qv[o0], qb = W.qv[o1];
-      W.qe[o] = (R)((qa + qb) / 2);
+      ld_members<R, P>(W.qv + o0, a0);
+      ld_members<R, P>(W.qv + o1, a1);
     } else {
-      const double za = W.zv[o0], zb = W.zv[o1];
-      const double z = r0 * za + r1 * zb;
-      const double eta = r0 * hv0 + r1 * hv1;
-      W.qe[o] = (R)((z + gc) / eta);
+      ld_members<R, P>(W.zv + o0, a0);
+      ld_members<R, P>(W.zv + o1, a1);
     }
+    double Fo[P], qo[P];
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      double he;
+      if (KE == KE_CELL) {
+        he = eh0 * hc0[p] + eh1 * hc1[p];
+      } else if (KE == KE_VERTEX) {
+        he = vk0 * hv0[p] + vk1 * hv1[p];  // the reference's zero cell part adds exactly 0
+      } else {
+        he = eh0 * hc0[p] + eh1 * hc1[p] + vk0 * hv0[p] + vk1 * hv1[p];
+      }
+      Fo[p] = he * ue[p];
+      if (PV == PVM_TRISK) {
+        qo[p] = (a0[p] + a1[p]) / 2;
+      } else {
+        const double z = r0 * a0[p] + r1 * a1[p];
+        const double eta = r0 * hv0[p] + r1 * hv1[p];
+        qo[p] = (z + gc) / eta;
+      }
+    }
+    st_members<R, P>(W.F + o, Fo);
+    st_members<R, P>(W.qe + o, qo);
   } else {
     int i, mm;
-    split<ENS>((vb - nbE) * blockDim.x + threadIdx.x, M, i, mm);
+    split_p<ENS, P>((vb - nbE) * blockDim.x + threadIdx.x, M, i, mm);
     if (i >= T.nc) return;
     int ce[CW], cv[CW];
     double kin[CW], kk[CW];
@@ -313,30 +374,39 @@ __device__ __forceinline__ void flux_body(const DevTables& T, const DevWorkT<R>&
     }
     pdl_wait();
     const size_t o = (size_t)i * M + mm;
-    const double hi = h[o];
-    double K = 0.0, B;
+    double hi[P], Kc[P], Bc[P];
+    ld_members<R, P>(h + o, hi);
+    double uk[CW][P], kv[CW][P];
     if (KE != KE_VERTEX) {
-      double uk[CW];
 #pragma unroll
-      for (int k = 0; k < CW; ++k) uk[k] = u[(size_t)ce[k] * M + mm];
-#pragma unroll
-      for (int k = 0; k < CW; ++k) K += kin[k] * (uk[k] * uk[k]);
-      B = K + T.gravity * hi;
-    } else {
-      B = T.gravity * hi;  // the reference's zero cell part adds exactly 0
+      for (int k = 0; k < CW; ++k) ld_members<R, P>(u + (size_t)ce[k] * M + mm, uk[k]);
     }
     if (KE != KE_CELL) {
-      double kv[CW];
 #pragma unroll
-      for (int k = 0; k < CW; ++k) kv[k] = W.Kv[(size_t)cv[k] * M + mm];
-      double s = 0.0;
-#pragma unroll
-      for (int k = 0; k < CW; ++k) s += kk[k] * kv[k];
-      K += s;
-      B += s;
+      for (int k = 0; k < CW; ++k) ld_members<R, P>(W.Kv + (size_t)cv[k] * M + mm, kv[k]);
     }
-    W.B[o] = (R)B;
-    if (want_K) W.K[o] = (R)K;
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      double K = 0.0, B;
+      if (KE != KE_VERTEX) {
+#pragma unroll
+        for (int k = 0; k < CW; ++k) K += kin[k] * (uk[k][p] * uk[k][p]);
+        B = K + T.gravity * hi[p];
+      } else {
+        B = T.gravity * hi[p];  // the reference's zero cell part adds exactly 0
+      }
+      if (KE != KE_CELL) {
+        double s = 0.0;
+#pragma unroll
+        for (int k = 0; k < CW; ++k) s += kk[k] * kv[k][p];
+        K += s;
+        B += s;
+      }
+      Kc[p] = K;
+      Bc[p] = B;
+    }
+    st_members<R, P>(W.B + o, Bc);
+    if (want_K) st_members<R, P>(W.K + o, Kc);
   }
 }
 

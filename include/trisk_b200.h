@@ -275,9 +275,14 @@ int trisk_ensemble_energy(TriskEnsemble* ensemble, int32_t group, double* energi
  * at the two cells; 7 geometry values (`geometry`, ne x 7 in file edge order); normalized
  * as (x - mean) * scale with norm = [24 means, 24 scales, sF, sQ], then rounded to BF16.
  * TRiSK PV flux only.
+ * flags: bit 0 (1) runs the network at every RK4 stage instead of once per step; bit 1 (2)
+ * makes the momentum correction work-free per member: its component along the energy
+ * gradient dE/du_e = u_e l_e (h_c0 d_c0 + h_c1 d_c1) (cell kinetic energy; l, d and the two
+ * cell distances are geometry columns 0..3) is removed, so it does no work on the flow to
+ * first order.
  * net = NULL removes the group's closure. */
 int trisk_ensemble_set_closure(TriskEnsemble* ensemble, int32_t group, TriskClosure* net, const float* geometry,
-                               const double* norm, int32_t every_stage);
+                               const double* norm, int32_t flags);
 int trisk_ensemble_closure_mask(TriskEnsemble* ensemble, int32_t group, const float* member_on);
 /* The features of the group's current member states into X (device, rows e * M + m in file
  * edge order, 24 BF16 each), for training data. */

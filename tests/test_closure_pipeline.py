@@ -64,6 +64,24 @@ def test_closure_pipeline_small(require_gpu, tendency_targets):
     masked.closure_mask(0, np.zeros(3))
     masked.run(40)
     assert np.array_equal(plain.get_member(0, 1), masked.get_member(0, 1))
+    # the work-free option removes the correction's power: over one short step (1 s, so the
+    # first-order change dominates) the energy changes far less than with the same
+    # (amplified, momentum-only) correction without it
+    strong = np.array(norm, dtype=np.float64)
+    strong[48], strong[49] = 0.0, 10.0 * strong[49]
+    de = {}
+    for wf in (False, True, None):
+        one = d.Ensemble([(m, 3, 1.0, 1)])
+        for k in range(3):
+            col.copy_(init[:, k])
+            one.set_member(0, k, col)
+        if wf is not None:
+            one.set_closure(0, mlp, edge_geometry(gc), strong, work_free=wf)
+        one.run(1)
+        de[wf] = one.energy(0)
+    power_free = np.abs(de[True] - de[None])
+    power = np.abs(de[False] - de[None])
+    assert np.all(power > 0) and np.all(power_free <= 0.05 * power), (power_free, power)
 
 
 def test_run_coarse_reports_errors(require_gpu):
