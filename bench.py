@@ -14,6 +14,11 @@ kinetic energy, FP64, dt = 75 s, a seeded synthetic height/wind state on the Ear
          measured HBM copy bandwidth.
   cpu_baseline  the CPU oracle (a C restatement of the reference kernels, not Julia) on
          all host cores, over a bounded sample of the same workload.
+  ensemble  64 x hexagon 5 + 32 x hexagon 6 + 8 x hexagon 7 in one persistent CUDA-graph
+         launch per phase, one simulated day each (FP64, and FP32 state).
+  closure  128 x hexagon 6 with the learned closure (FP32 state) for one simulated day, the
+         same without it, one plain hexagon-8 member, and the committed closure errors.
+  hexagon5  the reference's CPU-runnable case: CPU restatement and B200, 100 steps.
 
 --impl reference times that CPU restatement alone (the reference itself is Julia, which
 is not installed). With N > 1 GPUs (torchrun) every rank runs an independent replica.
