@@ -29,7 +29,7 @@ struct GroupDesc {
   int startV, nV;
   int startF, nEF, nCF;
   int startT, nET, nCT;
-  int P;  // members per thread in the vertex and flux phases (2 when M is even, else 1)
+  int P;  // members per thread in the three phases (2 when M is even, else 1)
 };
 
 struct GroupSet {
@@ -107,10 +107,16 @@ __global__ void __launch_bounds__(256, 4) kg_tend(const GroupSet G) {  // <= 64 
     S.flag = G.flag;
     S.c = EPI == EPI_STAGE3 ? D.dt : D.dt / 2;
     S.sixth = D.dt / 6;
-    if (D.W.dq)
+    if (D.P == 2) {
+      if (D.W.dq)
+        tend_body_p<PV, EPI, true, R, 2>(D.T, work_as<R>(D.W), S, D.M, D.nET, vb - D.startT);
+      else
+        tend_body_p<PV, EPI, false, R, 2>(D.T, work_as<R>(D.W), S, D.M, D.nET, vb - D.startT);
+    } else if (D.W.dq) {
       tend_body<PV, EPI, true, true, R>(D.T, work_as<R>(D.W), S, D.M, D.nET, vb - D.startT);
-    else
+    } else {
       tend_body<PV, EPI, true, false, R>(D.T, work_as<R>(D.W), S, D.M, D.nET, vb - D.startT);
+    }
   }
 }
 
@@ -553,8 +559,8 @@ int trisk_ensemble_create_precision(TriskModel* const* models, const int32_t* me
     D.nV = (int)cdiv(m->nv * M / D.P, B);
     D.nEF = (int)cdiv(m->ne * M / D.P, B);
     D.nCF = (int)cdiv(m->nc * M / D.P, B);
-    D.nET = (int)cdiv(m->ne * M, B);
-    D.nCT = (int)cdiv(m->nc * M, B);
+    D.nET = (int)cdiv(m->ne * M / D.P, B);
+    D.nCT = (int)cdiv(m->nc * M / D.P, B);
     D.startV = sV;
     D.startF = sF;
     D.startT = sT;

@@ -532,6 +532,163 @@ __device__ __forceinline__ void tend_body(const DevTables& T, const DevWorkT<R>&
   }
 }
 
+// The RK4 epilogue for P consecutive members at j (vector loads and stores of the stage
+// vectors; per member the arithmetic of epilogue<EPI>).
+template <int EPI, class R, int P>
+__device__ __forceinline__ void epilogue_p(const DevStageT<R>& S, size_t j, const double (&kv)[P]) {
+  if constexpr (P == 1) {
+    epilogue<EPI, R>(S, j, kv[0]);
+  } else {
+    double y[P], a[P], st[P], acc[P];
+    if (EPI == EPI_TENDENCY) {
+      st_members<R, P>(S.dy + j, kv);
+      return;
+    }
+    ld_members<R, P>(S.y + j, y);
+    if (EPI == EPI_STAGE2 || EPI == EPI_STAGE3 || EPI == EPI_STAGE4) ld_members<R, P>(S.acc + j, a);
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      if (EPI == EPI_STAGE1) {
+        acc[p] = kv[p];
+        st[p] = y[p] + S.c * kv[p];
+      } else if (EPI == EPI_STAGE2 || EPI == EPI_STAGE3) {
+        acc[p] = a[p] + 2 * kv[p];
+        st[p] = y[p] + S.c * kv[p];
+      } else {
+        st[p] = y[p] + S.sixth * (a[p] + kv[p]);
+      }
+    }
+    if (EPI == EPI_STAGE4) {
+      R out[P];
+      bool bad = false;
+#pragma unroll
+      for (int p = 0; p < P; ++p) {
+        out[p] = (R)st[p];
+        bad |= !isfinite(out[p]);
+      }
+      st_members<R, P>(S.y + j, st);
+      if (bad) atomicOr(S.flag, 1);
+    } else {
+      st_members<R, P>(S.acc + j, acc);
+      st_members<R, P>(S.st + j, st);
+    }
+  }
+}
+
+// The tendency phase of an ensemble group with P members per thread: as tend_body, with the
+// stencil sums accumulated while the stencil streams (same order per member), so that two
+// members fit the register budget.
+template <int PV, int EPI, bool CL, class R, int P>
+__device__ __forceinline__ void tend_body_p(const DevTables& T, const DevWorkT<R>& W, const DevStageT<R>& S,
+                                            int M, int nbE, int vb) {
+  if (vb < nbE) {
+    int e, mm;
+    split_p<true, P>(vb * blockDim.x + threadIdx.x, M, e, mm);
+    if (e >= T.ne) return;
+    const int ec0 = ldt<false>(T, T.edge_cells, e), ec1 = ldt<false>(T, T.edge_cells, T.lde + e);
+    const double invd = ldt<false>(T, T.inverse_dual, e);
+    const size_t o = (size_t)e * M + mm;
+    double s[P], du[P];
+    if (PV == PVM_TRISK) {
+      pdl_wait();
+      double qself[P];
+      ld_members<R, P>(W.qe + o, qself);
+#pragma unroll
+      for (int p = 0; p < P; ++p) s[p] = 0.0;
+#pragma unroll
+      for (int k = 0; k < TWD; ++k) {
+        const int te = ldt<false>(T, T.trisk_edges, k * T.lde + e);
+        const double tr = ldt<false>(T, T.trisk, k * T.lde + e);
+        double f[P], q[P];
+        ld_members<R, P>(W.F + (size_t)te * M + mm, f);
+        ld_members<R, P>(W.qe + (size_t)te * M + mm, q);
+#pragma unroll
+        for (int p = 0; p < P; ++p) s[p] += tr * f[p] * (qself[p] + q[p]);
+      }
+      double b0[P], b1[P];
+      ld_members<R, P>(W.B + (size_t)ec0 * M + mm, b0);
+      ld_members<R, P>(W.B + (size_t)ec1 * M + mm, b1);
+#pragma unroll
+      for (int p = 0; p < P; ++p) du[p] = s[p] / 2 - (b1[p] - b0[p]) * invd;
+    } else {
+      pdl_wait();
+      double qself[P], q0[P], q3[P], q6[P], q9[P];
+      if (PV == PVM_GASSMANN_MEAN) ld_members<R, P>(W.qe + o, qself);
+      if (PV == PVM_GASSMANN_DERIVED) {
+        const int g0 = ldt<false>(T, T.g_edges, e), g3 = ldt<false>(T, T.g_edges, 3 * T.lde + e);
+        const int g6 = ldt<false>(T, T.g_edges, 6 * T.lde + e), g9 = ldt<false>(T, T.g_edges, 9 * T.lde + e);
+        ld_members<R, P>(W.qe + (size_t)g0 * M + mm, q0);
+        ld_members<R, P>(W.qe + (size_t)g3 * M + mm, q3);
+        ld_members<R, P>(W.qe + (size_t)g6 * M + mm, q6);
+        ld_members<R, P>(W.qe + (size_t)g9 * M + mm, q9);
+      }
+#pragma unroll
+      for (int p = 0; p < P; ++p) s[p] = 0.0;
+#pragma unroll
+      for (int k = 0; k < GW; ++k) {
+        const int ge = ldt<false>(T, T.g_edges, k * T.lde + e);
+        const double gw = ldt<false>(T, T.g_weights, k * T.lde + e);
+        double f[P], q[P];
+        ld_members<R, P>(W.F + (size_t)ge * M + mm, f);
+        if (PV == PVM_GASSMANN_DERIVED) {
+          const int src = derived_pv_source(k);
+#pragma unroll
+          for (int p = 0; p < P; ++p) q[p] = src == 0 ? q0[p] : (src == 3 ? q3[p] : (src == 6 ? q6[p] : q9[p]));
+        } else if (PV == PVM_GASSMANN) {
+          const int gp = ldt<false>(T, T.g_pv_edges, k * T.lde + e);
+          ld_members<R, P>(W.qe + (size_t)gp * M + mm, q);
+        } else {
+          double qk[P];
+          ld_members<R, P>(W.qe + (size_t)ge * M + mm, qk);
+#pragma unroll
+          for (int p = 0; p < P; ++p) q[p] = (qself[p] + qk[p]) / 2;
+        }
+#pragma unroll
+        for (int p = 0; p < P; ++p) s[p] += gw * f[p] * q[p];
+      }
+      double b0[P], b1[P];
+      ld_members<R, P>(W.B + (size_t)ec0 * M + mm, b0);
+      ld_members<R, P>(W.B + (size_t)ec1 * M + mm, b1);
+#pragma unroll
+      for (int p = 0; p < P; ++p) du[p] = s[p] - (b1[p] - b0[p]) * invd;
+    }
+    if (CL) {  // learned momentum correction
+      double dqo[P];
+      ld_members<R, P>(W.dq + o, dqo);
+#pragma unroll
+      for (int p = 0; p < P; ++p) du[p] += dqo[p];
+    }
+    epilogue_p<EPI, R, P>(S, o, du);
+  } else {
+    int i, mm;
+    split_p<true, P>((vb - nbE) * blockDim.x + threadIdx.x, M, i, mm);
+    if (i >= T.nc) return;
+    pdl_wait();
+    double s[P];
+#pragma unroll
+    for (int p = 0; p < P; ++p) s[p] = 0.0;
+#pragma unroll
+    for (int k = 0; k < CW; ++k) {
+      const int ce = ldt<false>(T, T.cell_edges, k * T.ldc + i);
+      const double dv = ldt<false>(T, T.divergence, k * T.ldc + i);
+      double f[P];
+      ld_members<R, P>(W.F + (size_t)ce * M + mm, f);
+      if (CL) {
+        double df[P];
+        ld_members<R, P>(W.dF + (size_t)ce * M + mm, df);
+#pragma unroll
+        for (int p = 0; p < P; ++p) f[p] += df[p];
+      }
+#pragma unroll
+      for (int p = 0; p < P; ++p) s[p] += dv * f[p];
+    }
+    double dh[P];
+#pragma unroll
+    for (int p = 0; p < P; ++p) dh[p] = -s[p];
+    epilogue_p<EPI, R, P>(S, (size_t)T.ne * M + (size_t)i * M + mm, dh);
+  }
+}
+
 template <int PV, int EPI, bool ENS, bool KEEP = false>
 __global__ void __launch_bounds__(256) k_tend(DevTables T, DevWork W, DevStage S, int M, int nbE) {
   pdl_trigger();
