@@ -148,3 +148,34 @@ def test_fp32_state_ensemble(require_gpu, pv, ke):
     with pytest.raises(d.TriskError) as err:
         e32.run(1)
     assert err.value.status == 4
+
+
+@pytest.mark.parametrize("state_bits", [64, 32])
+def test_closure_two_members_per_thread(require_gpu, state_bits):
+    """The closure path with two members per thread (an even member count) against one member
+    per thread (an odd count): the network is row-wise, so every member is bit-identical."""
+    from dmplex_b200.closure import ClosureMLP
+    from dmplex_b200.coarsen import edge_geometry
+    si = w.si_parameters()
+    g = trisk_grid(3, True)
+    m = d.TRiSKShallowWater(g, pv_flux="trisk", kinetic_energy="cell", **si)
+    states = member_states(g, 5, 13)
+    net = ClosureMLP(seed=3)
+    u = np.abs(states[0][:g.ne]).mean()
+    norm = np.concatenate([np.zeros(24), np.ones(24), [1e-3 * u, 1e-3 * u / 3600]])
+    out = {}
+    for M in (4, 5):
+        ens = d.Ensemble([(m, M, 150.0, 6)], state_bits=state_bits)
+        for k in range(M):
+            ens.set_member(0, k, states[k])
+        ens.set_closure(0, net, edge_geometry(g), norm)
+        ens.run(6)
+        ens.closure_check()
+        out[M] = [ens.get_member(0, k) for k in range(4)]
+    plain = d.Ensemble([(m, 4, 150.0, 6)], state_bits=state_bits)
+    for k in range(4):
+        plain.set_member(0, k, states[k])
+    plain.run(6)
+    for k in range(4):
+        assert np.array_equal(out[4][k], out[5][k]), k
+        assert not np.array_equal(out[4][k], plain.get_member(0, k))
