@@ -142,7 +142,8 @@ __global__ void kg_features(DevTables T, DevWorkT<R> W, const R* y, int M, const
                             const FeatureNorm N, __nv_bfloat16* X, const int32_t* row_map, int64_t rows) {
   const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (r >= rows) return;
-  const int e = (int)(r / M), m = (int)(r - (int64_t)e * M);
+  int e, m;  // rows < 2^31 (checked when the ensemble is made)
+  split<true>((int)r, M, e, m);
   const R* u = y;
   const R* h = y + (size_t)T.ne * M;
   double f[NFEAT];
@@ -168,8 +169,14 @@ __global__ void kg_features(DevTables T, DevWorkT<R> W, const R* y, int M, const
 #pragma unroll
   for (int k = 0; k < NGEOM; ++k) f[17 + k] = geom[(size_t)e * NGEOM + k];
   const int64_t out = row_map ? (int64_t)row_map[e] * M + m : r;
+  // the row's 48 bytes as three 16-byte stores (rows are 16-byte aligned)
+  __align__(16) __nv_bfloat16 b[NFEAT];
 #pragma unroll
-  for (int k = 0; k < NFEAT; ++k) X[out * NFEAT + k] = __float2bfloat16_rn((float)((f[k] - N.mean[k]) * N.scale[k]));
+  for (int k = 0; k < NFEAT; ++k) b[k] = __float2bfloat16_rn((float)((f[k] - N.mean[k]) * N.scale[k]));
+  uint4* dst = reinterpret_cast<uint4*>(X + out * NFEAT);
+  const uint4* src = reinterpret_cast<const uint4*>(b);
+#pragma unroll
+  for (int c = 0; c < NFEAT / 8; ++c) dst[c] = src[c];
 }
 
 // dF = on[m] sF y0 (mass flux: added to F in the flux-form continuity equation only, so
@@ -180,7 +187,9 @@ __global__ void kg_closure_apply(R* dF, R* dq, const float* Y, const float* memb
                                  double sF, double sQ) {
   const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (r >= rows) return;
-  const double on = member_on[r % M];
+  int e, m;
+  split<true>((int)r, M, e, m);
+  const double on = member_on[m];
   dF[r] = (R)(on * sF * (double)Y[2 * r]);
   dq[r] = (R)(on * sQ * (double)Y[2 * r + 1]);
 }
@@ -231,7 +240,8 @@ __global__ void kg_work_project(DevTables T, const R* y, R* dq, const float* geo
                                 const double* sums) {
   const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (r >= rows) return;
-  const int e = (int)(r / M), m = (int)(r - (int64_t)e * M);
+  int e, m;
+  split<true>((int)r, M, e, m);
   const double gg = sums[2 * m + 1];
   if (!(gg > 0.0)) return;
   const R* h = y + (size_t)T.ne * M;
@@ -788,6 +798,7 @@ int trisk_ensemble_features(TriskEnsemble* ens, int32_t group, void* X, const do
   TRISK_API_BEGIN
   TriskEnsemble& e = *checked_e(ens);
   if (group < 0 || group >= e.G.n || !X || !norm || !geometry) throw Error(TRISK_ERR_ARGUMENT, "bad argument");
+  if (reinterpret_cast<uintptr_t>(X) % 16) throw Error(TRISK_ERR_ARGUMENT, "X must be 16-byte aligned");
   TriskModel& m = *e.models[group];
   if (m.pv != PVM_TRISK) throw Error(TRISK_ERR_UNSUPPORTED, "the closure's features need the TRiSK PV flux");
   DeviceGuard guard(e.device);

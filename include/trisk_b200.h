@@ -284,8 +284,8 @@ int trisk_ensemble_energy(TriskEnsemble* ensemble, int32_t group, double* energi
 int trisk_ensemble_set_closure(TriskEnsemble* ensemble, int32_t group, TriskClosure* net, const float* geometry,
                                const double* norm, int32_t flags);
 int trisk_ensemble_closure_mask(TriskEnsemble* ensemble, int32_t group, const float* member_on);
-/* The features of the group's current member states into X (device, rows e * M + m in file
- * edge order, 24 BF16 each), for training data. */
+/* The features of the group's current member states into X (device, 16-byte aligned, rows
+ * e * M + m in file edge order, 24 BF16 each), for training data. */
 int trisk_ensemble_features(TriskEnsemble* ensemble, int32_t group, void* X, const double* norm,
                             const float* geometry);
 /* TRISK_ERR_TIMEOUT if a bounded tensor-core wait of a closure network gave up. */
