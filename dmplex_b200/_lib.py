@@ -130,6 +130,9 @@ def _load():
         "trisk_closure_stream": (C.c_int, [_p, C.POINTER(_p)]),
         "trisk_ensemble_create": (C.c_int, [_p, _p, _p, _p, _i32, C.POINTER(_p)]),
         "trisk_ensemble_create_precision": (C.c_int, [_p, _p, _p, _p, _i32, _i32, C.POINTER(_p)]),
+        "trisk_ensemble_set_block": (C.c_int, [_p, _p]),
+        "trisk_ensemble_get_block": (C.c_int, [_p, _p]),
+        "trisk_ensemble_autotune": (C.c_int, [_p, _i32, C.POINTER(_f64)]),
         "trisk_ensemble_destroy": (None, [_p]),
         "trisk_ensemble_set_member": (C.c_int, [_p, _i32, _i32, _p]),
         "trisk_ensemble_get_member": (C.c_int, [_p, _i32, _i32, _p]),

@@ -312,7 +312,7 @@ struct TriskEnsemble {
   cudaEvent_t caller_ev = nullptr;  // for order_after_caller
   bool fp32 = false;                // state and work vectors stored as float (arithmetic FP64)
   int pv = 0, ke = 0;
-  int block = 128;
+  int block[3] = {128, 128, 128};  // threads per block of the vertex, flux and tendency phases
   int grid[3] = {0, 0, 0};
   GroupSet G{};
   ClosureSlot cl[trisk::MAX_GROUPS];
@@ -386,10 +386,10 @@ void with_real(const TriskEnsemble& e, F&& f) {
 }
 
 template <typename... KArgs, typename... Args>
-void elaunch(TriskEnsemble& e, void (*kernel)(KArgs...), int grid, bool pdl, Args&&... args) {
+void elaunch(TriskEnsemble& e, void (*kernel)(KArgs...), int phase, bool pdl, Args&&... args) {
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((unsigned)grid);
-  cfg.blockDim = dim3((unsigned)e.block);
+  cfg.gridDim = dim3((unsigned)e.grid[phase]);
+  cfg.blockDim = dim3((unsigned)e.block[phase]);
   cfg.stream = e.stream;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -452,14 +452,14 @@ void enqueue_ensemble_step(TriskEnsemble& e) {
     for (int stage = 1; stage <= 4; ++stage) {
       with_real(e, [&](auto r) {
         using R = decltype(r);
-        elaunch(e, kg_vertex<PV, KE, R>, e.grid[0], stage != 1, e.G, stage == 1 ? 1 : 0);
-        elaunch(e, kg_flux<PV, KE, R>, e.grid[1], true, e.G, stage == 1 ? 1 : 0, 0);
+        elaunch(e, kg_vertex<PV, KE, R>, 0, stage != 1, e.G, stage == 1 ? 1 : 0);
+        elaunch(e, kg_flux<PV, KE, R>, 1, true, e.G, stage == 1 ? 1 : 0, 0);
         if (closure) enqueue_closure(e, stage);
         switch (stage) {
-          case 1: elaunch(e, kg_tend<PV, EPI_STAGE1, R>, e.grid[2], true, e.G); break;
-          case 2: elaunch(e, kg_tend<PV, EPI_STAGE2, R>, e.grid[2], true, e.G); break;
-          case 3: elaunch(e, kg_tend<PV, EPI_STAGE3, R>, e.grid[2], true, e.G); break;
-          default: elaunch(e, kg_tend<PV, EPI_STAGE4, R>, e.grid[2], true, e.G); break;
+          case 1: elaunch(e, kg_tend<PV, EPI_STAGE1, R>, 2, true, e.G); break;
+          case 2: elaunch(e, kg_tend<PV, EPI_STAGE2, R>, 2, true, e.G); break;
+          case 3: elaunch(e, kg_tend<PV, EPI_STAGE3, R>, 2, true, e.G); break;
+          default: elaunch(e, kg_tend<PV, EPI_STAGE4, R>, 2, true, e.G); break;
         }
       });
     }
@@ -495,6 +495,45 @@ void drop_graph(TriskEnsemble& e) {
     cudaGraphExecDestroy(e.graph);
     e.graph = nullptr;
   }
+}
+
+// Virtual blocks of every group per phase for the current block sizes, and the persistent
+// grids (as many blocks as stay resident, never more than the work).
+void layout(TriskEnsemble& e) {
+  int sV = 0, sF = 0, sT = 0;
+  for (int g = 0; g < e.G.n; ++g) {
+    GroupDesc& D = e.G.g[g];
+    const TriskModel& m = *e.models[g];
+    const int64_t M = D.M;
+    D.nV = (int)cdiv(m.nv * M / D.P, e.block[0]);
+    D.nEF = (int)cdiv(m.ne * M / D.P, e.block[1]);
+    D.nCF = (int)cdiv(m.nc * M / D.P, e.block[1]);
+    D.nET = (int)cdiv(m.ne * M / D.P, e.block[2]);
+    D.nCT = (int)cdiv(m.nc * M / D.P, e.block[2]);
+    D.startV = sV;
+    D.startF = sF;
+    D.startT = sT;
+    sV += D.nV;
+    sF += D.nEF + D.nCF;
+    sT += D.nET + D.nCT;
+  }
+  e.G.totalV = sV;
+  e.G.totalF = sF;
+  e.G.totalT = sT;
+  int dev_sms = 0;
+  CUDA_CHECK(cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, e.device));
+  int occ[3] = {1, 1, 1};
+  with_modes_e(e.pv, e.ke, [&](auto pvc, auto kec) {
+    constexpr int PV = decltype(pvc)::value, KE = decltype(kec)::value;
+    with_real(e, [&](auto r) {
+      using R = decltype(r);
+      CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[0], kg_vertex<PV, KE, R>, e.block[0], 0));
+      CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[1], kg_flux<PV, KE, R>, e.block[1], 0));
+      CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[2], kg_tend<PV, EPI_STAGE2, R>, e.block[2], 0));
+    });
+  });
+  const int total[3] = {sV, sF, sT};
+  for (int p = 0; p < 3; ++p) e.grid[p] = std::max(1, std::min(total[p], dev_sms * std::max(occ[p], 1)));
 }
 
 TriskEnsemble* checked_e(TriskEnsemble* e) {
@@ -536,8 +575,6 @@ int trisk_ensemble_create_precision(TriskModel* const* models, const int32_t* me
   DeviceGuard guard(e->device);
   CUDA_CHECK(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
   CUDA_CHECK(cudaEventCreateWithFlags(&e->caller_ev, cudaEventDisableTiming));
-  int sV = 0, sF = 0, sT = 0;
-  const int B = e->block;
   for (int g = 0; g < ngroups; ++g) {
     TriskModel* m = models[g];
     if (!m) throw Error(TRISK_ERR_ARGUMENT, "model is NULL");
@@ -566,17 +603,6 @@ int trisk_ensemble_create_precision(TriskModel* const* models, const int32_t* me
     D.st = e->alloc_state(m->N * M);
     CUDA_CHECK(cudaMemset(D.y, 0, m->N * M * e->esize()));
     D.P = M % 2 == 0 ? 2 : 1;
-    D.nV = (int)cdiv(m->nv * M / D.P, B);
-    D.nEF = (int)cdiv(m->ne * M / D.P, B);
-    D.nCF = (int)cdiv(m->nc * M / D.P, B);
-    D.nET = (int)cdiv(m->ne * M / D.P, B);
-    D.nCT = (int)cdiv(m->nc * M / D.P, B);
-    D.startV = sV;
-    D.startF = sF;
-    D.startT = sT;
-    sV += D.nV;
-    sF += D.nEF + D.nCF;
-    sT += D.nET + D.nCT;
     e->models.push_back(m);
     e->max_state = std::max(e->max_state, m->N);
     e->max_members = std::max(e->max_members, (int)M);
@@ -584,9 +610,6 @@ int trisk_ensemble_create_precision(TriskModel* const* models, const int32_t* me
     e->step_bytes += 4 * (m->table_bytes_unique + 2 * Nb) + 15 * Nb;
   }
   e->G.n = ngroups;
-  e->G.totalV = sV;
-  e->G.totalF = sF;
-  e->G.totalT = sT;
   e->counters = e->alloc<int>(MAX_GROUPS);
   e->flag = e->alloc<int>(1);
   e->staging = e->alloc<double>(e->max_state);
@@ -594,21 +617,7 @@ int trisk_ensemble_create_precision(TriskModel* const* models, const int32_t* me
   CUDA_CHECK(cudaMemset(e->flag, 0, sizeof(int)));
   e->G.counters = e->counters;
   e->G.flag = e->flag;
-  // persistent grids: as many blocks as stay resident, never more than the work
-  int dev_sms = 0;
-  CUDA_CHECK(cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, e->device));
-  int occ[3] = {1, 1, 1};
-  with_modes_e(e->pv, e->ke, [&](auto pvc, auto kec) {
-    constexpr int PV = decltype(pvc)::value, KE = decltype(kec)::value;
-    with_real(*e, [&](auto r) {
-      using R = decltype(r);
-      CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[0], kg_vertex<PV, KE, R>, B, 0));
-      CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[1], kg_flux<PV, KE, R>, B, 0));
-      CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[2], kg_tend<PV, EPI_STAGE2, R>, B, 0));
-    });
-  });
-  const int total[3] = {sV, sF, sT};
-  for (int p = 0; p < 3; ++p) e->grid[p] = std::max(1, std::min(total[p], dev_sms * std::max(occ[p], 1)));
+  layout(*e);
   CUDA_CHECK(cudaDeviceSynchronize());
   *out = e.release();
   TRISK_API_END
@@ -718,6 +727,108 @@ int trisk_ensemble_stream(TriskEnsemble* ens, void** stream) {
 }
 
 int64_t trisk_ensemble_launch_count(TriskEnsemble* ens) { return ens ? ens->launches : -1; }
+
+int trisk_ensemble_set_block(TriskEnsemble* ens, const int32_t block[3]) {
+  TRISK_API_BEGIN
+  TriskEnsemble& e = *checked_e(ens);
+  if (!block) throw Error(TRISK_ERR_ARGUMENT, "NULL argument");
+  for (int p = 0; p < 3; ++p)
+    if (block[p] < 64 || block[p] > 256 || block[p] % 32)
+      throw Error(TRISK_ERR_ARGUMENT, "block sizes must be multiples of 32 in [64, 256]");
+  DeviceGuard guard(e.device);
+  CUDA_CHECK(cudaStreamSynchronize(e.stream));
+  for (int p = 0; p < 3; ++p) e.block[p] = block[p];
+  layout(e);
+  drop_graph(e);
+  TRISK_API_END
+}
+
+int trisk_ensemble_get_block(TriskEnsemble* ens, int32_t block[3]) {
+  TRISK_API_BEGIN
+  TriskEnsemble& e = *checked_e(ens);
+  if (!block) throw Error(TRISK_ERR_ARGUMENT, "NULL argument");
+  for (int p = 0; p < 3; ++p) block[p] = e.block[p];
+  TRISK_API_END
+}
+
+int trisk_ensemble_autotune(TriskEnsemble* ens, int32_t steps, double* best_ms) {
+  TRISK_API_BEGIN
+  TriskEnsemble& e = *checked_e(ens);
+  if (steps <= 0) throw Error(TRISK_ERR_ARGUMENT, "steps must be positive");
+  DeviceGuard guard(e.device);
+  CUDA_CHECK(cudaStreamSynchronize(e.stream));
+  // Times `steps` RK4 steps of all groups for every combination of the three phases' block
+  // sizes and keeps the fastest. The members' states, the step counters and each group's
+  // step count are saved first and restored after every trial and at the end, so the
+  // ensemble continues as if nothing had run (every candidate computes the same numbers).
+  static const int choices[] = {64, 128, 256};
+  std::vector<double*> saved(e.G.n);
+  std::vector<int> nsteps(e.G.n);
+  std::vector<int> counters(MAX_GROUPS);
+  CUDA_CHECK(cudaMemcpy(counters.data(), e.counters, MAX_GROUPS * sizeof(int), cudaMemcpyDeviceToHost));
+  for (int g = 0; g < e.G.n; ++g) {
+    const size_t bytes = (size_t)e.models[g]->N * e.G.g[g].M * e.esize();
+    saved[g] = reinterpret_cast<double*>(e.alloc<char>(bytes));  // freed with the ensemble
+    CUDA_CHECK(cudaMemcpyAsync(saved[g], e.G.g[g].y, bytes, cudaMemcpyDeviceToDevice, e.stream));
+    nsteps[g] = e.G.g[g].nsteps;
+    e.G.g[g].nsteps = steps + 2;  // every group takes part in every timed step
+  }
+  auto restore = [&]() {
+    for (int g = 0; g < e.G.n; ++g) {
+      const size_t bytes = (size_t)e.models[g]->N * e.G.g[g].M * e.esize();
+      CUDA_CHECK(cudaMemcpyAsync(e.G.g[g].y, saved[g], bytes, cudaMemcpyDeviceToDevice, e.stream));
+    }
+    CUDA_CHECK(cudaMemsetAsync(e.counters, 0, MAX_GROUPS * sizeof(int), e.stream));
+  };
+  cudaEvent_t e0, e1;
+  CUDA_CHECK(cudaEventCreate(&e0));
+  CUDA_CHECK(cudaEventCreate(&e1));
+  int best[3] = {e.block[0], e.block[1], e.block[2]};
+  double best_t = INFINITY;
+  try {
+    for (int a : choices)
+      for (int b : choices)
+        for (int c : choices) {
+          e.block[0] = a;
+          e.block[1] = b;
+          e.block[2] = c;
+          layout(e);
+          drop_graph(e);
+          restore();
+          ensure_ensemble_graph(e);
+          for (int s2 = 0; s2 < 2; ++s2) CUDA_CHECK(cudaGraphLaunch(e.graph, e.stream));  // warm-up
+          CUDA_CHECK(cudaEventRecord(e0, e.stream));
+          for (int s2 = 0; s2 < steps; ++s2) CUDA_CHECK(cudaGraphLaunch(e.graph, e.stream));
+          CUDA_CHECK(cudaEventRecord(e1, e.stream));
+          CUDA_CHECK(cudaEventSynchronize(e1));
+          float ms = 0;
+          CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+          if (ms < best_t) {
+            best_t = ms;
+            best[0] = a;
+            best[1] = b;
+            best[2] = c;
+          }
+        }
+  } catch (...) {
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    throw;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  for (int p = 0; p < 3; ++p) e.block[p] = best[p];
+  for (int g = 0; g < e.G.n; ++g) e.G.g[g].nsteps = nsteps[g];
+  layout(e);
+  drop_graph(e);
+  restore();
+  CUDA_CHECK(cudaMemcpyAsync(e.counters, counters.data(), MAX_GROUPS * sizeof(int), cudaMemcpyHostToDevice,
+                             e.stream));
+  CUDA_CHECK(cudaMemsetAsync(e.flag, 0, sizeof(int), e.stream));
+  CUDA_CHECK(cudaStreamSynchronize(e.stream));
+  if (best_ms) *best_ms = best_t / steps;
+  TRISK_API_END
+}
 
 int trisk_ensemble_bytes(TriskEnsemble* ens, double* step_bytes) {
   TRISK_API_BEGIN

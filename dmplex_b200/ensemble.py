@@ -48,6 +48,24 @@ class Ensemble:
         check(lib.trisk_ensemble_get_member(self._h, group, member, _state(y, m)))
         return y
 
+    def autotune(self, steps: int = 10) -> float:
+        """Picks the fastest phase block sizes for these groups (states are left as they
+        were); returns ms per RK4 step."""
+        best = C.c_double()
+        check(lib.trisk_ensemble_autotune(self._h, int(steps), C.byref(best)))
+        return best.value
+
+    def block(self) -> list:
+        b = np.zeros(3, dtype=np.int32)
+        check(lib.trisk_ensemble_get_block(self._h, b.ctypes.data))
+        return b.tolist()
+
+    def set_block(self, block) -> None:
+        b = np.ascontiguousarray(block, dtype=np.int32)
+        if b.shape != (3,):
+            raise ValueError("three block sizes")
+        check(lib.trisk_ensemble_set_block(self._h, b.ctypes.data))
+
     def run_async(self, steps: int) -> None:
         check(lib.trisk_ensemble_run_async(self._h, int(steps)))
 

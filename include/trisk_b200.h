@@ -258,6 +258,16 @@ int trisk_ensemble_steps(TriskEnsemble* ensemble, int64_t* steps_taken); /* per 
 int trisk_ensemble_reset(TriskEnsemble* ensemble);                        /* step counters to 0 */
 int trisk_ensemble_stream(TriskEnsemble* ensemble, void** stream);
 int64_t trisk_ensemble_launch_count(TriskEnsemble* ensemble);
+/* Threads per block of the ensemble's vertex, flux and tendency phases (multiples of 32 in
+ * [64, 256]; default 128 each). */
+int trisk_ensemble_set_block(TriskEnsemble* ensemble, const int32_t block[3]);
+int trisk_ensemble_get_block(TriskEnsemble* ensemble, int32_t block[3]);
+/* Autotuner of the batched path (no reference counterpart): times `steps` RK4 steps of all
+ * groups for every combination of the phase block sizes {64, 128, 256}, keeps the fastest
+ * and restores the members' states, step counters and step counts, so results are unchanged;
+ * best_ms gets the time per step. Each call keeps one copy of the states until the ensemble
+ * is destroyed. */
+int trisk_ensemble_autotune(TriskEnsemble* ensemble, int32_t steps, double* best_ms);
 /* Algorithmic bytes of one RK4 step of all groups: sum 4 (T + 2 M N) + 15 M N. */
 int trisk_ensemble_bytes(TriskEnsemble* ensemble, double* step_bytes);
 /* Per-member total energy sum_i A_i h_i (K_i + g h_i / 2) of a group (M values, host),

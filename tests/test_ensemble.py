@@ -179,3 +179,43 @@ def test_closure_two_members_per_thread(require_gpu, state_bits):
     for k in range(4):
         assert np.array_equal(out[4][k], out[5][k]), k
         assert not np.array_equal(out[4][k], plain.get_member(0, k))
+
+
+def test_ensemble_autotune_keeps_results(require_gpu):
+    """The batched path's autotuner times block-size combinations on the members' own states
+    and restores them (states, step counters, step counts): the run afterwards is bit for
+    bit the run without it, and other block sizes give the same numbers too."""
+    si = w.si_parameters()
+    grids = [trisk_grid(n, True) for n in (3, 4)]
+    models = [d.TRiSKShallowWater(g, pv_flux="gassmann", kinetic_energy="vertex", **si) for g in grids]
+    dts = [w.courant_dt(g) for g in grids]
+    states = [member_states(g, k, s) for g, k, s in zip(grids, (4, 3), (21, 22))]
+
+    def fresh():
+        ens = d.Ensemble([(m, k, dt, 4) for m, k, dt in zip(models, (4, 3), dts)])
+        for gi, group in enumerate(states):
+            for k, y in enumerate(group):
+                ens.set_member(gi, k, y)
+        return ens
+
+    ref = fresh()
+    ref.run(2)
+    tuned = fresh()
+    tuned.run(2)
+    ms = tuned.autotune(3)
+    assert ms > 0 and all(b in (64, 128, 256) for b in tuned.block())
+    assert tuned.steps_taken() == [2, 2]
+    ref.run(3)
+    tuned.run(3)
+    assert tuned.steps_taken() == [4, 4]
+    for gi, group in enumerate(states):
+        for k in range(len(group)):
+            assert np.array_equal(tuned.get_member(gi, k), ref.get_member(gi, k)), (gi, k)
+    other = fresh()
+    other.set_block([64, 256, 96])
+    other.run(4)
+    for gi, group in enumerate(states):
+        for k in range(len(group)):
+            assert np.array_equal(other.get_member(gi, k), ref.get_member(gi, k)), (gi, k)
+    with pytest.raises(d.TriskError):
+        other.set_block([32, 128, 128])
