@@ -36,6 +36,14 @@ class TriskError(RuntimeError):
         self.status = status
 
 
+class TriskIconTables(C.Structure):
+    _fields_ = [("nc", _i64), ("ne", _i64), ("nv", _i64), ("vw", _i32), ("gravity", _f64)] + [
+        (n, _p) for n in ("cell_edges", "divergence", "bilinear", "edge_cells", "edge_vertices", "edge_height",
+                          "gradient", "inverse_dual", "rbf_edges", "rbf", "edge_coriolis", "vertex_edges", "curl",
+                          "cell_areas", "divergence_damping")
+    ]
+
+
 class TriskPlex(C.Structure):
     _fields_ = [("nc", _i64), ("ne", _i64), ("nv", _i64), ("ncones", _i64)] + [
         (n, _p)
@@ -87,6 +95,12 @@ def _load():
         "trisk_abi_version": (_i32, []),
         "trisk_struct_size": (_i32, [_i32]),
         "trisk_mesh_create_hexagon": (C.c_int, [_i32, _i32, _f64, C.POINTER(_p)]),
+        "trisk_mesh_create_triangles": (C.c_int, [_i32, _i32, _f64, C.POINTER(_p)]),
+        "trisk_icon_create": (C.c_int, [_p, _i32, C.POINTER(_p)]),
+        "trisk_icon_destroy": (None, [_p]),
+        "trisk_icon_tendency": (C.c_int, [_p, _p, _p]),
+        "trisk_icon_rk4_step": (C.c_int, [_p, _p, _f64, _i64]),
+        "trisk_icon_launch_count": (_i64, [_p]),
         "trisk_icosahedral_mesh": (C.c_int, [_i32, _i32, _f64, _p, _p]),
         "trisk_lloyd": (C.c_int, [_p, _i64, _p, _i64, _i32, _i32, C.POINTER(_i32)]),
         "trisk_mesh_destroy": (None, [_p]),
@@ -158,7 +172,7 @@ def _load():
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
-    for which, cls in enumerate((TriskGrid, TriskCoefficients, TriskConfig, TriskPlex)):
+    for which, cls in enumerate((TriskGrid, TriskCoefficients, TriskConfig, TriskPlex, TriskIconTables)):
         if lib.trisk_struct_size(which) != C.sizeof(cls):
             raise ImportError(f"{cls.__name__}: binding size {C.sizeof(cls)} != library size "
                               f"{lib.trisk_struct_size(which)}")

@@ -464,6 +464,23 @@ HexMesh create_hexagon_mesh(int subdivisions, bool centroidal, double spring_bet
   return hm;
 }
 
+HexMesh create_triangle_mesh(int subdivisions, bool centroidal, double spring_beta) {
+  // create_spherical_mesh (Icosahedral.jl:22-61) as the cells, their circumcenters as the
+  // cell centers (the default of a triangle mesh, CellCenters.jl:37-42)
+  TriangleMesh tm = icosahedral_triangles(subdivisions, centroidal, spring_beta);
+  HexMesh m;
+  m.plex = plex_from_polygons(as_polygons(tm.triangles), tm.x);
+  m.generators.resize(m.plex.nc);
+#pragma omp parallel for schedule(static)
+  for (int64_t c = 0; c < m.plex.nc; ++c) {
+    auto v = m.plex.cell_vertices(c);
+    V3 a = m.plex.coordinates[m.plex.vertex_index(v[0])], b = m.plex.coordinates[m.plex.vertex_index(v[1])],
+       d = m.plex.coordinates[m.plex.vertex_index(v[2])];
+    m.generators[c] = normalize(cross(b - a, d - a));
+  }
+  return m;
+}
+
 // ---------------------------------------------------------------------------------------
 // Hilbert ordering (src/Topology/Ordering.jl)
 

@@ -105,6 +105,9 @@ struct HexMesh {
   std::vector<V3> generators;
 };
 HexMesh create_hexagon_mesh(int subdivisions, bool centroidal, double spring_beta = 0.0);
+// The triangles of create_spherical_mesh as cells (the ICON C grid), with their circumcenters
+// as `generators` (the cell centers).
+HexMesh create_triangle_mesh(int subdivisions, bool centroidal, double spring_beta = 0.0);
 
 // 3-D Hilbert key (Ordering.jl:10-41) and the cell permutation (Ordering.jl:85-92).
 uint64_t hilbert_key(uint64_t x0, uint64_t x1, uint64_t x2, int bits);

@@ -63,6 +63,7 @@ int32_t trisk_struct_size(int32_t which) {
     case 1: return (int32_t)sizeof(TriskCoefficients);
     case 2: return (int32_t)sizeof(TriskConfig);
     case 3: return (int32_t)sizeof(TriskPlex);
+    case 4: return (int32_t)sizeof(TriskIconTables);
     default: return -1;
   }
 }
@@ -76,6 +77,25 @@ int trisk_mesh_create_hexagon(int32_t subdivisions, int32_t centroidal, double s
   if (!(spring_beta >= 0)) throw trisk::Error(TRISK_ERR_ARGUMENT, "spring_beta must be >= 0");
   auto m = std::make_unique<TriskMesh>();
   m->hex = trisk::create_hexagon_mesh(subdivisions, centroidal != 0, spring_beta);
+  const trisk::Plex& p = m->hex.plex;
+  m->cone_offsets = plus_one(p.cone_offsets);
+  m->cones = plus_one(p.cones);
+  m->orientations.assign(p.orientations.begin(), p.orientations.end());
+  m->support_offsets = plus_one(p.support_offsets);
+  m->supports = plus_one(p.supports);
+  *out = m.release();
+  TRISK_API_END
+}
+
+int trisk_mesh_create_triangles(int32_t subdivisions, int32_t centroidal, double spring_beta, TriskMesh** out) {
+  TRISK_API_BEGIN
+  if (!out) throw trisk::Error(TRISK_ERR_ARGUMENT, "out is NULL");
+  *out = nullptr;
+  if (subdivisions < 0 || subdivisions > 10)
+    throw trisk::Error(TRISK_ERR_ARGUMENT, "subdivisions must be in 0..10");
+  if (!(spring_beta >= 0)) throw trisk::Error(TRISK_ERR_ARGUMENT, "spring_beta must be >= 0");
+  auto m = std::make_unique<TriskMesh>();
+  m->hex = trisk::create_triangle_mesh(subdivisions, centroidal != 0, spring_beta);
   const trisk::Plex& p = m->hex.plex;
   m->cone_offsets = plus_one(p.cone_offsets);
   m->cones = plus_one(p.cones);

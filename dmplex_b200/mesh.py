@@ -46,10 +46,12 @@ class HexMesh:
     mesh, with the icosahedral vertices (the generators) that the reference's examples
     pass as ``centers``."""
 
+    _CREATE = "trisk_mesh_create_hexagon"
+
     def __init__(self, subdivisions: int, centroidal: bool = False, spring_beta: float | None = None):
         handle = C.c_void_p()
         beta = 0.0 if spring_beta is None else float(spring_beta)
-        check(lib.trisk_mesh_create_hexagon(int(subdivisions), int(bool(centroidal)), beta, C.byref(handle)))
+        check(getattr(lib, self._CREATE)(int(subdivisions), int(bool(centroidal)), beta, C.byref(handle)))
         self._h = handle
         self.subdivisions, self.centroidal, self.spring_beta = int(subdivisions), bool(centroidal), spring_beta
         p = _lib.TriskPlex()
@@ -78,6 +80,19 @@ class HexMesh:
 
 def create_hexagon_mesh(subdivisions: int, centroidal: bool = False, spring_beta: float | None = None) -> HexMesh:
     return HexMesh(subdivisions, centroidal, spring_beta)
+
+
+class TriangleMesh(HexMesh):
+    """create_spherical_mesh(subdivisions; centroidal) with the triangles as cells and their
+    circumcenters as cell centers (``generators``): the ICON C grid (src/Grids/
+    Icosahedral.jl:22-61, CellCenters.jl:37-42)."""
+
+    _CREATE = "trisk_mesh_create_triangles"
+
+
+def create_triangle_mesh(subdivisions: int, centroidal: bool = False,
+                         spring_beta: float | None = None) -> TriangleMesh:
+    return TriangleMesh(subdivisions, centroidal, spring_beta)
 
 
 def icosahedral_mesh(subdivisions: int, centroidal: bool = False, spring_beta: float | None = None):

@@ -43,7 +43,8 @@ enum { TRISK_PV_TRISK = 0, TRISK_PV_GASSMANN = 1, TRISK_PV_GASSMANN_MEAN = 2 };
 size_t trisk_last_error(char* buf, size_t len);
 int32_t trisk_abi_version(void);
 /* sizeof of the structs below, so a binding can check its layout */
-int32_t trisk_struct_size(int32_t which); /* 0 TriskGrid, 1 TriskCoefficients, 2 TriskConfig, 3 TriskPlex */
+int32_t trisk_struct_size(int32_t which); /* 0 TriskGrid, 1 TriskCoefficients, 2 TriskConfig, 3 TriskPlex,
+                                          4 TriskIconTables */
 
 /* ---- mesh generation (set-up, host) ------------------------------------------------
  * Replaces create_hexagon_mesh(n; centroidal)   src/Grids/Hexagonal.jl:11-17
@@ -91,6 +92,10 @@ typedef struct { /* TRiSKGrid (src/FiniteVolumes/TRiSKGrid.jl:37-60) */
 /* spring_beta > 0 relaxes every bisection level by spring dynamics (Icosahedral.jl:49-56,
  * 78-109), 0 leaves it off; centroidal != 0 runs Lloyd's algorithm after every level. */
 int trisk_mesh_create_hexagon(int32_t subdivisions, int32_t centroidal, double spring_beta, TriskMesh** out);
+/* create_spherical_mesh(subdivisions; centroidal) (Icosahedral.jl:22-61) as a mesh whose
+ * cells are the triangles, centers their circumcenters (CellCenters.jl:37-42): the grid of
+ * ICONShallowWater (ICONShallowWater.jl:1-48). The other trisk_mesh_* calls apply. */
+int trisk_mesh_create_triangles(int32_t subdivisions, int32_t centroidal, double spring_beta, TriskMesh** out);
 void trisk_mesh_destroy(TriskMesh* mesh);
 /* The hexagon Plex (views into mesh-owned memory, valid until trisk_mesh_destroy). */
 int trisk_mesh_plex(TriskMesh* mesh, TriskPlex* out);
@@ -228,6 +233,41 @@ int trisk_l2_info(int32_t device, int64_t info[4]);
 /* Runs nsteps RK4 steps on the device-resident state with a CUDA event pair around every
  * kernel launch and returns the mean duration in ms of each phase kernel in ms[3]. */
 int trisk_profile_phases(TriskModel* model, double* y_device, double dt, int64_t nsteps, double ms[3]);
+
+/* ---- ICON triangle shallow water (ICONShallowWater.jl) ----------------
+ * Replaces ICONShallowWater(grid; gravity, coriolis, rbf_scale, divergence_damping,
+ * kinetic_gradient) (src/FiniteVolumes/ICONShallowWater.jl:96-147): the premultiplied
+ * coefficients of that constructor, 1-based Int64 and (entity, k) ordered as Julia holds
+ * them, for a grid of triangles (3 edges per cell, at most 6 edges per vertex, 4-edge RBF
+ * stencils). divergence_damping: nu_4 per edge, or NULL for none. */
+typedef struct {
+  int64_t nc, ne, nv;
+  int32_t vw;
+  double gravity;
+  const int64_t* cell_edges;       /* nc x 3 */
+  const double* divergence;        /* nc x 3: n_{e,i} l_e / A_i */
+  const double* bilinear;          /* nc x 3: e_bln_c_s */
+  const int64_t* edge_cells;       /* ne x 2 */
+  const int64_t* edge_vertices;    /* ne x 2 */
+  const double* edge_height;       /* ne x 2: c_lin_e */
+  const double* gradient;          /* ne x 2: coeff_gradekin */
+  const double* inverse_dual;      /* ne */
+  const int64_t* rbf_edges;        /* ne x 4 */
+  const double* rbf;               /* ne x 4 */
+  const double* edge_coriolis;     /* ne */
+  const int64_t* vertex_edges;     /* nv x vw */
+  const double* curl;              /* nv x vw */
+  const double* cell_areas;        /* nc (diagnostics on the caller's side) */
+  const double* divergence_damping;/* ne or NULL */
+} TriskIconTables;
+typedef struct TriskIconModel TriskIconModel;
+int trisk_icon_create(const TriskIconTables* tables, int32_t device, TriskIconModel** out);
+void trisk_icon_destroy(TriskIconModel* model);
+/* tendency!(dy, y, m) (ICONShallowWater.jl:191-208): host or device pointers. */
+int trisk_icon_tendency(TriskIconModel* model, const double* y, double* dy);
+/* rk4_step!(y, dt, tendency!, cache, m) (RungeKutta.jl:18-29), nsteps times, in place. */
+int trisk_icon_rk4_step(TriskIconModel* model, double* y, double dt, int64_t nsteps);
+int64_t trisk_icon_launch_count(TriskIconModel* model);
 
 /* ---- batched ensembles ------------------------------------------------------------
  * No counterpart in the reference, which runs one model per process (examples/
