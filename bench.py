@@ -19,6 +19,7 @@ kinetic energy, FP64, dt = 75 s, a seeded synthetic height/wind state on the Ear
   closure  128 x hexagon 6 with the learned closure (FP32 state) for one simulated day, the
          same without it, one plain hexagon-8 member, and the committed closure errors.
   hexagon5  the reference's CPU-runnable case: CPU restatement and B200, 100 steps.
+  icon   the ICON triangle model (level 8: 1.31 M triangles), ms per RK4 step.
 
 --impl reference times that CPU restatement alone (the reference itself is Julia, which
 is not installed). With N > 1 GPUs (torchrun) every rank runs an independent replica.
@@ -54,6 +55,7 @@ def parse():
     p.add_argument("--no-closure", action="store_true", help="skip the learned-closure leg")
     p.add_argument("--no-hexagon5", action="store_true", help="skip the hexagon-5 CPU/GPU leg")
     p.add_argument("--ensemble-days", type=float, default=1.0, help="simulated days of the ensemble leg")
+    p.add_argument("--no-icon", action="store_true", help="skip the ICON triangle-model leg")
     p.add_argument("--level", type=int, default=LEVEL, help="mesh level (7 is the benchmark workload)")
     p.add_argument("--block", default=None,
                    help="fixed block sizes of the three phases, e.g. 128,128,64 (skips the autotuner)")
@@ -167,6 +169,35 @@ def run_hexagon5_leg(local_rank, threads, cpu=True):
     out["gpu_step_gbs"] = out["gpu_step_bytes"] / (sec / 1000) / 1e9
     out["note"] = "tables and state (39 MB per step) stay in the 126 MB L2"
     return out
+
+
+def run_icon_leg(local_rank, level=8, steps=100):
+    """ICON triangle shallow water (the reference's ICONShallowWater) on create_triangle_mesh
+    (level), plain bisection — 20 * 4^level triangles, the size of the ICON grid R02B(level - 1): Williamson
+    test case 2 on the unit sphere, dt = 0.2 min d_e, `steps` RK4 steps on a device-resident
+    state, timed around the synchronous call (12 launches per step)."""
+    import torch
+    import dmplex_b200 as d
+    from dmplex_b200.icon import ICONShallowWater
+    g = d.TRiSKGrid(d.create_triangle_mesh(level))
+    m = ICONShallowWater(g, device=local_rank)
+    u0 = 0.2
+    x = g.edge_points
+    u = u0 * (-x[:, 1] * g.edge_normals[:, 0] + x[:, 0] * g.edge_normals[:, 1])
+    h = 1 - (u0 + u0 ** 2 / 2) * g.centers[:, 2] ** 2
+    yd = torch.from_numpy(np.concatenate([u, h])).to(f"cuda:{local_rank}")
+    dt = 0.2 * float(g.dual_lengths.min())
+    m.rk4_step(yd, dt, 5)
+    torch.cuda.synchronize(local_rank)
+    t0 = time.perf_counter()
+    m.rk4_step(yd, dt, steps)
+    torch.cuda.synchronize(local_rank)
+    ms = (time.perf_counter() - t0) * 1e3 / steps
+    return {"workload": f"ICON triangle shallow water, create_triangle_mesh({level}), TC2, FP64",
+            "cells": g.nc, "edges": g.ne, "ms_per_step": ms, "cell_steps_per_s": g.nc / (ms * 1e-3),
+            "published_a100_ms_per_step_same_size": {7: 1.5, 8: 2.4, 9: 7.8}.get(level),
+            "note": "the reference's A100 figure is on the ICON grid file of this size (R02B06/07/08 for "
+                    "levels 7/8/9); this mesh is the icosahedral bisection of the same size"}
 
 
 class ClockSampler:
@@ -506,6 +537,9 @@ def run_b200(args, rank, world, local_rank):
     closure = None
     if not args.no_closure:
         closure = run_closure_leg(local_rank)
+    icon_leg = None
+    if not args.no_icon:
+        icon_leg = run_icon_leg(local_rank)
     hexagon5 = None
     if rank == 0 and not args.no_hexagon5:
         hexagon5 = run_hexagon5_leg(local_rank, os.cpu_count() or 1, cpu=world == 1 and not args.no_cpu_baseline)
@@ -522,7 +556,7 @@ def run_b200(args, rank, world, local_rank):
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": config_dict(g, world, args.level), "clocks": clocks.summary(), "e2e": e2e,
                 "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu, "ensemble": ensemble,
-                "closure": closure, "hexagon5": hexagon5}
+                "closure": closure, "hexagon5": hexagon5, "icon": icon_leg}
         print(json.dumps(line), flush=True)
     del m
 

@@ -40,8 +40,11 @@ struct IconTables {
   const double* curl;            // IVW x ldv
 };
 
+// gh: g (h_r - h_l) / d_e of the stage state, computed in phase 1 so that the fused
+// tendency phase, whose cell threads overwrite the stage state with the next one, never
+// reads heights.
 struct IconWork {
-  double *v, *Ke, *F, *K, *zv, *D, *G;
+  double *v, *Ke, *F, *K, *zv, *D, *G, *gh;
 };
 
 // phase 1, edges (icon_edge_kernel!, ICONShallowWater.jl:149-159): RBF tangential velocity,
@@ -59,14 +62,17 @@ __global__ void __launch_bounds__(256) k_icon_edge(IconTables T, IconWork W, con
   }
   const int c0 = __ldcs(T.edge_cells + e), c1 = __ldcs(T.edge_cells + T.lde + e);
   const double eh0 = __ldcs(T.edge_height + e), eh1 = __ldcs(T.edge_height + T.lde + e);
+  const double invd = __ldcs(T.inverse_dual + e);
   pdl_wait();
   double s = 0.0;
 #pragma unroll
   for (int k = 0; k < IRW; ++k) s += rw[k] * u[re[k]];
   const double ue = u[e];
+  const double hl = h[c0], hr = h[c1];
   W.v[e] = s;
   W.Ke[e] = (ue * ue + s * s) / 2;
-  W.F[e] = (eh0 * h[c0] + eh1 * h[c1]) * ue;
+  W.F[e] = (eh0 * hl + eh1 * hr) * ue;
+  W.gh[e] = T.gravity * (hr - hl) * invd;
 }
 
 // phase 2: cells K = sum bilinear Ke (edge_sum_kernel!, :305-312; kinetic_energy!, :184-189)
@@ -162,7 +168,7 @@ __global__ void __launch_bounds__(256) k_icon_tend(IconTables T, IconWork W, Dev
     const double zeta = (W.zv[v0] + W.zv[v1]) / 2;
     const double Ke = W.Ke[e];
     const double gradK = Ke * (g0 - g1) + g1 * W.K[r] - g0 * W.K[l];
-    double du = (f + zeta) * W.v[e] - gradK - T.gravity * (S.h[r] - S.h[l]) * invd;
+    double du = (f + zeta) * W.v[e] - gradK - W.gh[e];
     if (T.damping) du = du + nu * (-(W.D[r] - W.D[l]) * invd);
     epilogue<EPI>(S, (size_t)e, du);
   } else {
@@ -390,6 +396,7 @@ int trisk_icon_create(const TriskIconTables* t, int32_t device, TriskIconModel**
   W.Ke = m->alloc<double>(t->ne);
   W.F = m->alloc<double>(t->ne);
   W.G = m->alloc<double>(t->ne);
+  W.gh = m->alloc<double>(t->ne);
   W.K = m->alloc<double>(t->nc);
   W.D = m->alloc<double>(t->nc);
   W.zv = m->alloc<double>(t->nv);

@@ -53,12 +53,16 @@ def rbf_coefficients(g: TRiSKGrid, scale: float = 0.5):
     n, x = g.edge_normals, g.edge_points
     ne = g.ne
     ce, cs, ec = g.cell_edges - 1, g.cell_signs, g.edge_cells - 1
-    stencil = np.zeros((ne, 4), dtype=np.int64)
-    for e in range(ne):
-        s = [f for side in range(2) for f, sg in zip(ce[ec[e, side]], cs[ec[e, side]]) if sg != 0 and f != e]
-        if len(s) != 4:
-            raise ValueError("the RBF stencil needs triangles")
-        stencil[e] = s
+    if ce.shape[1] != 3 or np.any(cs == 0):
+        raise ValueError("the RBF stencil needs triangles")
+    parts = []
+    for side in range(2):  # the cell's other two edges, in the cell's order
+        sides = ce[ec[:, side]]                                   # (ne, 3)
+        keep = sides != np.arange(ne)[:, None]
+        if not np.all(keep.sum(1) == 2):
+            raise ValueError("an edge is not a side of its cell")
+        parts.append(sides[keep].reshape(ne, 2))
+    stencil = np.concatenate(parts, axis=1)
 
     def kern(p, q):
         return 1.0 / np.sqrt(1.0 + (_arc_length(p, q) / scale) ** 2)
