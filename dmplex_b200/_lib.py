@@ -96,6 +96,8 @@ def _load():
         "trisk_struct_size": (_i32, [_i32]),
         "trisk_mesh_create_hexagon": (C.c_int, [_i32, _i32, _f64, C.POINTER(_p)]),
         "trisk_mesh_create_triangles": (C.c_int, [_i32, _i32, _f64, C.POINTER(_p)]),
+        "trisk_mesh_from_polygons": (C.c_int, [_p, _p, _i64, _p, _i64, _p, C.POINTER(_p)]),
+        "trisk_mesh_set_centers": (C.c_int, [_p, _p]),
         "trisk_icon_create": (C.c_int, [_p, _i32, C.POINTER(_p)]),
         "trisk_icon_destroy": (None, [_p]),
         "trisk_icon_tendency": (C.c_int, [_p, _p, _p]),

@@ -29,6 +29,15 @@ static std::vector<int64_t> plus_one(const std::vector<int64_t>& v) {
 
 static const double* flat(const std::vector<trisk::V3>& v) { return reinterpret_cast<const double*>(v.data()); }
 
+static void copy_plex(TriskMesh* m) {
+  const trisk::Plex& p = m->hex.plex;
+  m->cone_offsets = plus_one(p.cone_offsets);
+  m->cones = plus_one(p.cones);
+  m->orientations.assign(p.orientations.begin(), p.orientations.end());
+  m->support_offsets = plus_one(p.support_offsets);
+  m->supports = plus_one(p.supports);
+}
+
 static void ensure_grid(TriskMesh* m) {
   if (m->grid_built) return;
   m->grid = trisk::build_grid(m->hex.plex, m->hex.generators);
@@ -77,12 +86,7 @@ int trisk_mesh_create_hexagon(int32_t subdivisions, int32_t centroidal, double s
   if (!(spring_beta >= 0)) throw trisk::Error(TRISK_ERR_ARGUMENT, "spring_beta must be >= 0");
   auto m = std::make_unique<TriskMesh>();
   m->hex = trisk::create_hexagon_mesh(subdivisions, centroidal != 0, spring_beta);
-  const trisk::Plex& p = m->hex.plex;
-  m->cone_offsets = plus_one(p.cone_offsets);
-  m->cones = plus_one(p.cones);
-  m->orientations.assign(p.orientations.begin(), p.orientations.end());
-  m->support_offsets = plus_one(p.support_offsets);
-  m->supports = plus_one(p.supports);
+  copy_plex(m.get());
   *out = m.release();
   TRISK_API_END
 }
@@ -96,13 +100,58 @@ int trisk_mesh_create_triangles(int32_t subdivisions, int32_t centroidal, double
   if (!(spring_beta >= 0)) throw trisk::Error(TRISK_ERR_ARGUMENT, "spring_beta must be >= 0");
   auto m = std::make_unique<TriskMesh>();
   m->hex = trisk::create_triangle_mesh(subdivisions, centroidal != 0, spring_beta);
-  const trisk::Plex& p = m->hex.plex;
-  m->cone_offsets = plus_one(p.cone_offsets);
-  m->cones = plus_one(p.cones);
-  m->orientations.assign(p.orientations.begin(), p.orientations.end());
-  m->support_offsets = plus_one(p.support_offsets);
-  m->supports = plus_one(p.supports);
+  copy_plex(m.get());
   *out = m.release();
+  TRISK_API_END
+}
+
+int trisk_mesh_from_polygons(const int64_t* offsets, const int64_t* vertices, int64_t npolygons,
+                             const double* coordinates, int64_t nv, const double* centers, TriskMesh** out) {
+  // plex_from_polygons(polygons, coordinates) (Plex.jl:49-97), as the grid readers call it
+  // (FileGrids.jl:59,67,91,94)
+  TRISK_API_BEGIN
+  if (!out) throw trisk::Error(TRISK_ERR_ARGUMENT, "out is NULL");
+  *out = nullptr;
+  if (!offsets || !vertices || !coordinates) throw trisk::Error(TRISK_ERR_ARGUMENT, "NULL argument");
+  if (npolygons <= 0 || nv < 3) throw trisk::Error(TRISK_ERR_ARGUMENT, "need at least one polygon and three vertices");
+  if (offsets[0] != 1) throw trisk::Error(TRISK_ERR_ARGUMENT, "offsets[0] must be 1");
+  std::vector<std::vector<int64_t>> polys(npolygons);
+  for (int64_t c = 0; c < npolygons; ++c) {
+    const int64_t a = offsets[c], b = offsets[c + 1];
+    if (b - a < 3) throw trisk::Error(TRISK_ERR_ARGUMENT, "polygon " + std::to_string(c + 1) + " has fewer than three vertices");
+    polys[c].reserve(b - a);
+    for (int64_t i = a; i < b; ++i) {
+      const int64_t v = vertices[i - 1];
+      if (v < 1 || v > nv)
+        throw trisk::Error(TRISK_ERR_ARGUMENT, "polygon " + std::to_string(c + 1) + " names vertex " + std::to_string(v) +
+                                                   " outside 1.." + std::to_string(nv));
+      polys[c].push_back(v - 1);
+    }
+  }
+  std::vector<trisk::V3> x(nv);
+  std::memcpy(x.data(), coordinates, nv * sizeof(trisk::V3));
+  auto m = std::make_unique<TriskMesh>();
+  m->hex.plex = trisk::plex_from_polygons(polys, x);
+  m->hex.generators.resize(npolygons);
+  if (centers) {
+    std::memcpy(m->hex.generators.data(), centers, npolygons * sizeof(trisk::V3));
+  } else {  // the normalized vertex means (CellCenters.jl:35-36); plain means on a plane
+    for (int64_t c = 0; c < npolygons; ++c) {
+      trisk::V3 s{0, 0, 0};
+      for (int64_t v : polys[c]) s = s + x[v];
+      m->hex.generators[c] = m->hex.plex.sphere ? trisk::normalize(s) : s / (double)polys[c].size();
+    }
+  }
+  copy_plex(m.get());
+  *out = m.release();
+  TRISK_API_END
+}
+
+int trisk_mesh_set_centers(TriskMesh* m, const double* centers) {
+  TRISK_API_BEGIN
+  if (!m || !centers) throw trisk::Error(TRISK_ERR_ARGUMENT, "NULL argument");
+  std::memcpy(m->hex.generators.data(), centers, m->hex.generators.size() * sizeof(trisk::V3));
+  m->grid_built = false;  // the next trisk_mesh_grid rebuilds the tables for these centers
   TRISK_API_END
 }
 

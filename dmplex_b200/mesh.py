@@ -1,6 +1,7 @@
 """Mesh generation and TRiSK grid tables (host set-up), mirroring dmplex.jl's
 
     create_hexagon_mesh(n; centroidal)     src/Grids/Hexagonal.jl:11-17
+    plex_from_polygons(polygons, x)        src/Topology/Plex.jl:49-97
     TRiSKGrid(dm; centers)                 src/FiniteVolumes/TRiSKGrid.jl:76-162
     hilbert_permutation(dm)                src/Topology/Ordering.jl:85-92
     vertex_edge_areas(g)                   src/FiniteVolumes/TRiSKGrid.jl:179-191
@@ -52,8 +53,11 @@ class HexMesh:
         handle = C.c_void_p()
         beta = 0.0 if spring_beta is None else float(spring_beta)
         check(getattr(lib, self._CREATE)(int(subdivisions), int(bool(centroidal)), beta, C.byref(handle)))
-        self._h = handle
         self.subdivisions, self.centroidal, self.spring_beta = int(subdivisions), bool(centroidal), spring_beta
+        self._attach(handle)
+
+    def _attach(self, handle) -> None:
+        self._h = handle
         p = _lib.TriskPlex()
         check(lib.trisk_mesh_plex(self._h, C.byref(p)))
         self.plex = Plex(p)
@@ -66,6 +70,15 @@ class HexMesh:
         if getattr(self, "_h", None):
             lib.trisk_mesh_destroy(self._h)
             self._h = None
+
+    def set_centers(self, centers: np.ndarray) -> None:
+        """The cell centers (nc, 3) a TRiSKGrid of this mesh is built from
+        (TRiSKGrid(dm; centers), TRiSKGrid.jl:76-78)."""
+        c = np.ascontiguousarray(centers, dtype=np.float64)
+        if c.shape != (self.nc, 3):
+            raise ValueError(f"centers must have shape ({self.nc}, 3)")
+        check(lib.trisk_mesh_set_centers(self._h, c.ctypes.data))
+        self.generators = c.copy()
 
     def hilbert_permutation(self) -> np.ndarray:
         perm = np.zeros(self.nc, dtype=np.int64)
@@ -93,6 +106,40 @@ class TriangleMesh(HexMesh):
 def create_triangle_mesh(subdivisions: int, centroidal: bool = False,
                          spring_beta: float | None = None) -> TriangleMesh:
     return TriangleMesh(subdivisions, centroidal, spring_beta)
+
+
+class PolygonMesh(HexMesh):
+    """plex_from_polygons(polygons, coordinates) (src/Topology/Plex.jl:49-97): a mesh from
+    arbitrary polygons, as the grid-file readers build it. ``polygons``: a list of 1-based
+    vertex sequences, or an (nc, k) array; ``centers`` (nc, 3): the cell centers of its
+    TRiSKGrid (default: the normalized vertex means; see gridfiles.cell_centers)."""
+
+    def __init__(self, polygons, coordinates: np.ndarray, centers: np.ndarray | None = None):
+        if isinstance(polygons, np.ndarray) and polygons.ndim == 2:
+            sizes = np.full(len(polygons), polygons.shape[1], dtype=np.int64)
+            flat = np.ascontiguousarray(polygons, dtype=np.int64).ravel()
+        else:
+            sizes = np.array([len(p) for p in polygons], dtype=np.int64)
+            flat = np.ascontiguousarray(np.concatenate([np.asarray(p, dtype=np.int64) for p in polygons])
+                                        if len(polygons) else np.zeros(0, np.int64))
+        offsets = np.ascontiguousarray(np.concatenate([[1], 1 + np.cumsum(sizes)]), dtype=np.int64)
+        x = np.ascontiguousarray(coordinates, dtype=np.float64)
+        if x.ndim != 2 or x.shape[1] != 3:
+            raise ValueError("coordinates must have shape (nv, 3)")
+        c = None
+        if centers is not None:
+            c = np.ascontiguousarray(centers, dtype=np.float64)
+            if c.shape != (len(sizes), 3):
+                raise ValueError(f"centers must have shape ({len(sizes)}, 3)")
+        handle = C.c_void_p()
+        check(lib.trisk_mesh_from_polygons(offsets.ctypes.data, flat.ctypes.data, len(sizes), x.ctypes.data,
+                                           len(x), None if c is None else c.ctypes.data, C.byref(handle)))
+        self.subdivisions, self.centroidal, self.spring_beta = None, False, None
+        self._attach(handle)
+
+
+def plex_from_polygons(polygons, coordinates: np.ndarray, centers: np.ndarray | None = None) -> PolygonMesh:
+    return PolygonMesh(polygons, coordinates, centers)
 
 
 def icosahedral_mesh(subdivisions: int, centroidal: bool = False, spring_beta: float | None = None):

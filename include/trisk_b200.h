@@ -96,6 +96,19 @@ int trisk_mesh_create_hexagon(int32_t subdivisions, int32_t centroidal, double s
  * cells are the triangles, centers their circumcenters (CellCenters.jl:37-42): the grid of
  * ICONShallowWater (ICONShallowWater.jl:1-48). The other trisk_mesh_* calls apply. */
 int trisk_mesh_create_triangles(int32_t subdivisions, int32_t centroidal, double spring_beta, TriskMesh** out);
+/* plex_from_polygons(polygons, coordinates) (src/Topology/Plex.jl:49-97), the constructor the
+ * grid-file readers use (src/Grids/FileGrids.jl:52-107). Polygon c (c = 1..npolygons) lists
+ * the 1-based vertices vertices[offsets[c-1]-1 .. offsets[c]-2] (offsets[0] = 1, CSR like the
+ * Plex cones); polygons are turned counter-clockwise and edges numbered by first appearance
+ * as in the reference. coordinates: nv points (3 x nv). centers: nc cell centers for the TRiSK
+ * grid (3 x nc), or NULL for the normalized vertex means; trisk_mesh_set_centers replaces
+ * them. Errors: TRISK_ERR_ARGUMENT for an index outside 1..nv or a polygon of fewer than
+ * three vertices, TRISK_ERR_MESH for a degenerate edge. */
+int trisk_mesh_from_polygons(const int64_t* offsets, const int64_t* vertices, int64_t npolygons,
+                             const double* coordinates, int64_t nv, const double* centers, TriskMesh** out);
+/* Replace the cell centers (3 x nc) that trisk_mesh_grid builds the TRiSK tables from
+ * (TRiSKGrid(dm; centers), TRiSKGrid.jl:76-78); the tables are rebuilt on the next call. */
+int trisk_mesh_set_centers(TriskMesh* mesh, const double* centers);
 void trisk_mesh_destroy(TriskMesh* mesh);
 /* The hexagon Plex (views into mesh-owned memory, valid until trisk_mesh_destroy). */
 int trisk_mesh_plex(TriskMesh* mesh, TriskPlex* out);
