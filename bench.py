@@ -25,6 +25,7 @@ kinetic energy, FP64, dt = 75 s, a seeded synthetic height/wind state on the Ear
 is not installed). With N > 1 GPUs (torchrun) every rank runs an independent replica.
 """
 import argparse
+import ctypes as C
 import json
 import os
 import statistics
@@ -56,6 +57,7 @@ def parse():
     p.add_argument("--no-hexagon5", action="store_true", help="skip the hexagon-5 CPU/GPU leg")
     p.add_argument("--ensemble-days", type=float, default=1.0, help="simulated days of the ensemble leg")
     p.add_argument("--no-icon", action="store_true", help="skip the ICON triangle-model leg")
+    p.add_argument("--no-mpas", action="store_true", help="skip the 3-D MPAS-Gassmann operators leg")
     p.add_argument("--level", type=int, default=LEVEL, help="mesh level (7 is the benchmark workload)")
     p.add_argument("--block", default=None,
                    help="fixed block sizes of the three phases, e.g. 128,128,64 (skips the autotuner)")
@@ -198,6 +200,67 @@ def run_icon_leg(local_rank, level=8, steps=100):
             "published_a100_ms_per_step_same_size": {7: 1.5, 8: 2.4, 9: 7.8}.get(level),
             "note": "the reference's A100 figure is on the ICON grid file of this size (R02B06/07/08 for "
                     "levels 7/8/9); this mesh is the icosahedral bisection of the same size"}
+
+
+def run_mpas_leg(local_rank, level=7, nlev=30, calls=50, cpu_level=5):
+    """The horizontal operators of the 3-D MPAS-Gassmann dycore (slow_tendencies!, flat ground,
+    the reference's ICON-IAP defaults) on create_hexagon_mesh(level) x nlev equidistant layers
+    up to 30 km — the grid of the reference's baroclinic wave — on a perturbed stratified
+    state, device-resident: `calls` calls timed with CUDA events on the library's stream,
+    against the algorithmic bytes of the five phases. The CPU oracle (numpy, one thread) is
+    timed on create_hexagon_mesh(cpu_level) with the same layers."""
+    import torch
+    import dmplex_b200 as d
+    from dmplex_b200 import mpas
+    from oracle.mpas_oracle import MpasOracle
+
+    def case(n):
+        g = d.TRiSKGrid(d.create_hexagon_mesh(n))
+        v = mpas.vertical_grid(nlev, 30000.0)
+        t = mpas.mpas_tables(g, v)
+        rng = np.random.default_rng(11)
+        z = v["z_full"]
+        rho = np.repeat((1.2 * np.exp(-z / 8000.0))[:, None], g.nc, axis=1) * (1 + 1e-3 * rng.standard_normal((nlev, g.nc)))
+        theta = np.repeat((290.0 * np.exp(z / 30000.0))[:, None], g.nc, axis=1)
+        vn = 10 * rng.standard_normal((nlev, g.ne))
+        w = np.zeros((nlev + 1, g.nc))
+        w[1:nlev] = 0.1 * rng.standard_normal((nlev - 1, g.nc))
+        return g, t, (vn, w, rho, rho * theta)
+
+    g, t, state = case(level)
+    ops = mpas.MPASOperators(t, device=local_rank)
+    dev = f"cuda:{local_rank}"
+    ys = [torch.from_numpy(np.ascontiguousarray(x)).to(dev) for x in state]
+    out = ops.work(torch.device(dev))
+    f = ops.fields(*ys, out=out)
+    sp = C.c_void_p()
+    from dmplex_b200._lib import check, lib
+    check(lib.trisk_mpas_stream(ops._h, C.byref(sp)))
+    stream = torch.cuda.ExternalStream(sp.value, device=dev)
+    for _ in range(5):
+        check(lib.trisk_mpas_slow_tendencies_async(ops._h, C.byref(f), 1.0))
+    check(lib.trisk_mpas_synchronize(ops._h))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(calls):
+        check(lib.trisk_mpas_slow_tendencies_async(ops._h, C.byref(f), 1.0))
+    e1.record(stream)
+    check(lib.trisk_mpas_synchronize(ops._h))
+    ms = e0.elapsed_time(e1) / calls
+    nbytes = mpas.algorithmic_bytes(t)
+    peak = measured_peak()[0]
+    gc, tc, sc = case(cpu_level)
+    o = MpasOracle(tc)
+    t0 = time.perf_counter()
+    o.slow_tendencies(*sc)
+    cpu_s = time.perf_counter() - t0
+    return {"workload": f"MPAS-Gassmann slow_tendencies!, create_hexagon_mesh({level}) x {nlev} layers, flat, "
+                        f"ICON-IAP defaults, FP64", "cells": g.nc, "edges": g.ne, "layers": nlev,
+            "ms_per_call": ms, "cell_levels_per_s": g.nc * nlev / (ms * 1e-3), "launches_per_call": 5,
+            "algorithmic_bytes": nbytes, "gbs": nbytes / (ms * 1e-3) / 1e9, "frac": nbytes / (ms * 1e-3) / 1e9 / peak,
+            "cpu_oracle": {"cells": gc.nc, "seconds_per_call": cpu_s, "cell_levels_per_s": gc.nc * nlev / cpu_s,
+                           "cores": 1, "kind": "port (numpy)"},
+            "published_a100_context": "hexagon 7, 30 layers: vn_tendency alone 4.5 ms per time step (two stages)"}
 
 
 class ClockSampler:
@@ -540,6 +603,9 @@ def run_b200(args, rank, world, local_rank):
     icon_leg = None
     if not args.no_icon:
         icon_leg = run_icon_leg(local_rank)
+    mpas_leg = None
+    if not args.no_mpas:
+        mpas_leg = run_mpas_leg(local_rank)
     hexagon5 = None
     if rank == 0 and not args.no_hexagon5:
         hexagon5 = run_hexagon5_leg(local_rank, os.cpu_count() or 1, cpu=world == 1 and not args.no_cpu_baseline)
@@ -556,7 +622,7 @@ def run_b200(args, rank, world, local_rank):
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": config_dict(g, world, args.level), "clocks": clocks.summary(), "e2e": e2e,
                 "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu, "ensemble": ensemble,
-                "closure": closure, "hexagon5": hexagon5, "icon": icon_leg}
+                "closure": closure, "hexagon5": hexagon5, "icon": icon_leg, "mpas": mpas_leg}
         print(json.dumps(line), flush=True)
     del m
 

@@ -44,6 +44,22 @@ class TriskIconTables(C.Structure):
     ]
 
 
+class TriskMpasTables(C.Structure):
+    _fields_ = [("nc", _i64), ("ne", _i64), ("nv", _i64), ("nlev", _i64)] + [
+        (n, _i32) for n in ("cw", "vw", "nt", "vertex_kinetic", "iap_pv", "vertical", "five_band", "reserved")
+    ] + [
+        (n, _p) for n in ("cell_edges", "edge_cells", "edge_vertices", "vertex_edges", "vertex_cells",
+                          "vk_cell_vertices", "kinetic", "inner", "vk_kites", "edge_weight", "rhombus",
+                          "inverse_dual", "edge_coriolis", "curl", "vertex_weight", "vk_weights", "coriolis",
+                          "trisk", "dz_cells", "dzh_cells", "wlow", "dz_edges", "dzh_edges", "trisk_index")
+    ]
+
+
+class TriskMpasFields(C.Structure):
+    _fields_ = [(n, _p) for n in ("vn", "w", "rho", "rhotheta", "theta", "exner", "K", "Kv", "qv", "zetav", "rhov",
+                                  "qe", "rhoe", "Fs", "eta", "tvn", "tw")]
+
+
 class TriskPlex(C.Structure):
     _fields_ = [("nc", _i64), ("ne", _i64), ("nv", _i64), ("ncones", _i64)] + [
         (n, _p)
@@ -103,6 +119,13 @@ def _load():
         "trisk_icon_tendency": (C.c_int, [_p, _p, _p]),
         "trisk_icon_rk4_step": (C.c_int, [_p, _p, _f64, _i64]),
         "trisk_icon_launch_count": (_i64, [_p]),
+        "trisk_mpas_create": (C.c_int, [_p, _i32, _i32, C.POINTER(_p)]),
+        "trisk_mpas_destroy": (None, [_p]),
+        "trisk_mpas_slow_tendencies": (C.c_int, [_p, _p, _f64]),
+        "trisk_mpas_slow_tendencies_async": (C.c_int, [_p, _p, _f64]),
+        "trisk_mpas_stream": (C.c_int, [_p, C.POINTER(_p)]),
+        "trisk_mpas_synchronize": (C.c_int, [_p]),
+        "trisk_mpas_launch_count": (_i64, [_p]),
         "trisk_icosahedral_mesh": (C.c_int, [_i32, _i32, _f64, _p, _p]),
         "trisk_lloyd": (C.c_int, [_p, _i64, _p, _i64, _i32, _i32, C.POINTER(_i32)]),
         "trisk_mesh_destroy": (None, [_p]),
@@ -174,7 +197,8 @@ def _load():
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
-    for which, cls in enumerate((TriskGrid, TriskCoefficients, TriskConfig, TriskPlex, TriskIconTables)):
+    for which, cls in enumerate((TriskGrid, TriskCoefficients, TriskConfig, TriskPlex, TriskIconTables,
+                                  TriskMpasTables, TriskMpasFields)):
         if lib.trisk_struct_size(which) != C.sizeof(cls):
             raise ImportError(f"{cls.__name__}: binding size {C.sizeof(cls)} != library size "
                               f"{lib.trisk_struct_size(which)}")

@@ -73,6 +73,8 @@ int32_t trisk_struct_size(int32_t which) {
     case 2: return (int32_t)sizeof(TriskConfig);
     case 3: return (int32_t)sizeof(TriskPlex);
     case 4: return (int32_t)sizeof(TriskIconTables);
+    case 5: return (int32_t)sizeof(TriskMpasTables);
+    case 6: return (int32_t)sizeof(TriskMpasFields);
     default: return -1;
   }
 }

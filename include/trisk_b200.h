@@ -44,7 +44,7 @@ size_t trisk_last_error(char* buf, size_t len);
 int32_t trisk_abi_version(void);
 /* sizeof of the structs below, so a binding can check its layout */
 int32_t trisk_struct_size(int32_t which); /* 0 TriskGrid, 1 TriskCoefficients, 2 TriskConfig, 3 TriskPlex,
-                                          4 TriskIconTables */
+                                          4 TriskIconTables, 5 TriskMpasTables, 6 TriskMpasFields */
 
 /* ---- mesh generation (set-up, host) ------------------------------------------------
  * Replaces create_hexagon_mesh(n; centroidal)   src/Grids/Hexagonal.jl:11-17
@@ -281,6 +281,75 @@ int trisk_icon_tendency(TriskIconModel* model, const double* y, double* dy);
 /* rk4_step!(y, dt, tendency!, cache, m) (RungeKutta.jl:18-29), nsteps times, in place. */
 int trisk_icon_rk4_step(TriskIconModel* model, double* y, double dt, int64_t nsteps);
 int64_t trisk_icon_launch_count(TriskIconModel* model);
+
+/* ---- 3-D MPAS-Gassmann horizontal operators -----------------------------------------
+ * Replaces slow_tendencies!(m, ys, pressure) of MPASGassmannNonhydrostatic for flat ground
+ * (src/Nonhydrostatic/MPAS/Gassmann/Stepping.jl:22-56): the kernels diagnose,
+ * vertex_kinetic, cell_from_vertex, w_kinetic, eta, edge_density, w_tendency_vi or
+ * w_tendency, vertex_pv, edge_pv (src/Nonhydrostatic/MPAS/Operators.jl:6-133) and
+ * vn_tendency (Gassmann/Tendencies.jl:38-75, oro = 0). The tables are the model's arrays
+ * (MPASGassmannNonhydrostatic.jl:131-150, built at :152-307): 1-based Int64, (entity, k)
+ * ordered as Julia holds them, except the TRiSK tables, which the reference keeps
+ * edge-first: trisk[e + ne*j], trisk_index[e + ne*(j + nt*c)] (Int32, c = 0..2: the edge
+ * e' and the two edges of its PV). Vertical metrics per column: dz_cells[k*nc + i] (Julia's
+ * m.dz), dzh_cells and wlow (nlev + 1 interfaces), dz_edges and dzh_edges (m.metric.dz,
+ * .dzh). vertex_kinetic = 0 leaves the vk_* tables unread (m.vertex_kinetic === nothing). */
+typedef struct {
+  int64_t nc, ne, nv, nlev;
+  int32_t cw, vw, nt;          /* widths: cell tables, vertex tables, TRiSK neighbours */
+  int32_t vertex_kinetic;      /* 1: vk_* tables given */
+  int32_t iap_pv;              /* edge PV: 1 the rhombus PV (m.iap_pv), 0 the vertex mean */
+  int32_t vertical;            /* 0 advective, 1 vector invariant, 2 ICON-IAP mass fluxes */
+  int32_t five_band;           /* 1: the five-band solver (K_w left out of the w tendency) */
+  int32_t reserved;
+  const int64_t* cell_edges;       /* nc x cw */
+  const int64_t* edge_cells;       /* ne x 2 */
+  const int64_t* edge_vertices;    /* ne x 2 */
+  const int64_t* vertex_edges;     /* nv x vw */
+  const int64_t* vertex_cells;     /* nv x vw */
+  const int64_t* vk_cell_vertices; /* nc x cw */
+  const double* kinetic;           /* nc x cw: alpha l_e d_{e,i} / 2A_i */
+  const double* inner;             /* nc x cw: l_e d_{e,i} / A_i */
+  const double* vk_kites;          /* nc x cw */
+  const double* edge_weight;       /* ne x 2: d_{e,i} / d_e */
+  const double* rhombus;           /* ne x 2 */
+  const double* inverse_dual;      /* ne: 1 / (a d_e) */
+  const double* edge_coriolis;     /* ne */
+  const double* curl;              /* nv x vw: t_{e,v} d_e / (a A_v) */
+  const double* vertex_weight;     /* nv x vw: K_{i,v} / A_v */
+  const double* vk_weights;        /* nv x vw */
+  const double* coriolis;          /* nv */
+  const double* trisk;             /* edge-first ne x nt */
+  const double* dz_cells;          /* nlev x nc (level slabs) */
+  const double* dzh_cells;         /* (nlev + 1) x nc */
+  const double* wlow;              /* (nlev + 1) x nc */
+  const double* dz_edges;          /* nlev x ne */
+  const double* dzh_edges;         /* (nlev + 1) x ne */
+  const int32_t* trisk_index;      /* edge-first ne x nt x 3 */
+} TriskMpasTables;
+/* The stage state ys and the work arrays slow_tendencies! fills, all DEVICE pointers in the
+ * reference's layout (level slabs, horizontal index fastest): vn nlev x ne, w (nlev + 1) x nc,
+ * rho and rhotheta nlev x nc; theta, exner, K nlev x nc; Kv (may be NULL without the vertex
+ * kinetic energy), qv, zetav, rhov nlev x nv; qe, rhoe, Fs nlev x ne; eta (nlev + 1) x ne
+ * (left untouched by the advective form, as there); tvn nlev x ne; tw (nlev + 1) x nc. */
+typedef struct {
+  const double *vn, *w, *rho, *rhotheta;
+  double *theta, *exner, *K, *Kv, *qv, *zetav, *rhov, *qe, *rhoe, *Fs, *eta, *tvn, *tw;
+} TriskMpasFields;
+typedef struct TriskMpas TriskMpas;
+/* Uploads the tables once. levels_per_thread: levels each thread walks with its neighbour
+ * tables in registers (0 = 8; 1, 2, 4, 8 or 16). Tables wider than 10 edges per cell, 4 per
+ * vertex or 18 TRiSK neighbours return TRISK_ERR_UNSUPPORTED. */
+int trisk_mpas_create(const TriskMpasTables* tables, int32_t device, int32_t levels_per_thread, TriskMpas** out);
+void trisk_mpas_destroy(TriskMpas* ops);
+/* slow_tendencies!(m, ys, pressure) for flat ground; returns when the results are complete.
+ * Ordered after the work already queued on the legacy default stream. */
+int trisk_mpas_slow_tendencies(TriskMpas* ops, const TriskMpasFields* fields, double pressure);
+/* The same without waiting (trisk_mpas_stream gives the stream it runs on). */
+int trisk_mpas_slow_tendencies_async(TriskMpas* ops, const TriskMpasFields* fields, double pressure);
+int trisk_mpas_stream(TriskMpas* ops, void** stream);
+int trisk_mpas_synchronize(TriskMpas* ops);
+int64_t trisk_mpas_launch_count(TriskMpas* ops);
 
 /* ---- batched ensembles ------------------------------------------------------------
  * No counterpart in the reference, which runs one model per process (examples/
