@@ -202,20 +202,22 @@ def run_icon_leg(local_rank, level=8, steps=100):
                     "levels 7/8/9); this mesh is the icosahedral bisection of the same size"}
 
 
-def run_mpas_leg(local_rank, level=7, nlev=30, calls=50, cpu_level=5):
+def run_mpas_leg(local_rank, level=7, nlev=30, calls=50, cpu_level=5, hilbert=True, lpt=0):
     """The horizontal operators of the 3-D MPAS-Gassmann dycore (slow_tendencies!, flat ground,
     the reference's ICON-IAP defaults) on create_hexagon_mesh(level) x nlev equidistant layers
-    up to 30 km — the grid of the reference's baroclinic wave — on a perturbed stratified
-    state, device-resident: `calls` calls timed with CUDA events on the library's stream,
+    up to 30 km — the grid of the reference's baroclinic wave, Hilbert-ordered as its
+    example orders it (hilbert_order) — on a perturbed stratified state, device-resident: `calls` calls timed with CUDA events on the library's stream,
     against the algorithmic bytes of the five phases. The CPU oracle (numpy, one thread) is
     timed on create_hexagon_mesh(cpu_level) with the same layers."""
     import torch
     import dmplex_b200 as d
     from dmplex_b200 import mpas
+    from dmplex_b200.gridfiles import hilbert_order
     from oracle.mpas_oracle import MpasOracle
 
     def case(n):
-        g = d.TRiSKGrid(d.create_hexagon_mesh(n))
+        mesh = d.create_hexagon_mesh(n)
+        g = d.TRiSKGrid(hilbert_order(mesh) if hilbert else mesh)
         v = mpas.vertical_grid(nlev, 30000.0)
         t = mpas.mpas_tables(g, v)
         rng = np.random.default_rng(11)
@@ -228,7 +230,7 @@ def run_mpas_leg(local_rank, level=7, nlev=30, calls=50, cpu_level=5):
         return g, t, (vn, w, rho, rho * theta)
 
     g, t, state = case(level)
-    ops = mpas.MPASOperators(t, device=local_rank)
+    ops = mpas.MPASOperators(t, device=local_rank, levels_per_thread=lpt)
     dev = f"cuda:{local_rank}"
     ys = [torch.from_numpy(np.ascontiguousarray(x)).to(dev) for x in state]
     out = ops.work(torch.device(dev))
@@ -254,8 +256,9 @@ def run_mpas_leg(local_rank, level=7, nlev=30, calls=50, cpu_level=5):
     t0 = time.perf_counter()
     o.slow_tendencies(*sc)
     cpu_s = time.perf_counter() - t0
-    return {"workload": f"MPAS-Gassmann slow_tendencies!, create_hexagon_mesh({level}) x {nlev} layers, flat, "
-                        f"ICON-IAP defaults, FP64", "cells": g.nc, "edges": g.ne, "layers": nlev,
+    return {"workload": f"MPAS-Gassmann slow_tendencies!, create_hexagon_mesh({level})"
+                        f"{' Hilbert-ordered' if hilbert else ''} x {nlev} layers, flat, ICON-IAP defaults, FP64",
+            "levels_per_thread": ops.levels_per_thread, "cells": g.nc, "edges": g.ne, "layers": nlev,
             "ms_per_call": ms, "cell_levels_per_s": g.nc * nlev / (ms * 1e-3), "launches_per_call": 5,
             "algorithmic_bytes": nbytes, "gbs": nbytes / (ms * 1e-3) / 1e9, "frac": nbytes / (ms * 1e-3) / 1e9 / peak,
             "cpu_oracle": {"cells": gc.nc, "seconds_per_call": cpu_s, "cell_levels_per_s": gc.nc * nlev / cpu_s,

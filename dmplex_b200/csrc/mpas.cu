@@ -1,7 +1,7 @@
 // The horizontal operators of dmplex.jl's 3-D MPAS-Gassmann dycore: slow_tendencies! for flat
 // ground (src/Nonhydrostatic/MPAS/Gassmann/Stepping.jl:22-56) — the kernels of
 // src/Nonhydrostatic/MPAS/Operators.jl and vn_tendency_kernel! (Tendencies.jl:38-75) — in five
-// fused launches over (entity, level):
+// fused launches over (entity, level), the last two side by side on two streams:
 //
 //   1 vertices  vertex_pv_kernel! + vertex_kinetic_kernel!         (zeta_v, rho_v, q_v, K_v)
 //   2 cells     diagnose_kernel! + cell_from_vertex_kernel! + w_kinetic_kernel!  (theta, pi, K)
@@ -19,6 +19,7 @@
 // the build does not contract to FMA, so results equal the CPU restatement bit for bit (the
 // Exner pressure uses CUDA's pow).
 #include <algorithm>
+#include <utility>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -79,12 +80,13 @@ struct MpasFieldsDev {
 __device__ __forceinline__ size_t at(int k, int n, int i) { return (size_t)k * n + i; }
 
 // 1: vertex_pv_kernel! (Operators.jl:88-102) and vertex_kinetic_kernel! (:18-25)
+template <bool VK>
 __global__ void __launch_bounds__(MB) k_mpas_vertex(MpasTables T, MpasFieldsDev F, int lpt) {
   const int v = blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= T.nv) return;
   const int k0 = blockIdx.y * lpt, k1 = min(k0 + lpt, T.nlev);
   int ve[MVW], vc[MVW];
-  double cu[MVW], wt[MVW], kw[MVW];
+  double cu[MVW], wt[MVW], kw[VK ? MVW : 1];
 #pragma unroll
   for (int j = 0; j < MVW; ++j)
     if (j < T.vw) {
@@ -92,7 +94,7 @@ __global__ void __launch_bounds__(MB) k_mpas_vertex(MpasTables T, MpasFieldsDev 
       vc[j] = T.vertex_cells[j * T.ldv + v];
       cu[j] = T.curl[j * T.ldv + v];
       wt[j] = T.vertex_weight[j * T.ldv + v];
-      kw[j] = T.vk ? T.vk_weights[j * T.ldv + v] : 0.0;
+      if constexpr (VK) kw[j] = T.vk_weights[j * T.ldv + v];
     }
   const double f = T.coriolis[v];
   for (int k = k0; k < k1; ++k) {
@@ -108,7 +110,7 @@ __global__ void __launch_bounds__(MB) k_mpas_vertex(MpasTables T, MpasFieldsDev 
     F.zv[at(k, T.nv, v)] = z;
     F.rv[at(k, T.nv, v)] = h;
     F.qv[at(k, T.nv, v)] = (z + f) / h;
-    if (T.vk) {
+    if constexpr (VK) {
       double s = 0.0;
 #pragma unroll
       for (int j = 0; j < MVW; ++j)
@@ -122,19 +124,22 @@ __global__ void __launch_bounds__(MB) k_mpas_vertex(MpasTables T, MpasFieldsDev 
 }
 
 // 2: diagnose_kernel! (:6-15), cell_from_vertex_kernel! (:28-35), w_kinetic_kernel! (:38-41)
+template <bool VK>
 __global__ void __launch_bounds__(MB) k_mpas_cell(MpasTables T, MpasFieldsDev F, int lpt) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= T.nc) return;
   const int k0 = blockIdx.y * lpt, k1 = min(k0 + lpt, T.nlev);
-  int ce[MCW], cv[MCW];
-  double kin[MCW], kt[MCW];
+  int ce[MCW], cv[VK ? MCW : 1];
+  double kin[MCW], kt[VK ? MCW : 1];
 #pragma unroll
   for (int j = 0; j < MCW; ++j)
     if (j < T.cw) {
       ce[j] = T.cell_edges[j * T.ldc + i];
       kin[j] = T.kinetic[j * T.ldc + i];
-      cv[j] = T.vk ? T.kcv[j * T.ldc + i] : 0;
-      kt[j] = T.vk ? T.kites[j * T.ldc + i] : 0.0;
+      if constexpr (VK) {
+        cv[j] = T.kcv[j * T.ldc + i];
+        kt[j] = T.kites[j * T.ldc + i];
+      }
     }
   for (int k = k0; k < k1; ++k) {
     const double* vn = F.vn + (size_t)k * T.ne;
@@ -150,7 +155,7 @@ __global__ void __launch_bounds__(MB) k_mpas_cell(MpasTables T, MpasFieldsDev F,
     const double r = F.rho[o], rt = F.rt[o];
     F.theta[o] = rt / r;
     F.exner[o] = pow(RD * rt / P0, RD / CVD);
-    if (T.vk) {
+    if constexpr (VK) {
       const double* Kv = F.Kv + (size_t)k * T.nv;
       double sv = 0.0;
 #pragma unroll
@@ -212,10 +217,7 @@ __global__ void __launch_bounds__(MB) k_mpas_edge(MpasTables T, MpasFieldsDev F,
 // 4: w_tendency_vi_kernel! (:69-86) with the vector-invariant vertical advection, else
 // w_tendency_kernel! (:118-133); rows 0..nlev (interfaces), zero at ground and top
 template <bool VI>
-__global__ void __launch_bounds__(MB) k_mpas_wtend(MpasTables T, MpasFieldsDev F, int lpt) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= T.nc) return;
-  const int k0 = blockIdx.y * lpt, k1 = min(k0 + lpt, T.nlev + 1);
+__device__ __forceinline__ void wtend_rows(const MpasTables& T, const MpasFieldsDev& F, int i, int k0, int k1) {
   int ce[MCW];
   double cwt[MCW];
   int el[VI ? 1 : MCW], er[VI ? 1 : MCW];
@@ -286,10 +288,8 @@ __device__ __forceinline__ double edge_w(const MpasTables& T, const MpasFieldsDe
 // 5: vn_tendency_kernel! (Tendencies.jl:38-75), flat ground (oro = 0). The TRiSK sums of
 // LPT levels are accumulated neighbour by neighbour so that each table entry is read once.
 template <int LPT, bool VI>
-__global__ void __launch_bounds__(MB) k_mpas_vn(MpasTables T, MpasFieldsDev F, double pressure) {
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= T.ne) return;
-  const int k0 = blockIdx.y * LPT, k1 = min(k0 + LPT, T.nlev);
+__device__ __forceinline__ void vn_rows(const MpasTables& T, const MpasFieldsDev& F, int e, int k0, double pressure) {
+  const int k1 = min(k0 + LPT, T.nlev);
   double s[LPT];
 #pragma unroll
   for (int q = 0; q < LPT; ++q) s[q] = 0.0;
@@ -303,7 +303,9 @@ __global__ void __launch_bounds__(MB) k_mpas_vn(MpasTables T, MpasFieldsDev F, d
       const int k = k0 + q;
       if (k < k1) {
         const size_t base = (size_t)k * T.ne;
-        s[q] += wt * F.Fs[base + a] * (F.qe[base + b] + F.qe[base + c]);
+        const double qb = F.qe[base + b];
+        const double qc = c == b ? qb : F.qe[base + c];  // the rhombus PV of one edge, twice
+        s[q] += wt * F.Fs[base + a] * (qb + qc);
       }
     }
   }
@@ -343,13 +345,27 @@ __global__ void __launch_bounds__(MB) k_mpas_vn(MpasTables T, MpasFieldsDev F, d
   }
 }
 
+template <bool VI>
+__global__ void __launch_bounds__(MB) k_mpas_wtend(MpasTables T, MpasFieldsDev F, int lpt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k0 = blockIdx.y * lpt;
+  if (i < T.nc) wtend_rows<VI>(T, F, i, k0, min(k0 + lpt, T.nlev + 1));
+}
+
+template <int LPT, bool VI>
+__global__ void __launch_bounds__(MB) k_mpas_vn(MpasTables T, MpasFieldsDev F, double pressure) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < T.ne) vn_rows<LPT, VI>(T, F, e, blockIdx.y * LPT, pressure);
+}
+
 }  // namespace
 
 struct TriskMpas {
   int device = 0;
   int lpt = 8;
   cudaStream_t stream = nullptr;
-  cudaEvent_t caller_ev = nullptr;
+  cudaStream_t side = nullptr;  // the w tendency beside the vn tendency
+  cudaEvent_t caller_ev = nullptr, fork_ev = nullptr, join_ev = nullptr;
   MpasTables T{};
   std::vector<void*> allocations;
   int64_t launches = 0;
@@ -358,11 +374,13 @@ struct TriskMpas {
     int prev = -1;
     cudaGetDevice(&prev);
     cudaSetDevice(device);
-    if (caller_ev) cudaEventDestroy(caller_ev);
-    if (stream) {
-      cudaStreamSynchronize(stream);
-      cudaStreamDestroy(stream);
-    }
+    for (cudaStream_t s : {stream, side})
+      if (s) {
+        cudaStreamSynchronize(s);
+        cudaStreamDestroy(s);
+      }
+    for (cudaEvent_t e : {caller_ev, fork_ev, join_ev})
+      if (e) cudaEventDestroy(e);
     for (void* p : allocations) cudaFree(p);
     if (prev >= 0) cudaSetDevice(prev);
   }
@@ -417,10 +435,11 @@ TriskMpas* checked_mpas(TriskMpas* m) {
 }
 
 template <typename... KArgs, typename... Args>
-void mlaunch(TriskMpas& m, void (*kernel)(KArgs...), int64_t n, int64_t rows, int lpt, Args&&... args) {
+void mlaunch(TriskMpas& m, cudaStream_t st, void (*kernel)(KArgs...), int64_t n, int64_t rows, int lpt,
+             Args&&... args) {
   if (n <= 0 || rows <= 0) return;
   dim3 grid((unsigned)cdiv(n, MB), (unsigned)cdiv(rows, lpt));
-  kernel<<<grid, MB, 0, m.stream>>>(std::forward<Args>(args)...);
+  kernel<<<grid, MB, 0, st>>>(std::forward<Args>(args)...);
   CUDA_CHECK(cudaGetLastError());
   m.launches++;
 }
@@ -428,21 +447,31 @@ void mlaunch(TriskMpas& m, void (*kernel)(KArgs...), int64_t n, int64_t rows, in
 template <int LPT>
 void launch_vn(TriskMpas& m, const MpasFieldsDev& F, double pressure) {
   if (m.T.vertical > 0)
-    mlaunch(m, k_mpas_vn<LPT, true>, m.T.ne, m.T.nlev, LPT, m.T, F, pressure);
+    mlaunch(m, m.stream, k_mpas_vn<LPT, true>, m.T.ne, m.T.nlev, LPT, m.T, F, pressure);
   else
-    mlaunch(m, k_mpas_vn<LPT, false>, m.T.ne, m.T.nlev, LPT, m.T, F, pressure);
+    mlaunch(m, m.stream, k_mpas_vn<LPT, false>, m.T.ne, m.T.nlev, LPT, m.T, F, pressure);
 }
 
 void slow_tendencies(TriskMpas& m, const MpasFieldsDev& F, double pressure) {
   const MpasTables& T = m.T;
   const int lpt = m.lpt;
-  mlaunch(m, k_mpas_vertex, T.nv, T.nlev, lpt, T, F, lpt);
-  mlaunch(m, k_mpas_cell, T.nc, T.nlev, lpt, T, F, lpt);
-  mlaunch(m, k_mpas_edge, T.ne, T.nlev + 1, lpt, T, F, lpt);
+  if (T.vk) {
+    mlaunch(m, m.stream, k_mpas_vertex<true>, T.nv, T.nlev, lpt, T, F, lpt);
+    mlaunch(m, m.stream, k_mpas_cell<true>, T.nc, T.nlev, lpt, T, F, lpt);
+  } else {
+    mlaunch(m, m.stream, k_mpas_vertex<false>, T.nv, T.nlev, lpt, T, F, lpt);
+    mlaunch(m, m.stream, k_mpas_cell<false>, T.nc, T.nlev, lpt, T, F, lpt);
+  }
+  mlaunch(m, m.stream, k_mpas_edge, T.ne, T.nlev + 1, lpt, T, F, lpt);
+  // phases 4 and 5 read only what 1-3 wrote: the w tendency runs on a second stream beside
+  // the vn tendency, joined before the call ends
+  CUDA_CHECK(cudaEventRecord(m.fork_ev, m.stream));
+  CUDA_CHECK(cudaStreamWaitEvent(m.side, m.fork_ev, 0));
   if (T.vertical > 0)
-    mlaunch(m, k_mpas_wtend<true>, T.nc, T.nlev + 1, lpt, T, F, lpt);
+    mlaunch(m, m.side, k_mpas_wtend<true>, T.nc, T.nlev + 1, lpt, T, F, lpt);
   else
-    mlaunch(m, k_mpas_wtend<false>, T.nc, T.nlev + 1, lpt, T, F, lpt);
+    mlaunch(m, m.side, k_mpas_wtend<false>, T.nc, T.nlev + 1, lpt, T, F, lpt);
+  CUDA_CHECK(cudaEventRecord(m.join_ev, m.side));
   switch (lpt) {
     case 1: launch_vn<1>(m, F, pressure); break;
     case 2: launch_vn<2>(m, F, pressure); break;
@@ -450,6 +479,7 @@ void slow_tendencies(TriskMpas& m, const MpasFieldsDev& F, double pressure) {
     case 16: launch_vn<16>(m, F, pressure); break;
     default: launch_vn<8>(m, F, pressure); break;
   }
+  CUDA_CHECK(cudaStreamWaitEvent(m.stream, m.join_ev, 0));
 }
 
 MpasFieldsDev device_fields(const TriskMpas& m, const TriskMpasFields* f) {
@@ -573,7 +603,10 @@ int trisk_mpas_create(const TriskMpasTables* t, int32_t device, int32_t levels_p
   T.dzh_e = m->upload(t->dzh_edges, (size_t)(nl + 1) * ne, "dzh_edges");
   T.Kh = T.five_band ? m->alloc<double>((size_t)nl * nc) : nullptr;
   CUDA_CHECK(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
+  CUDA_CHECK(cudaStreamCreateWithFlags(&m->side, cudaStreamNonBlocking));
   CUDA_CHECK(cudaEventCreateWithFlags(&m->caller_ev, cudaEventDisableTiming));
+  CUDA_CHECK(cudaEventCreateWithFlags(&m->fork_ev, cudaEventDisableTiming));
+  CUDA_CHECK(cudaEventCreateWithFlags(&m->join_ev, cudaEventDisableTiming));
   CUDA_CHECK(cudaDeviceSynchronize());
   *out = m.release();
   TRISK_API_END

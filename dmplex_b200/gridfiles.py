@@ -12,6 +12,7 @@ rules a TRiSKGrid built on them uses:
     cell_centers(dm; method)              src/Grids/CellCenters.jl:25-46
     voronoi_generators(dm; iterations)    CellCenters.jl:49-81
     check_plex(dm; closed)                src/Topology/Plex.jl:329-359
+    hilbert_order(dm)                     src/Topology/Ordering.jl:44-82
 
 A reader returns a PolygonMesh (the Plex of plex_from_polygons, built by the library) whose
 ``generators`` are ``cell_centers(mesh)``: what ``TRiSKGrid(read_grid(f))`` uses in the
@@ -374,3 +375,23 @@ def read_grid(filename: str, dual: bool = False, centers: str | None = "auto") -
     if kind == "mpas":
         return read_mpas_grid(filename, dual, centers)
     raise ValueError(f"{filename} is neither an ICON nor an MPAS grid file")
+
+
+def hilbert_order(mesh: HexMesh) -> PolygonMesh:
+    """The same mesh renumbered for locality (Ordering.jl:44-82): cells along the Hilbert
+    curve of their centroids (hilbert_permutation), vertices in order of first appearance in
+    the new cell order, edges by first appearance as plex_from_polygons numbers them. Cell c
+    of the result is cell perm[c] of ``mesh``; its centers are the mesh's centers permuted
+    the same way."""
+    perm = mesh.hilbert_permutation() - 1
+    rings = cell_vertex_table(mesh)
+    polys = [rings[c] - 1 for c in perm]
+    flat = np.concatenate(polys)
+    ids, at = np.unique(flat, return_index=True)
+    if len(ids) != mesh.nv:
+        raise ValueError("vertices without cells")
+    first = np.empty(mesh.nv, dtype=np.int64)
+    first[flat[np.sort(at)]] = np.arange(mesh.nv)    # new number = rank of first appearance
+    x = np.empty_like(mesh.plex.coordinates)
+    x[first] = mesh.plex.coordinates
+    return PolygonMesh([first[p] + 1 for p in polys], x, centers=mesh.generators[perm])

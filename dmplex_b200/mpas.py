@@ -13,8 +13,8 @@ Fields live on the device in the reference's layout: a Julia (n, nlev) array is 
 (nlev, n) C-ordered tensor (level slabs, the horizontal index fastest); ``vn`` (nlev, ne),
 ``w`` (nlev + 1, nc), ``rho``, ``rhotheta`` (nlev, nc). ``MPASOperators.slow_tendencies``
 fills the work arrays slow_tendencies! fills (theta, exner, K, qv, zetav, rhov, Kv, qe,
-rhoe, Fs, eta) and the tendencies tvn and tw, in five fused launches of the library's
-``trisk_mpas_*`` kernels.
+rhoe, Fs, eta) and the tendencies tvn and tw, in five launches of the library's
+``trisk_mpas_*`` kernels (the w and vn tendencies side by side on two streams).
 """
 from __future__ import annotations
 
@@ -258,6 +258,7 @@ class MPASOperators:
         self._h = h
         self.nc, self.ne, self.nv, self.nlev = t["nc"], t["ne"], t["nv"], t["nlev"]
         self.vertex_kinetic = bool(s.vertex_kinetic)
+        self.levels_per_thread = int(levels_per_thread) or 8
 
     def __del__(self):
         if getattr(self, "_h", None):

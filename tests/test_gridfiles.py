@@ -260,3 +260,18 @@ def test_gpu_model_on_a_read_grid(require_gpu, tmp_path, kind):
     ref = o.rk4_step(y.copy(), 300.0, 3)
     d.rk4_step(y, 300.0, d.tendency, d.RK4Cache(y), m, nsteps=3)
     assert np.array_equal(y, ref)
+
+
+def test_hilbert_order():
+    """hilbert_order(dm) (Ordering.jl:44-82): cells along the Hilbert curve, vertices and
+    edges by first appearance; the same mesh otherwise."""
+    m = d.create_hexagon_mesh(3)
+    h = gf.hilbert_order(m)
+    assert gf.check_plex(h)
+    perm = m.hilbert_permutation() - 1
+    g0, g1 = d.TRiSKGrid(m), d.TRiSKGrid(h)
+    assert np.allclose(g1.cell_areas, g0.cell_areas[perm], rtol=1e-13, atol=0)
+    assert np.array_equal(h.generators, m.generators[perm])
+    flat = np.concatenate(gf.cell_vertex_table(h)) - 1
+    assert np.array_equal(np.unique(flat, return_index=True)[1], np.sort(np.unique(flat, return_index=True)[1]))
+    assert h.orthogonality_defect() < 1e-12
