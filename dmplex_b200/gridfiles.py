@@ -153,12 +153,17 @@ def _edge_vertices(mesh: HexMesh) -> np.ndarray:
     return np.stack([p.cones[off], p.cones[off + 1]], axis=1) - p.nc - p.ne - 1
 
 
-def cell_vertex_table(mesh: HexMesh) -> list:
-    """get_cell_vertices for every cell (Plex.jl:226-230), 1-based vertex indices: corner i
-    is where cone edge i starts."""
+def cell_vertex_csr(mesh: HexMesh):
+    """get_cell_vertices of all cells (Plex.jl:226-230) as (sizes, flat 1-based vertex
+    list): corner i of a cell is where its cone edge i starts."""
     cell, edge, orient, pos, sizes = _cone_table(mesh)
     ev = _edge_vertices(mesh)
-    start = np.where(orient == 0, ev[edge, 0], ev[edge, 1]) + 1
+    return sizes, np.where(orient == 0, ev[edge, 0], ev[edge, 1]) + 1
+
+
+def cell_vertex_table(mesh: HexMesh) -> list:
+    """get_cell_vertices for every cell, one array per cell (see cell_vertex_csr)."""
+    sizes, start = cell_vertex_csr(mesh)
     return np.split(start, np.cumsum(sizes)[:-1])
 
 
@@ -384,9 +389,12 @@ def hilbert_order(mesh: HexMesh) -> PolygonMesh:
     of the result is cell perm[c] of ``mesh``; its centers are the mesh's centers permuted
     the same way."""
     perm = mesh.hilbert_permutation() - 1
-    rings = cell_vertex_table(mesh)
-    polys = [rings[c] - 1 for c in perm]
-    flat = np.concatenate(polys)
+    sizes, verts = cell_vertex_csr(mesh)
+    starts = np.cumsum(sizes) - sizes
+    new_sizes = sizes[perm]
+    # the vertex list of the permuted cells: cell perm[c]'s run, for c in order
+    idx = np.repeat(starts[perm] - (np.cumsum(new_sizes) - new_sizes), new_sizes) + np.arange(new_sizes.sum())
+    flat = verts[idx] - 1
     ids, at = np.unique(flat, return_index=True)
     if len(ids) != mesh.nv:
         raise ValueError("vertices without cells")
@@ -394,4 +402,4 @@ def hilbert_order(mesh: HexMesh) -> PolygonMesh:
     first[flat[np.sort(at)]] = np.arange(mesh.nv)    # new number = rank of first appearance
     x = np.empty_like(mesh.plex.coordinates)
     x[first] = mesh.plex.coordinates
-    return PolygonMesh([first[p] + 1 for p in polys], x, centers=mesh.generators[perm])
+    return PolygonMesh((new_sizes, first[flat] + 1), x, centers=mesh.generators[perm])

@@ -111,17 +111,22 @@ def create_triangle_mesh(subdivisions: int, centroidal: bool = False,
 class PolygonMesh(HexMesh):
     """plex_from_polygons(polygons, coordinates) (src/Topology/Plex.jl:49-97): a mesh from
     arbitrary polygons, as the grid-file readers build it. ``polygons``: a list of 1-based
-    vertex sequences, or an (nc, k) array; ``centers`` (nc, 3): the cell centers of its
+    vertex sequences, an (nc, k) array, or a pair (sizes, flat vertex list); ``centers`` (nc, 3): the cell centers of its
     TRiSKGrid (default: the normalized vertex means; see gridfiles.cell_centers)."""
 
     def __init__(self, polygons, coordinates: np.ndarray, centers: np.ndarray | None = None):
-        if isinstance(polygons, np.ndarray) and polygons.ndim == 2:
+        if isinstance(polygons, tuple) and len(polygons) == 2:      # (sizes, flat): CSR
+            sizes = np.asarray(polygons[0], dtype=np.int64)
+            flat = np.ascontiguousarray(polygons[1], dtype=np.int64)
+        elif isinstance(polygons, np.ndarray) and polygons.ndim == 2:
             sizes = np.full(len(polygons), polygons.shape[1], dtype=np.int64)
             flat = np.ascontiguousarray(polygons, dtype=np.int64).ravel()
         else:
             sizes = np.array([len(p) for p in polygons], dtype=np.int64)
             flat = np.ascontiguousarray(np.concatenate([np.asarray(p, dtype=np.int64) for p in polygons])
                                         if len(polygons) else np.zeros(0, np.int64))
+        if sizes.sum() != len(flat):
+            raise ValueError("polygon sizes do not match the vertex list")
         offsets = np.ascontiguousarray(np.concatenate([[1], 1 + np.cumsum(sizes)]), dtype=np.int64)
         x = np.ascontiguousarray(coordinates, dtype=np.float64)
         if x.ndim != 2 or x.shape[1] != 3:

@@ -206,3 +206,15 @@ def test_gpu_argument_errors(require_gpu):
     bad["trisk_index"][0, 0, 0] = g.ne + 5
     with pytest.raises(d.TriskError):
         mpas.MPASOperators(bad)
+
+
+def test_operators_fail_loudly_without_a_gpu():
+    """On a machine without a CUDA device the library refuses to create the operators (no
+    CPU fallback)."""
+    from conftest import gpu_available
+    if gpu_available():
+        pytest.skip("a GPU is present")
+    g = hex_grid(1)
+    t = mpas.mpas_tables(g, mpas.vertical_grid(4, 1000.0))
+    with pytest.raises(d.TriskError, match="CUDA"):
+        mpas.MPASOperators(t)
