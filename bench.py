@@ -173,6 +173,17 @@ def run_hexagon5_leg(local_rank, threads, cpu=True):
     return out
 
 
+def optional_leg(fn, *args, **kwargs):
+    """Run an auxiliary leg (no collectives inside); a failure is reported in the JSON line
+    as {"error": ...} and on stderr instead of taking the headline measurement with it."""
+    import traceback
+    try:
+        return fn(*args, **kwargs)
+    except Exception as exc:  # noqa: BLE001 - reported, not hidden
+        traceback.print_exc()
+        return {"error": f"{type(exc).__name__}: {exc}"}
+
+
 def run_icon_leg(local_rank, level=8, steps=100, hilbert=True):
     """ICON triangle shallow water (the reference's ICONShallowWater) on create_triangle_mesh
     (level), plain bisection — 20 * 4^level triangles, the size of the ICON grid R02B(level - 1): Williamson
@@ -598,23 +609,26 @@ def run_b200(args, rank, world, local_rank):
 
     ensemble = None
     if not args.no_ensemble:
-        ensemble = run_ensemble_leg(local_rank, seed=1000 * (rank + 1), days=args.ensemble_days)
-        f32 = run_ensemble_leg(local_rank, seed=1000 * (rank + 1), days=args.ensemble_days, state_bits=32)
-        ensemble["fp32_state"] = {k: f32[k] for k in ("value", "gpu_seconds_per_simulated_day", "gbs", "frac")}
-        if world > 1:
+        ensemble = optional_leg(run_ensemble_leg, local_rank, seed=1000 * (rank + 1), days=args.ensemble_days)
+        f32 = optional_leg(run_ensemble_leg, local_rank, seed=1000 * (rank + 1), days=args.ensemble_days,
+                           state_bits=32)
+        if "error" not in ensemble and "error" not in f32:
+            ensemble["fp32_state"] = {k: f32[k] for k in ("value", "gpu_seconds_per_simulated_day", "gbs", "frac")}
+        if world > 1 and "error" not in ensemble:
             ensemble["value_all_ranks"] = world * ensemble["value"]
     closure = None
     if not args.no_closure:
-        closure = run_closure_leg(local_rank)
+        closure = optional_leg(run_closure_leg, local_rank)
     icon_leg = None
     if not args.no_icon:
-        icon_leg = run_icon_leg(local_rank)
+        icon_leg = optional_leg(run_icon_leg, local_rank)
     mpas_leg = None
     if not args.no_mpas:
-        mpas_leg = run_mpas_leg(local_rank)
+        mpas_leg = optional_leg(run_mpas_leg, local_rank)
     hexagon5 = None
     if rank == 0 and not args.no_hexagon5:
-        hexagon5 = run_hexagon5_leg(local_rank, os.cpu_count() or 1, cpu=world == 1 and not args.no_cpu_baseline)
+        hexagon5 = optional_leg(run_hexagon5_leg, local_rank, os.cpu_count() or 1,
+                                cpu=world == 1 and not args.no_cpu_baseline)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
