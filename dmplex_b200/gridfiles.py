@@ -60,6 +60,8 @@ class _Dataset:
         return name in self.ds.variables
 
     def attribute(self, name: str):
+        # the global attributes as scipy keeps them (getattr would also find the file's
+        # methods and fields for names such as "mode" or "filename")
         value = self.ds._attributes.get(name)
         if isinstance(value, bytes):
             value = value.decode("utf-8", "replace")

@@ -1,6 +1,4 @@
 """Host-side helpers of bench.py and the byte model of the MPAS-Gassmann roofline, on CPU."""
-import numpy as np
-
 import dmplex_b200 as d
 from dmplex_b200 import mpas
 
