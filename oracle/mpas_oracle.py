@@ -20,13 +20,18 @@ order (numpy does not contract to FMA):
     Rd, Cpd, Cvd, P0                   src/Nonhydrostatic/Common/Constants.jl:12-14
 
 Fields are numpy arrays (nlev, n) / (nlev + 1, n): the memory of the reference's (n, nlev)
-column-major arrays. Tables are those of dmplex_b200.mpas.mpas_tables ((entity, k), 1-based;
+column-major arrays. ``MpasOracleC`` runs the same restatement in C with OpenMP
+(oracle/mpas_oracle.c), bit for bit the same, for the timed CPU baseline. Tables are those of dmplex_b200.mpas.mpas_tables ((entity, k), 1-based;
 ``trisk`` and ``trisk_index`` edge-first as in the reference). Pinned by the reference's
 own operator test (test/extruded.jl:54-106) in tests/test_mpas.py.
 """
 from __future__ import annotations
 
+import math
+
 import numpy as np
+
+_POW = np.frompyfunc(math.pow, 2, 1)
 
 RD = 287.0
 CPD = 1004.0
@@ -56,7 +61,9 @@ class MpasOracle:
             v = vn[:, self.ce[:, j]]
             K = K + t["kinetic"][:, j] * (v * v)
         theta = rhotheta / rho
-        exner = np.power(RD * rhotheta / P0, RD / CVD)
+        # the C library's pow, element by element (numpy's own vectorized pow differs from it
+        # in the last bit for a few percent of the values)
+        exner = _POW(RD * rhotheta / P0, RD / CVD).astype(np.float64)
         return theta, exner, K
 
     def vertex_kinetic(self, vn):
@@ -220,4 +227,79 @@ class MpasOracle:
             tw = self.w_tendency(w, vn)
         tvn = self.vn_tendency(vn, Fs, w, rho, theta, exner, K, qe, eta, pressure)
         out.update(K=K, qv=qv, zetav=zv, rhov=rv, qe=qe, rhoe=rhoe, Fs=Fs, eta=eta, tw=tw, tvn=tvn)
+        return out
+
+
+_TABLE_INDEX = ("cell_edges", "edge_cells", "edge_vertices", "vertex_edges", "vertex_cells", "vk_cell_vertices")
+_TABLE_REAL = ("kinetic", "inner", "vk_kites", "edge_weight", "rhombus", "inverse_dual", "edge_coriolis", "curl",
+               "vertex_weight", "vk_weights", "coriolis", "trisk", "dz_cells", "dzh_cells", "wlow", "dz_edges",
+               "dzh_edges")
+_FIELDS_OUT = ("theta", "exner", "K", "Kv", "qv", "zetav", "rhov", "qe", "rhoe", "Fs", "eta", "tvn", "tw", "Kh")
+
+
+def _c_structs():
+    import ctypes as C
+    p = C.c_void_p
+
+    class Tables(C.Structure):
+        _fields_ = ([(n, C.c_int64) for n in ("nc", "ne", "nv", "nlev")]
+                    + [(n, C.c_int32) for n in ("cw", "vw", "nt", "vk", "iap_pv", "vertical", "five_band", "reserved")]
+                    + [(n, p) for n in _TABLE_INDEX + _TABLE_REAL + ("trisk_index",)])
+
+    class Fields(C.Structure):
+        _fields_ = [(n, p) for n in ("vn", "w", "rho", "rt", "theta", "exner", "K", "Kv", "qv", "zv", "rv", "qe",
+                                     "rhoe", "Fs", "eta", "tvn", "tw", "Kh")]
+    return Tables, Fields
+
+
+class MpasOracleC:
+    """slow_tendencies of MpasOracle in C with OpenMP on ``threads`` host threads."""
+
+    def __init__(self, t: dict, threads: int = 1):
+        import ctypes as C
+        from oracle.oracle import _lib
+        self.lib = _lib
+        Tables, Fields = _c_structs()
+        if _lib.mpas_oracle_tables_size() != C.sizeof(Tables) or _lib.mpas_oracle_fields_size() != C.sizeof(Fields):
+            raise RuntimeError("oracle struct layout mismatch")
+        self._Fields = Fields
+        s = Tables()
+        s.nc, s.ne, s.nv, s.nlev = t["nc"], t["ne"], t["nv"], t["nlev"]
+        s.cw, s.vw, s.nt = t["cell_edges"].shape[1], t["vertex_edges"].shape[1], t["trisk"].shape[1]
+        s.vk = int(t.get("vk_weights") is not None)
+        s.iap_pv, s.vertical, s.five_band = int(bool(t["iap_pv"])), int(t["vertical"]), int(bool(t["five_band"]))
+        self._keep = []
+        for name in _TABLE_INDEX + _TABLE_REAL + ("trisk_index",):
+            a = t.get(name)
+            if a is None:
+                continue
+            dt = np.int64 if name in _TABLE_INDEX else (np.int32 if name == "trisk_index" else np.float64)
+            a = np.ascontiguousarray(a, dtype=dt)
+            self._keep.append(a)
+            setattr(s, name, a.ctypes.data)
+        self._s = s
+        self.nc, self.ne, self.nv, self.nlev = t["nc"], t["ne"], t["nv"], t["nlev"]
+        self.vk = bool(s.vk)
+        self.threads = int(threads)
+
+    def slow_tendencies(self, vn, w, rho, rhotheta, pressure=1.0) -> dict:
+        import ctypes as C
+        nc, ne, nv, nl = self.nc, self.ne, self.nv, self.nlev
+        shapes = {"theta": (nl, nc), "exner": (nl, nc), "K": (nl, nc), "Kv": (nl, nv), "qv": (nl, nv),
+                  "zetav": (nl, nv), "rhov": (nl, nv), "qe": (nl, ne), "rhoe": (nl, ne), "Fs": (nl, ne),
+                  "eta": (nl + 1, ne), "tvn": (nl, ne), "tw": (nl + 1, nc), "Kh": (nl, nc)}
+        out = {k: np.zeros(v) for k, v in shapes.items()}
+        ins = [np.ascontiguousarray(x, dtype=np.float64) for x in (vn, w, rho, rhotheta)]
+        f = self._Fields()
+        for name, a in zip(("vn", "w", "rho", "rt"), ins):
+            setattr(f, name, a.ctypes.data)
+        for name, key in (("theta", "theta"), ("exner", "exner"), ("K", "K"), ("Kv", "Kv"), ("qv", "qv"),
+                          ("zv", "zetav"), ("rv", "rhov"), ("qe", "qe"), ("rhoe", "rhoe"), ("Fs", "Fs"),
+                          ("eta", "eta"), ("tvn", "tvn"), ("tw", "tw"), ("Kh", "Kh")):
+            setattr(f, name, out[key].ctypes.data)
+        self.lib.mpas_oracle_set_threads(self.threads)
+        self.lib.mpas_oracle_slow_tendencies(C.byref(self._s), C.byref(f), C.c_double(pressure))
+        del out["Kh"]
+        if not self.vk:
+            del out["Kv"]
         return out

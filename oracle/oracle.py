@@ -39,7 +39,9 @@ def build() -> None:
 
 
 def _load():
-    if not os.path.exists(LIB_PATH):
+    sources = [os.path.join(HERE, f) for f in ("trisk_oracle.c", "trisk_oracle.h", "mpas_oracle.c", "mpas_oracle.h")]
+    if not os.path.exists(LIB_PATH) or any(os.path.getmtime(f) > os.path.getmtime(LIB_PATH)
+                                           for f in sources if os.path.exists(f)):
         build()
     lib = C.CDLL(LIB_PATH)
     p, d = C.c_void_p, C.c_double
@@ -59,6 +61,10 @@ def _load():
         ("oracle_potential_enstrophy", d, [p, p, p]),
         ("oracle_relative_vorticity", None, [p, p, p]),
         ("oracle_tangential_velocity", None, [p, p, p]),
+        ("mpas_oracle_set_threads", None, [C.c_int]),
+        ("mpas_oracle_tables_size", C.c_int, []),
+        ("mpas_oracle_fields_size", C.c_int, []),
+        ("mpas_oracle_slow_tendencies", None, [p, p, d]),
     ]:
         fn = getattr(lib, name)
         fn.restype, fn.argtypes = res, args
