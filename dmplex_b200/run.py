@@ -1,22 +1,24 @@
-"""Williamson test case 2 (steady geostrophic solid-body rotation) on the GPU, the counterpart
-of the reference's examples/trisk_shallow_water.jl:
+"""The shallow-water examples of the reference on the GPU: Williamson test case 2 (steady
+geostrophic solid-body rotation, examples/trisk_shallow_water.jl) and the Galewsky jet
+(examples/trisk_galewsky.jl):
 
-    python -m dmplex_b200.run [mesh] [resolution] [flags]
+    python -m dmplex_b200.run [mesh] [resolution] [flags]                              # case 2
+    python -m dmplex_b200.run --case=galewsky [mesh] [resolution] [days] [perturbed] [flags]
 
 mesh: hexagon (the Voronoi dual of the icosahedral mesh, its generators as centers), triangle
 (the icosahedral mesh; the ICON model, --icon), or an ICON or MPAS grid file (classic NetCDF:
-TRiSK on its Voronoi cells, the ICON model with --icon on its triangles). Units a = Omega = g
-= 1; u0 = 0.2, h = 1 - (u0 + u0^2/2) z^2, dt = min(0.2 sqrt(4 pi / nc), 0.4 min d_e), one time
-unit (trisk_shallow_water.jl:79-108). Flags as there: --gassmann, --gassmann-mean,
---kinetic=cell|mixed|vertex|alpha, --spring[=beta], --scvt, --icon, --centered-k. Further:
+TRiSK on its Voronoi cells, the ICON model with --icon on its triangles). The cases, their
+units, time steps and report times are those of the examples (dmplex_b200.cases). Flags as
+there: --gassmann, --gassmann-mean, --kinetic=cell|mixed|vertex|alpha, --spring[=beta], --scvt,
+--icon, --centered-k. Further:
 
     --log=FILE        JSON-lines record of the diagnostics (RunLog)
     --checkpoint=FILE state written at the end (and every --every=N steps)
     --resume=FILE     continue from a checkpoint of the same mesh and configuration
-    --vtkhdf=FILE     cell vorticity (TRiSK) or height change (ICON) as a VTKHDF file
+    --vtkhdf=FILE     cell vorticity (TRiSK; 1/s for the Galewsky jet) or height change (ICON)
 
 The diagnostics (mass change, relative energy and enstrophy change, |h - h0|_2 and max, ms per
-step) are printed four times per run as the reference prints them. Runs on the GPU only.
+step) are printed at the examples' report steps. Runs on the GPU only.
 """
 from __future__ import annotations
 
@@ -27,34 +29,40 @@ import time
 
 import numpy as np
 
-U0 = 0.2
-
-
-def velocity(x):
-    return U0 * np.stack([-x[:, 1], x[:, 0], np.zeros(len(x))], axis=1)
-
-
-def height(x):
-    return 1 - (U0 + U0 ** 2 / 2) * x[:, 2] ** 2
+from .cases import CASES
 
 
 def parse(argv: list) -> dict:
-    """The example's arguments (trisk_shallow_water.jl:29-41, 79-82)."""
+    """The examples' arguments (trisk_shallow_water.jl:29-41, 79-82; trisk_galewsky.jl:39-51,
+    126-131) plus this driver's own."""
     flags = [a for a in argv if a.startswith("--")]
     pos = [a for a in argv if not a.startswith("--")]
-    icon = "--icon" in flags
-    spring = [a for a in flags if a.startswith("--spring")]
-    kinetic = [a.split("=", 1)[1] for a in flags if a.startswith("--kinetic=")]
     value = {a.split("=", 1)[0]: a.split("=", 1)[1] for a in flags if "=" in a}
     known = {"--icon", "--gassmann", "--gassmann-mean", "--scvt", "--centered-k", "--spring", "--kinetic", "--log",
-             "--checkpoint", "--resume", "--vtkhdf", "--every", "--device"}
+             "--checkpoint", "--resume", "--vtkhdf", "--every", "--device", "--case"}
     for a in flags:
         if a.split("=", 1)[0] not in known:
             raise ValueError(f"unknown flag {a}")
-    kin = kinetic[0] if kinetic else "cell"
+    case = value.get("--case", "williamson2")
+    if case not in CASES:
+        raise ValueError(f"unknown case {case} (one of {', '.join(CASES)})")
+    icon = "--icon" in flags
+    spring = [a for a in flags if a.startswith("--spring")]
+    kin = value.get("--kinetic", "cell")
+    galewsky = case == "galewsky"
+    if len(pos) > (4 if galewsky else 2):
+        raise ValueError("too many arguments")
+    perturbed = True
+    if galewsky and len(pos) > 3:
+        if pos[3].lower() not in ("true", "false"):
+            raise ValueError("perturbed must be true or false")
+        perturbed = pos[3].lower() == "true"
     return {
+        "case": case,
         "mesh": pos[0] if pos else ("triangle" if icon else "hexagon"),
-        "resolution": int(pos[1]) if len(pos) > 1 else 5,
+        "resolution": int(pos[1]) if len(pos) > 1 else (6 if galewsky else 5),
+        "days": float(pos[2]) if galewsky and len(pos) > 2 else (6.0 if galewsky else None),
+        "perturbed": perturbed,
         "icon": icon,
         "pv_flux": "gassmann_mean" if "--gassmann-mean" in flags else "gassmann" if "--gassmann" in flags else "trisk",
         "kinetic_energy": kin if kin in ("cell", "mixed", "vertex") else float(kin),
@@ -67,9 +75,14 @@ def parse(argv: list) -> dict:
     }
 
 
+def make_case(cfg: dict):
+    return CASES[cfg["case"]](cfg["days"], cfg["perturbed"])
+
+
 def config_meta(cfg: dict) -> dict:
     """What a checkpoint records of the run's configuration (a resume must match it)."""
-    keys = ("mesh", "resolution", "icon", "pv_flux", "kinetic_energy", "spring_beta", "centroidal", "kinetic_gradient")
+    keys = ("case", "mesh", "resolution", "days", "perturbed", "icon", "pv_flux", "kinetic_energy", "spring_beta",
+            "centroidal", "kinetic_gradient")
     return json.loads(json.dumps({k: cfg[k] for k in keys}))
 
 
@@ -91,18 +104,24 @@ def load_mesh(cfg: dict):
     return d.read_grid(mesh, dual=(not cfg["icon"]) if icon_file else cfg["icon"])
 
 
-class _TriskEngine:
-    """TRiSKShallowWater on the GPU with the example's diagnostics."""
+def edge_and_cell_state(grid, case) -> np.ndarray:
+    """[u; h]: the normal wind at the edge points, the height at the cell centers."""
+    u = np.einsum("ij,ij->i", case.velocity(grid.edge_points), grid.edge_normals)
+    return np.ascontiguousarray(np.concatenate([u, case.height(grid.centers)]))
 
-    def __init__(self, grid, cfg):
+
+class _TriskEngine:
+    """TRiSKShallowWater on the GPU with the examples' diagnostics."""
+
+    def __init__(self, grid, cfg, case, dt):
         import dmplex_b200 as d
-        self.d, self.grid = d, grid
-        self.m = d.TRiSKShallowWater(grid, pv_flux=cfg["pv_flux"], kinetic_energy=cfg["kinetic_energy"],
-                                     device=cfg["device"])
+        self.d, self.grid, self.case = d, grid, case
+        self.m = d.TRiSKShallowWater(grid, gravity=case.gravity, omega=1.0, pv_flux=cfg["pv_flux"],
+                                     kinetic_energy=cfg["kinetic_energy"], device=cfg["device"])
         self.cache = None
 
     def initial_state(self):
-        return self.d.initial_state(self.m, velocity, height)
+        return self.d.initial_state(self.m, self.case.velocity, self.case.height)
 
     def step(self, y, dt, n):
         if self.cache is None:
@@ -116,21 +135,21 @@ class _TriskEngine:
 
     def cell_field(self, y, y0):
         from .vtkhdf import cell_vorticity
-        return "vorticity", cell_vorticity(self.grid, y)
+        return "vorticity", self.case.vorticity_scale * cell_vorticity(self.grid, y)
 
 
 class _IconEngine:
-    """ICONShallowWater on the GPU (mass only among the invariants, as the model offers)."""
+    """ICONShallowWater on the GPU (mass only among the invariants, as the model offers), with
+    the case's divergence damping."""
 
-    def __init__(self, grid, cfg):
+    def __init__(self, grid, cfg, case, dt):
         from .icon import ICONShallowWater
-        self.grid = grid
-        self.m = ICONShallowWater(grid, kinetic_gradient=cfg["kinetic_gradient"], device=cfg["device"])
+        self.grid, self.case = grid, case
+        self.m = ICONShallowWater(grid, gravity=case.gravity, divergence_damping=case.icon_damping(grid, dt),
+                                  kinetic_gradient=cfg["kinetic_gradient"], device=cfg["device"])
 
     def initial_state(self):
-        g = self.grid
-        u = np.einsum("ij,ij->i", velocity(g.edge_points), g.edge_normals)
-        return np.ascontiguousarray(np.concatenate([u, height(g.centers)]))
+        return edge_and_cell_state(self.grid, self.case)
 
     def step(self, y, dt, n):
         self.m.rk4_step(y, dt, n)
@@ -143,23 +162,23 @@ class _IconEngine:
 
 
 def main(argv: list | None = None, engine=None) -> dict:
-    """Run the case; returns the last diagnostics record. ``engine(grid, cfg)`` replaces the
-    GPU model (used by the tests with the CPU oracle)."""
+    """Run the case; returns the last diagnostics record. ``engine(grid, cfg, case, dt)``
+    replaces the GPU model (used by the tests with the CPU oracle)."""
     import dmplex_b200 as d
     from .checkpoint import RunLog, load_state, save_state
     cfg = parse(sys.argv[1:] if argv is None else argv)
+    case = make_case(cfg)
     mesh = load_mesh(cfg)
     g = d.TRiSKGrid(mesh)
+    dt, nsteps = case.steps(g)
     if engine is None:
         engine = _IconEngine if cfg["icon"] else _TriskEngine
-    model = engine(g, cfg)
-    print(f"{g.nc} cells, {g.ne} edges, {g.nv} vertices, {'ICON' if cfg['icon'] else cfg['pv_flux']} model",
-          flush=True)
+    model = engine(g, cfg, case, dt)
+    print(f"{g.nc} cells, {g.ne} edges, {g.nv} vertices; {case.name}, "
+          f"{'ICON' if cfg['icon'] else cfg['pv_flux']} model; {nsteps} RK4 steps", flush=True)
     y0 = model.initial_state()
     y = y0.copy()
     h0 = y0[g.ne:].copy()
-    dt = min(0.2 * math.sqrt(4 * math.pi / g.nc), 0.4 * float(g.dual_lengths.min()))
-    nsteps = math.ceil(1.0 / dt)
     start = 0
     meta = config_meta(cfg)
     if cfg["resume"]:
@@ -168,31 +187,33 @@ def main(argv: list | None = None, engine=None) -> dict:
             raise ValueError("the checkpoint was written by a run of another configuration")
         start = header["step"]
     inv0 = model.diagnostics(y0)
+    reports = case.reports(nsteps)
+    stops = sorted(reports | ({s for s in range(cfg["every"], nsteps + 1, cfg["every"])} if cfg["every"] else set()))
     log = RunLog(cfg["log"], **meta) if cfg["log"] else None
     elapsed, last = 0.0, {}
-    every = max(1, nsteps // 4)
     step = start
     try:
-        while step < nsteps:
-            n = min(every - step % every, nsteps - step)
-            if cfg["every"]:
-                n = min(n, cfg["every"] - step % cfg["every"])
+        for stop in stops:
+            if stop <= step:
+                continue
             t0 = time.perf_counter()
-            model.step(y, dt, n)
+            model.step(y, dt, stop - step)
             elapsed += time.perf_counter() - t0
-            step += n
+            step = stop
             if cfg["checkpoint"] and cfg["every"] and step % cfg["every"] == 0:
                 save_state(cfg["checkpoint"], y, g, step=step, time=step * dt, meta={"config": meta})
-            if step % every == 0 or step == nsteps:
+            if step in reports:
                 inv = model.diagnostics(y)
                 dh = y[g.ne:] - h0
-                last = {"step": step, "t": step * dt, "h_l2": float(np.sqrt(np.sum(g.cell_areas * dh ** 2) / (4 * np.pi))),
-                        "h_max": float(np.abs(dh).max()), "mass": inv["mass"] - inv0["mass"],
+                last = {"step": step, case.time_label: step * dt / case.time_unit,
+                        "h_l2": float(np.sqrt(np.sum(g.cell_areas * dh ** 2) / (4 * np.pi))),
+                        "h_max": float(np.abs(dh).max()), "mass": (inv["mass"] - inv0["mass"]) / inv0["mass"],
                         "ms_per_step": 1e3 * elapsed / max(step - start, 1)}
                 for k in ("energy", "enstrophy"):
                     if k in inv:
                         last[k] = (inv[k] - inv0[k]) / inv0[k]
-                print("t = {t:.3f}  |h - h0|_2 = {h_l2:.3e}  max = {h_max:.3e}  mass: {mass:.2e}".format(**last)
+                print(f"{case.time_label} = {last[case.time_label]:.3f}  |h - h0|_2 = {last['h_l2']:.3e}  "
+                      f"max = {last['h_max']:.3e}  mass: {last['mass']:.2e}"
                       + "".join(f"  {k}: {last[k]:.2e}" for k in ("energy", "enstrophy") if k in last), flush=True)
                 if log:
                     log.write(**last)

@@ -1,7 +1,8 @@
-"""The Williamson-2 driver (the counterpart of the reference's examples/trisk_shallow_water.jl):
-its flags, a whole run with the CPU oracle standing in for the GPU model (diagnostics, run
-log, checkpoints, VTKHDF output), a resumed run equal to the uninterrupted one bit for bit,
-and on the GPU the same run through the library's models."""
+"""The shallow-water driver (the counterpart of the reference's examples/trisk_shallow_water.jl
+and examples/trisk_galewsky.jl): its flags, a whole run with the CPU oracle standing in for
+the GPU model (diagnostics, run log, checkpoints, VTKHDF output), a resumed run equal to the
+uninterrupted one bit for bit, the Galewsky jet's set-up, and on the GPU the same runs through
+the library's TRiSK and ICON models."""
 import numpy as np
 import pytest
 
@@ -16,14 +17,13 @@ from hdf5_spec_reader import read_hdf5
 class OracleEngine:
     """The CPU oracle behind the driver's engine interface (test infrastructure)."""
 
-    def __init__(self, grid, cfg):
-        self.grid = grid
-        self.o = Oracle(d.model_tables(grid, pv_flux=cfg["pv_flux"], kinetic_energy=cfg["kinetic_energy"]))
+    def __init__(self, grid, cfg, case, dt):
+        self.grid, self.case = grid, case
+        self.o = Oracle(d.model_tables(grid, gravity=case.gravity, omega=1.0, pv_flux=cfg["pv_flux"],
+                                       kinetic_energy=cfg["kinetic_energy"]))
 
     def initial_state(self):
-        g = self.grid
-        u = np.einsum("ij,ij->i", run.velocity(g.edge_points), g.edge_normals)
-        return np.ascontiguousarray(np.concatenate([u, run.height(g.centers)]))
+        return run.edge_and_cell_state(self.grid, self.case)
 
     def step(self, y, dt, n):
         self.o.rk4_step(y, dt, n)
@@ -34,7 +34,7 @@ class OracleEngine:
 
     def cell_field(self, y, y0):
         from dmplex_b200.vtkhdf import cell_vorticity
-        return "vorticity", cell_vorticity(self.grid, y)
+        return "vorticity", self.case.vorticity_scale * cell_vorticity(self.grid, y)
 
 
 def test_parse():
@@ -48,8 +48,15 @@ def test_parse():
     assert (c["pv_flux"], c["kinetic_energy"], c["centroidal"], c["spring_beta"], c["every"]) == (
         "gassmann_mean", 0.375, True, 1.1, 7)
     assert run.parse(["--kinetic=vertex", "--gassmann"])["kinetic_energy"] == "vertex"
-    with pytest.raises(ValueError):
-        run.parse(["--bogus"])
+    c = run.parse(["--case=galewsky", "hexagon", "7", "2.5", "false", "--gassmann-mean"])
+    assert (c["case"], c["resolution"], c["days"], c["perturbed"], c["pv_flux"]) == (
+        "galewsky", 7, 2.5, False, "gassmann_mean")
+    c = run.parse(["--case=galewsky"])
+    assert (c["resolution"], c["days"], c["perturbed"]) == (6, 6.0, True)
+    for bad in (["--bogus"], ["--case=unknown"], ["hexagon", "3", "1.0"], ["--case=galewsky", "hexagon", "3", "1",
+                                                                            "maybe"]):
+        with pytest.raises(ValueError):
+            run.parse(bad)
     with pytest.raises(ValueError):
         run.load_mesh(run.parse(["no_such_file.nc"]))
 
@@ -70,10 +77,11 @@ def test_driver_with_the_oracle(tmp_path, capsys):
     # a run resumed from a checkpoint of the same configuration after 5 steps ends in the
     # same state, bit for bit
     cfg = run.parse(args)
+    case = run.make_case(cfg)
     g = d.TRiSKGrid(run.load_mesh(cfg))
-    eng = OracleEngine(g, cfg)
+    dt, _ = case.steps(g)
+    eng = OracleEngine(g, cfg, case, dt)
     y = eng.initial_state()
-    dt = min(0.2 * np.sqrt(4 * np.pi / g.nc), 0.4 * float(g.dual_lengths.min()))
     eng.step(y, dt, 5)
     save_state(str(tmp_path / "mid.bin"), y, g, step=5, time=5 * dt, meta={"config": run.config_meta(cfg)})
     run.main(["hexagon", "3", "--gassmann", "--kinetic=vertex", f"--resume={tmp_path / 'mid.bin'}",
@@ -94,11 +102,45 @@ def test_driver_fails_loudly_without_a_gpu():
         run.main(["hexagon", "2"])
 
 
+def test_galewsky_case():
+    """The jet: the balanced height has mean depth 1 and balances the jet up to a truncation
+    error that falls with resolution (its tendency against that of the same jet over a flat
+    surface: 9 % at level 4, less than half that at level 5); half a day with
+    the oracle conserves mass, energy and enstrophy as the scheme does, reported in days."""
+    from dmplex_b200.cases import Galewsky
+    case = Galewsky(days=0.5, perturbed=False)
+    phi = np.linspace(-np.pi / 2, np.pi / 2, 2001)
+    h = case.balanced_height(phi)
+    assert abs(np.trapezoid(h * np.cos(phi), phi) / 2 - 1) < 1e-6
+    assert case.jet(np.array([0.0, np.pi / 4, 1.2]))[0] == 0 and case.jet(np.array([np.pi / 4]))[0] > 0.7 * case.u_max
+
+    def imbalance(level):
+        g = d.TRiSKGrid(d.create_hexagon_mesh(level))
+        o = Oracle(d.model_tables(g, gravity=case.gravity, omega=1.0))
+        y = run.edge_and_cell_state(g, case)
+        flat = y.copy()
+        flat[g.ne:] = 1.0
+        return np.linalg.norm(o.tendency(y)) / np.linalg.norm(o.tendency(flat)), g, y
+    r4, g, y = imbalance(4)
+    r5, _, _ = imbalance(5)
+    assert r4 < 0.15 and r5 < r4 / 2                 # balanced up to a truncation error that converges
+    perturbed = run.edge_and_cell_state(g, Galewsky(days=0.5))
+    assert 0 < np.abs(perturbed - y).max() <= 120 / 1e4
+    last = run.main(["--case=galewsky", "hexagon", "3", "0.5", "--kinetic=vertex"], engine=OracleEngine)
+    assert last["day"] == pytest.approx(0.5) and abs(last["mass"]) < 1e-14
+    assert abs(last["energy"]) < 1e-5 and abs(last["enstrophy"]) < 1e-2
+
+
 @pytest.mark.gpu
-@pytest.mark.parametrize("args", [["hexagon", "3", "--gassmann", "--kinetic=vertex"], ["triangle", "3", "--icon"]])
+@pytest.mark.parametrize("args", [["hexagon", "3", "--gassmann", "--kinetic=vertex"], ["triangle", "3", "--icon"],
+                                  ["--case=galewsky", "hexagon", "4", "0.5"],
+                                  ["--case=galewsky", "triangle", "4", "0.5", "--icon"]])
 def test_driver_on_the_gpu(require_gpu, tmp_path, args):
     last = run.main(args + [f"--log={tmp_path / 'run.jsonl'}", f"--checkpoint={tmp_path / 'end.bin'}",
                             f"--vtkhdf={tmp_path / 'out.vtkhdf'}"])
-    assert abs(last["mass"]) < 1e-13 and last["h_l2"] < 2e-3
-    assert len(read_run_log(str(tmp_path / "run.jsonl"))) == 4
+    assert abs(last["mass"]) < 1e-13
+    if "--case=galewsky" not in args:
+        assert last["h_l2"] < 2e-3 and len(read_run_log(str(tmp_path / "run.jsonl"))) == 4
+    else:
+        assert len(read_run_log(str(tmp_path / "run.jsonl"))) == 1 and last["day"] == pytest.approx(0.5)
     read_hdf5(str(tmp_path / "out.vtkhdf"))
