@@ -58,6 +58,7 @@ def parse():
     p.add_argument("--ensemble-days", type=float, default=1.0, help="simulated days of the ensemble leg")
     p.add_argument("--no-icon", action="store_true", help="skip the ICON triangle-model leg")
     p.add_argument("--no-mpas", action="store_true", help="skip the 3-D MPAS-Gassmann operators leg")
+    p.add_argument("--no-galewsky", action="store_true", help="skip the Galewsky-jet leg (hexagon 8, 6 days)")
     p.add_argument("--level", type=int, default=LEVEL, help="mesh level (7 is the benchmark workload)")
     p.add_argument("--block", default=None,
                    help="fixed block sizes of the three phases, e.g. 128,128,64 (skips the autotuner)")
@@ -214,6 +215,52 @@ def run_icon_leg(local_rank, level=8, steps=100, hilbert=True):
             "published_a100_ms_per_step_same_size": {7: 1.5, 8: 2.4, 9: 7.8}.get(level),
             "note": "the reference's A100 figure is on the ICON grid file of this size (R02B06/07/08 for "
                     "levels 7/8/9); this mesh is the icosahedral bisection of the same size"}
+
+
+def run_galewsky_leg(local_rank, level=8, days=6.0, schemes=("trisk", "gassmann")):
+    """The Galewsky jet of the reference's examples/trisk_galewsky.jl through the public API:
+    create_hexagon_mesh(level) with its generators as centers, the example's nondimensional
+    gravity, balanced height and bump, dt rule and `days` days, FP64, device-resident state,
+    the wall time of all RK4 steps (one synchronous rk4_step call after a 2-step warm-up on a
+    copy), and the outcome the reference reports beside it: potential enstrophy change and the
+    largest relative vorticity. The reference: 28 s (TRiSK), 58 s (gassmann) and 43 s
+    (gassmann_mean) for hexagon 8 over 6 days on 4 x A100, |zeta| <= 1.6e-4 1/s and +0.4 %
+    enstrophy for TRiSK, 5e-4 and +51 % for gassmann (docs/STATUS.md:30-34)."""
+    import torch
+    import dmplex_b200 as d
+    from dmplex_b200.cases import OMEGA, Galewsky
+    from dmplex_b200.vtkhdf import cell_vorticity
+    case = Galewsky(days)
+    g = d.TRiSKGrid(d.create_hexagon_mesh(level))
+    dt, nsteps = case.steps(g)
+    dev = f"cuda:{local_rank}"
+    out = {"workload": f"Galewsky jet, create_hexagon_mesh({level}), {days:g} days, FP64", "cells": g.nc,
+           "steps": nsteps, "dt_seconds": dt / OMEGA}
+    published = {"trisk": 28.0, "gassmann": 58.0, "gassmann_mean": 43.0}
+    published_outcome = {"trisk": "|zeta| <= 1.6e-4 1/s, potential enstrophy +0.4 %",
+                         "gassmann_mean": "|zeta| <= 1.6e-4 1/s, potential enstrophy +0.4 %",
+                         "gassmann": "|zeta| 5e-4 1/s, potential enstrophy +51 %"}
+    for pv in schemes:
+        m = d.TRiSKShallowWater(g, gravity=case.gravity, omega=1.0, pv_flux=pv, device=local_rank)
+        y = torch.from_numpy(d.initial_state(m, case.velocity, case.height)).to(dev)
+        warm = y.clone()
+        d.rk4_step(warm, dt, d.tendency, d.RK4Cache(warm), m, nsteps=2)
+        mass0, energy0, ens0 = d.total_mass(m, y), d.total_energy(m, y), d.potential_enstrophy(m, y)
+        torch.cuda.synchronize(local_rank)
+        t0 = time.perf_counter()
+        d.rk4_step(y, dt, d.tendency, d.RK4Cache(y), m, nsteps=nsteps)
+        torch.cuda.synchronize(local_rank)
+        wall = time.perf_counter() - t0
+        zeta = OMEGA * cell_vorticity(g, y.cpu().numpy())
+        out[pv] = {"seconds": wall, "ms_per_step": 1e3 * wall / nsteps,
+                   "mass_change": (d.total_mass(m, y) - mass0) / mass0,
+                   "energy_change": (d.total_energy(m, y) - energy0) / energy0,
+                   "enstrophy_change": (d.potential_enstrophy(m, y) - ens0) / ens0,
+                   "max_abs_vorticity_per_s": float(np.abs(zeta).max()),
+                   "published_4xa100_seconds": published.get(pv),
+                   "published_outcome": published_outcome.get(pv)}
+        del m
+    return out
 
 
 def run_mpas_leg(local_rank, level=7, nlev=30, calls=50, cpu_level=None, hilbert=True, lpt=0, cpu_calls=3):
@@ -630,6 +677,9 @@ def run_b200(args, rank, world, local_rank):
     mpas_leg = None
     if not args.no_mpas:
         mpas_leg = optional_leg(run_mpas_leg, local_rank)
+    galewsky = None
+    if world == 1 and not args.no_galewsky:   # an end-to-end run, not a per-GPU rate: at N = 1 only
+        galewsky = optional_leg(run_galewsky_leg, local_rank)
     hexagon5 = None
     if rank == 0 and not args.no_hexagon5:
         hexagon5 = optional_leg(run_hexagon5_leg, local_rank, os.cpu_count() or 1,
@@ -647,7 +697,7 @@ def run_b200(args, rank, world, local_rank):
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": config_dict(g, world, args.level), "clocks": clocks.summary(), "e2e": e2e,
                 "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu, "ensemble": ensemble,
-                "closure": closure, "hexagon5": hexagon5, "icon": icon_leg, "mpas": mpas_leg}
+                "closure": closure, "hexagon5": hexagon5, "icon": icon_leg, "mpas": mpas_leg, "galewsky": galewsky}
         print(json.dumps(line), flush=True)
     del m
 
