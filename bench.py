@@ -224,8 +224,8 @@ def run_galewsky_leg(local_rank, level=8, days=6.0, schemes=("trisk", "gassmann"
     the wall time of all RK4 steps (one synchronous rk4_step call after a 2-step warm-up on a
     copy), and the outcome the reference reports beside it: potential enstrophy change and the
     largest relative vorticity. The reference: 28 s (TRiSK), 58 s (gassmann) and 43 s
-    (gassmann_mean) for hexagon 8 over 6 days on 4 x A100, |zeta| <= 1.6e-4 1/s and +0.4 %
-    enstrophy for TRiSK, 5e-4 and +51 % for gassmann (docs/STATUS.md:30-34)."""
+    (gassmann_mean) for hexagon 8 over 6 days on 4 x A100, and on hexagon 7 |zeta| <= 1.6e-4 1/s
+    and +0.4 % enstrophy for TRiSK, 5e-4 and +51 % for gassmann (docs/STATUS.md:29-34)."""
     import torch
     import dmplex_b200 as d
     from dmplex_b200.cases import OMEGA, Galewsky
@@ -237,9 +237,9 @@ def run_galewsky_leg(local_rank, level=8, days=6.0, schemes=("trisk", "gassmann"
     out = {"workload": f"Galewsky jet, create_hexagon_mesh({level}), {days:g} days, FP64", "cells": g.nc,
            "steps": nsteps, "dt_seconds": dt / OMEGA}
     published = {"trisk": 28.0, "gassmann": 58.0, "gassmann_mean": 43.0}
-    published_outcome = {"trisk": "|zeta| <= 1.6e-4 1/s, potential enstrophy +0.4 %",
-                         "gassmann_mean": "|zeta| <= 1.6e-4 1/s, potential enstrophy +0.4 %",
-                         "gassmann": "|zeta| 5e-4 1/s, potential enstrophy +51 %"}
+    published_outcome = {"trisk": "hexagon 7: |zeta| <= 1.6e-4 1/s, potential enstrophy +0.4 %",
+                         "gassmann_mean": "hexagon 7: |zeta| <= 1.6e-4 1/s, potential enstrophy +0.4 %",
+                         "gassmann": "hexagon 7: |zeta| 5e-4 1/s, potential enstrophy +51 %"}
     for pv in schemes:
         m = d.TRiSKShallowWater(g, gravity=case.gravity, omega=1.0, pv_flux=pv, device=local_rank)
         y = torch.from_numpy(d.initial_state(m, case.velocity, case.height)).to(dev)
