@@ -134,7 +134,7 @@ def test_galewsky_case():
 @pytest.mark.gpu
 @pytest.mark.parametrize("args", [["hexagon", "3", "--gassmann", "--kinetic=vertex"], ["triangle", "3", "--icon"],
                                   ["--case=galewsky", "hexagon", "4", "0.5"],
-                                  ["--case=galewsky", "triangle", "4", "0.5", "--icon"]])
+                                  ["--case=galewsky", "triangle", "4", "0.5", "--icon", "--centered-k"]])
 def test_driver_on_the_gpu(require_gpu, tmp_path, args):
     last = run.main(args + [f"--log={tmp_path / 'run.jsonl'}", f"--checkpoint={tmp_path / 'end.bin'}",
                             f"--vtkhdf={tmp_path / 'out.vtkhdf'}"])
