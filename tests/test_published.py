@@ -3,7 +3,8 @@ its test suite: the kinetic-energy error of a solid-body rotation for the cell a
 on plain, spring-dynamics and centroidal hexagon meshes (:95-96), the TRiSK tangential
 reconstruction error on the three meshes (:61-62), and Williamson test case 2 at t = 1 — max
 and L2 height errors on spring hexagons for the cell, mixed and vertex kinetic energy
-(:96-98) and the L2 error on centroidal hexagons (:63-64). Each published figure is checked to
+(:96-98) and the L2 error on centroidal hexagons (:63-64); for the ICON model, the mesh
+asymmetry and TC2 error on bisection and spring triangles (:40-55). Each published figure is checked to
 its significant digits as printed: ours must round to it, within half a unit of its last digit
 plus 1 % for the rounding of the geometry. These pin the mesh generators, the TRiSK tables,
 the kinetic-energy forms and the time stepping together; the GPU path equals the oracle bit
@@ -119,3 +120,51 @@ def test_level7_figures():
         solid = np.einsum("ij,ij->i", np.cross(w, g.edge_points), g.edge_normals)
         tang = np.einsum("ij,ij->i", np.cross(w, g.edge_points), np.cross(g.edge_points, g.edge_normals))
         assert close(np.abs(Oracle(d.model_tables(g)).tangential_velocity(solid) - tang).max(), pub)
+
+
+# the ICON triangle model (docs/STATUS.md:40-55)
+def _triangles(kind, n):
+    return d.TRiSKGrid(d.create_triangle_mesh(n, **({"spring_beta": 1.2} if kind == "spring" else {})))
+
+
+def _asymmetry(g):
+    """max |d_l - d_r| / d over the edges: how far the circumcenters sit from symmetric."""
+    return (np.abs(g.cell_distances[:, 0] - g.cell_distances[:, 1]) / g.dual_lengths).max()
+
+
+def _icon_tc2_l2(g):
+    from dmplex_b200 import icon
+    from oracle.icon_oracle import IconOracle
+    o = IconOracle(icon.icon_tables(g))
+    u0 = 0.2
+    x = g.edge_points
+    u = u0 * np.einsum("ij,ij->i", np.stack([-x[:, 1], x[:, 0], np.zeros(len(x))], axis=1), g.edge_normals)
+    y = np.concatenate([u, 1 - (u0 + u0 ** 2 / 2) * g.centers[:, 2] ** 2])
+    y0 = y.copy()
+    dt = min(0.2 * np.sqrt(4 * np.pi / g.nc), 0.4 * float(g.dual_lengths.min()))
+    o.rk4_step(y, dt, int(np.ceil(1 / dt)))
+    dh = (y - y0)[g.ne:]
+    return np.sqrt(np.sum(g.cell_areas * dh ** 2) / (4 * np.pi))
+
+
+def test_icon_on_bisection_and_spring_triangles():
+    """Plain bisection keeps max |d_l - d_r|/d = 0.19 at every level; TC2 L2 8.5e-5 on 1280
+    cells, 1.9e-5 / 7.0e-6 on triangle 4/5 (convergence stalls); with spring dynamics
+    (beta = 1.2) TC2 2.3e-5 / 5.6e-6 on triangle 4/5 (second order)."""
+    for n in (3, 4, 5):
+        assert close(_asymmetry(_triangles("plain", n)), "0.19")
+    for n, pub in ((3, "8.5e-5"), (4, "1.9e-5"), (5, "7.0e-6")):
+        assert close(_icon_tc2_l2(_triangles("plain", n)), pub), n
+    for n, pub in ((4, "2.3e-5"), (5, "5.6e-6")):
+        assert close(_icon_tc2_l2(_triangles("spring", n)), pub), n
+
+
+@pytest.mark.slow
+@pytest.mark.skipif(not os.environ.get("TRISK_LONG_TESTS"), reason="long: set TRISK_LONG_TESTS=1")
+def test_icon_level6_and_7_figures():
+    """TC2 L2 3.9e-6 (plain) and 1.4e-6 (spring) on triangle 6; spring asymmetry 0.10 / 0.089
+    on levels 6 / 7."""
+    assert close(_icon_tc2_l2(_triangles("plain", 6)), "3.9e-6")
+    g6 = _triangles("spring", 6)
+    assert close(_icon_tc2_l2(g6), "1.4e-6")
+    assert close(_asymmetry(g6), "0.10") and close(_asymmetry(_triangles("spring", 7)), "0.089")
