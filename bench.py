@@ -282,8 +282,10 @@ def run_galewsky_leg(local_rank, level=8, days=6.0, schemes=("trisk", "gassmann"
         yh = y.cpu().numpy()
         out["icon_centered"] = {"cells": gt.nc, "steps": ni, "seconds": wall, "ms_per_step": 1e3 * wall / ni,
                                 "mass_change": (m.total_mass(yh) - mass0) / mass0, "finite": bool(np.isfinite(yh).all()),
+                                "max_abs_vorticity_per_s": float(np.abs(OMEGA * cell_vorticity(gt, yh)).max()),
                                 "published": "ICON model on the ICON grid R02B07 (the same number of triangles), "
-                                             "4 x A100: 6 days in 60 s (docs/EXAMPLES.md:126-129)"}
+                                             "4 x A100: 40406 steps in 60 s, |zeta| <= 1.7e-4 1/s "
+                                             "(docs/STATUS.md:104-105)"}
         del m
     return out
 

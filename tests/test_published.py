@@ -168,3 +168,24 @@ def test_icon_level6_and_7_figures():
     g6 = _triangles("spring", 6)
     assert close(_icon_tc2_l2(g6), "1.4e-6")
     assert close(_asymmetry(g6), "0.10") and close(_asymmetry(_triangles("spring", 7)), "0.089")
+
+
+@pytest.mark.slow
+@pytest.mark.skipif(not os.environ.get("TRISK_LONG_TESTS"), reason="long: set TRISK_LONG_TESTS=1")
+def test_icon_galewsky_on_bisection_triangles():
+    """The Galewsky jet on plain triangle 5 blows up before day 3 with ICON's kinetic-energy
+    gradient and stays stable with the centered one (:44-50)."""
+    from dmplex_b200 import icon, run
+    from dmplex_b200.cases import Galewsky
+    from oracle.icon_oracle import IconOracle
+    case = Galewsky(3.0)
+    g = _triangles("plain", 5)
+    dt, n = case.steps(g)
+    for gradient, survives in (("icon", False), ("centered", True)):
+        t = icon.icon_tables(g, gravity=case.gravity, kinetic_gradient=gradient)
+        t["divergence_damping"] = case.icon_damping(g, dt)
+        o = IconOracle(t)
+        y = run.edge_and_cell_state(g, case)
+        with np.errstate(all="ignore"):
+            o.rk4_step(y, dt, n)
+        assert bool(np.isfinite(y).all() and np.abs(y[:g.ne]).max() < 1.0) == survives, gradient
