@@ -13,7 +13,9 @@ entities with each per-entity sum in the reference's order (numpy does not contr
 
 It works on the tables of dmplex_b200.icon.icon_tables (1-based, (entity, k)), the same the
 library uploads. Its correctness is pinned by the reference's own ICON test assertions
-(test/finite_volumes.jl:112-166) in tests/test_icon.py.
+(test/finite_volumes.jl:112-166) in tests/test_icon.py, and by the ICON figures it publishes
+(docs/STATUS.md:40-55: TC2 errors on bisection and spring triangles, the Galewsky failure mode
+of ICON's kinetic-energy gradient) in tests/test_published.py.
 """
 from __future__ import annotations
 

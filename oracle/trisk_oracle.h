@@ -23,7 +23,11 @@
  * cannot run here (no Julia). The oracle is pinned by the reference's own test-suite
  * properties (test/finite_volumes.jl: operator identities, semi-discrete energy
  * conservation, mass conservation to round-off, TC2 error and convergence bounds), which
- * tests/test_oracle.py re-runs against it. Bitwise agreement with Julia is unverifiable.
+ * tests/test_oracle.py re-runs against it, and by the accuracy figures the reference publishes
+ * for this path (docs/STATUS.md: kinetic-energy, tangential and TC2 errors on plain, spring
+ * and centroidal meshes; the Galewsky outcome of each PV flux), which tests/test_published.py
+ * and tests/test_galewsky_pin.py reproduce to the digits printed. Bitwise agreement with
+ * Julia is unverifiable.
  */
 #ifndef TRISK_ORACLE_H
 #define TRISK_ORACLE_H
