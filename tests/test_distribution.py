@@ -1,9 +1,10 @@
 """Domain decomposition with a halo exchange per tendency (the reference's TRiSKDistribution):
 the equal-area partition, the owned/ghost sets, and the reference's 1-vs-n property
-(test/finite_volumes.jl:245-261): owned values after RK4 steps on 2 or 3 ranks equal the
-undivided run bit for bit. On CPU the local tendency is the oracle's on the local tables
-(gloo ranks); on the GPU, two ranks share one GPU and exchange through host memory (gloo),
-each running the library's kernels on its local tables."""
+(test/finite_volumes.jl:245-261; "1, 3, 4 ranks bitwise identical", docs/STATUS.md:15-18):
+owned values after RK4 steps on 2, 3 or 4 ranks equal the undivided run bit for bit. On CPU
+the local tendency is the oracle's on the local tables (gloo ranks); on the GPU, two ranks
+share one GPU and exchange through host memory (gloo), each running the library's kernels on
+its local tables."""
 import os
 import socket
 
@@ -102,7 +103,7 @@ def _spawn(target, world, *args):
 
 
 @pytest.mark.parametrize("world,pv,ke", [(2, "trisk", "cell"), (3, "gassmann", "vertex"),
-                                         (2, "gassmann_mean", "mixed")])
+                                         (2, "gassmann_mean", "mixed"), (4, "trisk", "mixed")])
 def test_one_vs_n_bitwise_cpu(world, pv, ke):
     import dmplex_b200 as d
     from dmplex_b200 import workloads as w
