@@ -185,7 +185,7 @@ def optional_leg(fn, *args, **kwargs):
         return {"error": f"{type(exc).__name__}: {exc}"}
 
 
-def run_icon_leg(local_rank, level=8, steps=100, hilbert=True):
+def run_icon_leg(local_rank, level=8, steps=100, hilbert=True, cpu_steps=3):
     """ICON triangle shallow water (the reference's ICONShallowWater) on create_triangle_mesh
     (level), plain bisection — 20 * 4^level triangles, the size of the ICON grid R02B(level - 1): Williamson
     test case 2 on the unit sphere, dt = 0.2 min d_e, `steps` RK4 steps on a device-resident
@@ -201,7 +201,8 @@ def run_icon_leg(local_rank, level=8, steps=100, hilbert=True):
     x = g.edge_points
     u = u0 * (-x[:, 1] * g.edge_normals[:, 0] + x[:, 0] * g.edge_normals[:, 1])
     h = 1 - (u0 + u0 ** 2 / 2) * g.centers[:, 2] ** 2
-    yd = torch.from_numpy(np.concatenate([u, h])).to(f"cuda:{local_rank}")
+    y_host = np.concatenate([u, h])
+    yd = torch.from_numpy(y_host).to(f"cuda:{local_rank}")
     dt = 0.2 * float(g.dual_lengths.min())
     m.rk4_step(yd, dt, 5)
     torch.cuda.synchronize(local_rank)
@@ -209,9 +210,21 @@ def run_icon_leg(local_rank, level=8, steps=100, hilbert=True):
     m.rk4_step(yd, dt, steps)
     torch.cuda.synchronize(local_rank)
     ms = (time.perf_counter() - t0) * 1e3 / steps
+    # CPU baseline: the oracle's C port on all host cores, a few steps of the same workload
+    from oracle.icon_oracle import IconOracleC
+    threads = os.cpu_count() or 1
+    o = IconOracleC(m.tables, threads=threads)
+    yc = y_host.copy()
+    o.rk4_step(yc, dt, 1)
+    t0 = time.perf_counter()
+    o.rk4_step(yc, dt, cpu_steps)
+    cpu_ms = (time.perf_counter() - t0) * 1e3 / cpu_steps
     return {"workload": f"ICON triangle shallow water, create_triangle_mesh({level})"
                         f"{' Hilbert-ordered' if hilbert else ''}, TC2, FP64",
             "cells": g.nc, "edges": g.ne, "ms_per_step": ms, "cell_steps_per_s": g.nc / (ms * 1e-3),
+            "cpu_baseline": {"ms_per_step": cpu_ms, "cell_steps_per_s": g.nc / (cpu_ms * 1e-3), "cores": threads,
+                             "kind": "port", "sample": f"{cpu_steps} RK4 steps, the oracle's C restatement with "
+                                                       "OpenMP (not Julia)"},
             "published_a100_ms_per_step_same_size": {7: 1.5, 8: 2.4, 9: 7.8}.get(level),
             "note": "the reference's A100 figure is on the ICON grid file of this size (R02B06/07/08 for "
                     "levels 7/8/9); this mesh is the icosahedral bisection of the same size"}

@@ -12,7 +12,8 @@ entities with each per-entity sum in the reference's order (numpy does not contr
     total_mass, total_energy   TRiSKShallowWater.jl:397-411 (K from kinetic_energy!, :184-189)
 
 It works on the tables of dmplex_b200.icon.icon_tables (1-based, (entity, k)), the same the
-library uploads. Its correctness is pinned by the reference's own ICON test assertions
+library uploads. ``IconOracleC`` runs the same restatement in C with OpenMP
+(oracle/icon_oracle.c), bit for bit the same. Its correctness is pinned by the reference's own ICON test assertions
 (test/finite_volumes.jl:112-166) in tests/test_icon.py, and by the ICON figures it publishes
 (docs/STATUS.md:40-55: TC2 errors on bisection and spring triangles, the Galewsky failure mode
 of ICON's kinetic-energy gradient) in tests/test_published.py.
@@ -95,3 +96,59 @@ class IconOracle:
         u, h = y[:self.ne], y[self.ne:]
         K = self.kinetic_energy(u, h)[3]
         return float(np.sum(self.t["cell_areas"] * h * (K + self.t["gravity"] * h / 2)))
+
+
+_INDEX = ("cell_edges", "edge_cells", "edge_vertices", "rbf_edges", "vertex_edges")
+_REAL = ("divergence", "bilinear", "edge_height", "gradient", "inverse_dual", "rbf", "edge_coriolis", "curl",
+         "cell_areas")
+
+
+class IconOracleC:
+    """tendency and rk4_step of IconOracle in C with OpenMP (oracle/icon_oracle.c), bit for bit
+    the same, on ``threads`` host threads."""
+
+    def __init__(self, tables: dict, threads: int = 1):
+        import ctypes as C
+        from oracle.oracle import _lib
+
+        class Tables(C.Structure):
+            _fields_ = ([(n, C.c_int64) for n in ("nc", "ne", "nv")] + [("vw", C.c_int32), ("reserved", C.c_int32),
+                                                                       ("gravity", C.c_double)]
+                        + [(n, C.c_void_p) for n in _INDEX + _REAL + ("divergence_damping",)])
+        if _lib.icon_oracle_tables_size() != C.sizeof(Tables):
+            raise RuntimeError("oracle struct layout mismatch")
+        t = tables
+        s = Tables()
+        s.nc, s.ne, s.nv, s.vw, s.gravity = t["nc"], t["ne"], t["nv"], t["vw"], t["gravity"]
+        self._keep = []
+        for name in _INDEX + _REAL:
+            a = np.ascontiguousarray(t[name], dtype=np.int64 if name in _INDEX else np.float64)
+            self._keep.append(a)
+            setattr(s, name, a.ctypes.data)
+        nu = t.get("divergence_damping")
+        if nu is not None and len(nu):
+            a = np.ascontiguousarray(nu, dtype=np.float64)
+            self._keep.append(a)
+            s.divergence_damping = a.ctypes.data
+        self._s, self._lib, self.threads = s, _lib, int(threads)
+        self.ne, self.nc = t["ne"], t["nc"]
+        self.cell_areas = np.ascontiguousarray(t["cell_areas"], dtype=np.float64)
+
+    def tendency(self, y):
+        import ctypes as C
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        dy = np.empty_like(y)
+        self._lib.icon_oracle_set_threads(self.threads)
+        self._lib.icon_oracle_tendency(C.byref(self._s), y.ctypes.data, dy.ctypes.data)
+        return dy
+
+    def rk4_step(self, y, dt, nsteps=1):
+        import ctypes as C
+        if y.dtype != np.float64 or not y.flags.c_contiguous:
+            raise ValueError("y must be a contiguous float64 array")
+        self._lib.icon_oracle_set_threads(self.threads)
+        self._lib.icon_oracle_rk4_step(C.byref(self._s), y.ctypes.data, float(dt), int(nsteps))
+        return y
+
+    def total_mass(self, y):
+        return float(np.sum(self.cell_areas * y[self.ne:]))

@@ -39,7 +39,8 @@ def build() -> None:
 
 
 def _load():
-    sources = [os.path.join(HERE, f) for f in ("trisk_oracle.c", "trisk_oracle.h", "mpas_oracle.c", "mpas_oracle.h")]
+    sources = [os.path.join(HERE, f) for f in ("trisk_oracle.c", "trisk_oracle.h", "mpas_oracle.c", "mpas_oracle.h",
+                                               "icon_oracle.c", "icon_oracle.h")]
     if not os.path.exists(LIB_PATH) or any(os.path.getmtime(f) > os.path.getmtime(LIB_PATH)
                                            for f in sources if os.path.exists(f)):
         build()
@@ -65,6 +66,10 @@ def _load():
         ("mpas_oracle_tables_size", C.c_int, []),
         ("mpas_oracle_fields_size", C.c_int, []),
         ("mpas_oracle_slow_tendencies", None, [p, p, d]),
+        ("icon_oracle_set_threads", None, [C.c_int]),
+        ("icon_oracle_tables_size", C.c_int, []),
+        ("icon_oracle_tendency", None, [p, p, p]),
+        ("icon_oracle_rk4_step", None, [p, p, d, C.c_int64]),
     ]:
         fn = getattr(lib, name)
         fn.restype, fn.argtypes = res, args

@@ -128,3 +128,19 @@ def test_icon_tc2_gpu(require_gpu):
     assert np.sqrt(np.sum(g.cell_areas * dh ** 2) / (4 * np.pi)) < 1e-4
     with pytest.raises(ValueError):
         icon.ICONShallowWater(g, divergence_damping=np.ones(3))
+
+
+@pytest.mark.parametrize("gradient,nu", [("icon", 0.0), ("centered", 1e-4)])
+def test_c_oracle_matches_numpy_oracle(gradient, nu):
+    """oracle/icon_oracle.c (the CPU baseline) is the numpy restatement bit for bit."""
+    from oracle.icon_oracle import IconOracleC
+    g = tri_grid(4, 1.2)
+    t = icon.icon_tables(g, kinetic_gradient=gradient)
+    t["divergence_damping"] = np.full(g.ne, nu) if nu else np.zeros(0)
+    rng = np.random.default_rng(5)
+    y = tc2_state(g) + 1e-3 * rng.standard_normal(g.ne + g.nc)
+    ref = IconOracle(t)
+    for threads in (1, 4):
+        c = IconOracleC(t, threads=threads)
+        assert np.array_equal(c.tendency(y), ref.tendency(y))
+        assert np.array_equal(c.rk4_step(y.copy(), 0.01, 3), ref.rk4_step(y.copy(), 0.01, 3))

@@ -134,8 +134,8 @@ def _asymmetry(g):
 
 def _icon_tc2_l2(g):
     from dmplex_b200 import icon
-    from oracle.icon_oracle import IconOracle
-    o = IconOracle(icon.icon_tables(g))
+    from oracle.icon_oracle import IconOracleC
+    o = IconOracleC(icon.icon_tables(g), threads=os.cpu_count() or 1)
     u0 = 0.2
     x = g.edge_points
     u = u0 * np.einsum("ij,ij->i", np.stack([-x[:, 1], x[:, 0], np.zeros(len(x))], axis=1), g.edge_normals)
@@ -177,14 +177,14 @@ def test_icon_galewsky_on_bisection_triangles():
     gradient and stays stable with the centered one (:44-50)."""
     from dmplex_b200 import icon, run
     from dmplex_b200.cases import Galewsky
-    from oracle.icon_oracle import IconOracle
+    from oracle.icon_oracle import IconOracleC
     case = Galewsky(3.0)
     g = _triangles("plain", 5)
     dt, n = case.steps(g)
     for gradient, survives in (("icon", False), ("centered", True)):
         t = icon.icon_tables(g, gravity=case.gravity, kinetic_gradient=gradient)
         t["divergence_damping"] = case.icon_damping(g, dt)
-        o = IconOracle(t)
+        o = IconOracleC(t, threads=os.cpu_count() or 1)
         y = run.edge_and_cell_state(g, case)
         with np.errstate(all="ignore"):
             o.rk4_step(y, dt, n)
