@@ -239,10 +239,8 @@ def run_galewsky_leg(local_rank, level=8, days=6.0, schemes=("trisk", "gassmann"
     largest relative vorticity. The reference: 28 s (TRiSK), 58 s (gassmann) and 43 s
     (gassmann_mean) for hexagon 8 over 6 days on 4 x A100, and on hexagon 7 |zeta| <= 1.6e-4 1/s
     and +0.4 % enstrophy for TRiSK, 5e-4 and +51 % for gassmann (docs/STATUS.md:29-34)."""
-    import torch
     import dmplex_b200 as d
     from dmplex_b200.cases import OMEGA, Galewsky
-    from dmplex_b200.vtkhdf import cell_vorticity
     case = Galewsky(days)
     g = d.TRiSKGrid(d.create_hexagon_mesh(level))
     dt, nsteps = case.steps(g)
@@ -254,53 +252,65 @@ def run_galewsky_leg(local_rank, level=8, days=6.0, schemes=("trisk", "gassmann"
                          "gassmann_mean": "hexagon 7: |zeta| <= 1.6e-4 1/s, potential enstrophy +0.4 %",
                          "gassmann": "hexagon 7: |zeta| 5e-4 1/s, potential enstrophy +51 %"}
     for pv in schemes:
-        m = d.TRiSKShallowWater(g, gravity=case.gravity, omega=1.0, pv_flux=pv, device=local_rank)
-        y = torch.from_numpy(d.initial_state(m, case.velocity, case.height)).to(dev)
-        warm = y.clone()
-        d.rk4_step(warm, dt, d.tendency, d.RK4Cache(warm), m, nsteps=2)
-        mass0, energy0, ens0 = d.total_mass(m, y), d.total_energy(m, y), d.potential_enstrophy(m, y)
-        torch.cuda.synchronize(local_rank)
-        t0 = time.perf_counter()
-        d.rk4_step(y, dt, d.tendency, d.RK4Cache(y), m, nsteps=nsteps)
-        torch.cuda.synchronize(local_rank)
-        wall = time.perf_counter() - t0
-        zeta = OMEGA * cell_vorticity(g, y.cpu().numpy())
-        out[pv] = {"seconds": wall, "ms_per_step": 1e3 * wall / nsteps,
-                   "mass_change": (d.total_mass(m, y) - mass0) / mass0,
-                   "energy_change": (d.total_energy(m, y) - energy0) / energy0,
-                   "enstrophy_change": (d.potential_enstrophy(m, y) - ens0) / ens0,
-                   "max_abs_vorticity_per_s": float(np.abs(zeta).max()),
-                   "published_4xa100_seconds": published.get(pv),
-                   "published_outcome": published_outcome.get(pv)}
-        del m
+        out[pv] = optional_leg(_galewsky_trisk, d, g, case, pv, dt, nsteps, dev, local_rank,
+                               published.get(pv), published_outcome.get(pv))
     if icon:
-        # ICON triangles of the same level (plain bisection, Hilbert-ordered) with ICON's
-        # divergence damping; the centered kinetic-energy gradient, which the reference
-        # prescribes for irregular triangles (ICON's own form blows up on bisection meshes)
-        from dmplex_b200.icon import ICONShallowWater
-        gt = d.TRiSKGrid(d.hilbert_order(d.create_triangle_mesh(level)))
-        dti, ni = case.steps(gt)
-        m = ICONShallowWater(gt, gravity=case.gravity, divergence_damping=case.icon_damping(gt, dti),
-                             kinetic_gradient="centered", device=local_rank)
-        u = np.einsum("ij,ij->i", case.velocity(gt.edge_points), gt.edge_normals)
-        y = torch.from_numpy(np.concatenate([u, case.height(gt.centers)])).to(dev)
-        warm = y.clone()
-        m.rk4_step(warm, dti, 2)
-        mass0 = m.total_mass(y.cpu().numpy())
-        torch.cuda.synchronize(local_rank)
-        t0 = time.perf_counter()
-        m.rk4_step(y, dti, ni)
-        torch.cuda.synchronize(local_rank)
-        wall = time.perf_counter() - t0
-        yh = y.cpu().numpy()
-        out["icon_centered"] = {"cells": gt.nc, "steps": ni, "seconds": wall, "ms_per_step": 1e3 * wall / ni,
-                                "mass_change": (m.total_mass(yh) - mass0) / mass0, "finite": bool(np.isfinite(yh).all()),
-                                "max_abs_vorticity_per_s": float(np.abs(OMEGA * cell_vorticity(gt, yh)).max()),
-                                "published": "ICON model on the ICON grid R02B07 (the same number of triangles), "
-                                             "4 x A100: 40406 steps in 60 s, |zeta| <= 1.7e-4 1/s "
-                                             "(docs/STATUS.md:104-105)"}
-        del m
+        out["icon_centered"] = optional_leg(_galewsky_icon, d, case, level, dev, local_rank)
     return out
+
+
+def _galewsky_trisk(d, g, case, pv, dt, nsteps, dev, local_rank, published_seconds, published_outcome):
+    """One PV flux of the Galewsky leg (its own error, if any, stays in its own entry)."""
+    import torch
+    from dmplex_b200.cases import OMEGA
+    from dmplex_b200.vtkhdf import cell_vorticity
+    m = d.TRiSKShallowWater(g, gravity=case.gravity, omega=1.0, pv_flux=pv, device=local_rank)
+    y = torch.from_numpy(d.initial_state(m, case.velocity, case.height)).to(dev)
+    warm = y.clone()
+    d.rk4_step(warm, dt, d.tendency, d.RK4Cache(warm), m, nsteps=2)
+    mass0, energy0, ens0 = d.total_mass(m, y), d.total_energy(m, y), d.potential_enstrophy(m, y)
+    torch.cuda.synchronize(local_rank)
+    t0 = time.perf_counter()
+    d.rk4_step(y, dt, d.tendency, d.RK4Cache(y), m, nsteps=nsteps)
+    torch.cuda.synchronize(local_rank)
+    wall = time.perf_counter() - t0
+    zeta = OMEGA * cell_vorticity(g, y.cpu().numpy())
+    return {"seconds": wall, "ms_per_step": 1e3 * wall / nsteps,
+            "mass_change": (d.total_mass(m, y) - mass0) / mass0,
+            "energy_change": (d.total_energy(m, y) - energy0) / energy0,
+            "enstrophy_change": (d.potential_enstrophy(m, y) - ens0) / ens0,
+            "max_abs_vorticity_per_s": float(np.abs(zeta).max()),
+            "published_4xa100_seconds": published_seconds, "published_outcome": published_outcome}
+
+
+def _galewsky_icon(d, case, level, dev, local_rank):
+    """ICON triangles of the same level (plain bisection, Hilbert-ordered) with ICON's
+    divergence damping and the centered kinetic-energy gradient, which the reference prescribes
+    for irregular triangles (ICON's own form blows up on bisection meshes)."""
+    import torch
+    from dmplex_b200.cases import OMEGA
+    from dmplex_b200.vtkhdf import cell_vorticity
+    from dmplex_b200.icon import ICONShallowWater
+    gt = d.TRiSKGrid(d.hilbert_order(d.create_triangle_mesh(level)))
+    dti, ni = case.steps(gt)
+    m = ICONShallowWater(gt, gravity=case.gravity, divergence_damping=case.icon_damping(gt, dti),
+                         kinetic_gradient="centered", device=local_rank)
+    u = np.einsum("ij,ij->i", case.velocity(gt.edge_points), gt.edge_normals)
+    y = torch.from_numpy(np.concatenate([u, case.height(gt.centers)])).to(dev)
+    warm = y.clone()
+    m.rk4_step(warm, dti, 2)
+    mass0 = m.total_mass(y.cpu().numpy())
+    torch.cuda.synchronize(local_rank)
+    t0 = time.perf_counter()
+    m.rk4_step(y, dti, ni)
+    torch.cuda.synchronize(local_rank)
+    wall = time.perf_counter() - t0
+    yh = y.cpu().numpy()
+    return {"cells": gt.nc, "steps": ni, "seconds": wall, "ms_per_step": 1e3 * wall / ni,
+            "mass_change": (m.total_mass(yh) - mass0) / mass0, "finite": bool(np.isfinite(yh).all()),
+            "max_abs_vorticity_per_s": float(np.abs(OMEGA * cell_vorticity(gt, yh)).max()),
+            "published": "ICON model on the ICON grid R02B07 (the same number of triangles), "
+                         "4 x A100: 40406 steps in 60 s, |zeta| <= 1.7e-4 1/s (docs/STATUS.md:104-105)"}
 
 
 def run_mpas_leg(local_rank, level=7, nlev=30, calls=50, cpu_level=None, hilbert=True, lpt=0, cpu_calls=3):
