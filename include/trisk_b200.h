@@ -450,7 +450,7 @@ int trisk_closure_stream(TriskClosure* closure, void** stream);
  * CUDA.jl's, or code running while a stream is being captured into a CUDA graph).
  *
  * *out = sum_i a[i] * b[i] over caller-owned device vectors (with a = the cell areas and
- * b = the heights this is total_mass, TRiSKShallowWater.jl:397). a, b and out must be
+ * b = the heights this is the total mass, dot(areas, h)). a, b and out must be
  * device pointers on one device; the work is enqueued on `stream` (a cudaStream_t, NULL for
  * the default stream) and not waited for. The call makes no cudaMalloc, cudaFree or other
  * allocating call: its scratch is a static 64 KiB device array that every GPU loading the

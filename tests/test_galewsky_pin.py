@@ -3,8 +3,9 @@
 expected vortex roll-up (|zeta| <= 1.6e-4 1/s, potential enstrophy +0.4 %), :gassmann |zeta|
 5e-4 and +51 % enstrophy" (docs/STATUS.md:29-31). The CPU oracle on the same set-up
 (dmplex_b200.cases.Galewsky) gives 1.555e-4 / +0.37 %, 1.591e-4 / +0.39 % and 5.16e-4 /
-+50.6 %; the library's model equals the oracle bit for bit. About two and a half minutes each
-on 8 host threads, so it runs only with TRISK_LONG_TESTS=1."""
++50.6 %; the library's model equals the oracle bit for bit. The oracle run takes about two and a
+half minutes per scheme on 8 host threads, so it runs only with TRISK_LONG_TESTS=1; the same
+outcome through the CUDA path is a default GPU test."""
 import os
 
 import numpy as np
@@ -41,3 +42,29 @@ def test_galewsky_hexagon7_matches_the_published_outcome(pv_flux, zeta_range, en
     assert abs(o.total_mass(y) - m0) / m0 < 1e-12 and abs(o.total_energy(y) - e0) / e0 < 1e-9
     assert zeta_range[0] < zeta <= zeta_range[1]
     assert enstrophy_range[0] < (o.potential_enstrophy(y) - z0) / z0 < enstrophy_range[1]
+
+
+@pytest.fixture(scope="module")
+def hexagon7_grid():
+    return d.TRiSKGrid(d.create_hexagon_mesh(7))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("pv_flux,zeta_range,enstrophy_range", PUBLISHED)
+def test_galewsky_hexagon7_on_the_gpu_matches_the_published_outcome(require_gpu, hexagon7_grid, pv_flux, zeta_range,
+                                                                    enstrophy_range):
+    """The same published outcome through the library's CUDA path (TRiSKShallowWater, rk4_step
+    as one CUDA-graph call of 7685 steps, the diagnostics entry points): about a second per
+    scheme on a B200."""
+    g = hexagon7_grid
+    case = Galewsky(6.0)
+    dt, n = case.steps(g)
+    m = d.TRiSKShallowWater(g, gravity=case.gravity, omega=1.0, pv_flux=pv_flux, device=0)
+    y = run.edge_and_cell_state(g, case)
+    m0, e0, z0 = d.total_mass(m, y), d.total_energy(m, y), d.potential_enstrophy(m, y)
+    d.rk4_step(y, dt, d.tendency, d.RK4Cache(y), m, nsteps=n)
+    assert np.isfinite(y).all()
+    zeta = np.abs(OMEGA * cell_vorticity(g, y)).max()
+    assert abs(d.total_mass(m, y) - m0) / m0 < 1e-12 and abs(d.total_energy(m, y) - e0) / e0 < 1e-9
+    assert zeta_range[0] < zeta <= zeta_range[1]
+    assert enstrophy_range[0] < (d.potential_enstrophy(m, y) - z0) / z0 < enstrophy_range[1]
