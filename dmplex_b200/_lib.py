@@ -167,6 +167,7 @@ def _load():
         "trisk_closure_adam": (C.c_int, [_p, C.c_float, C.c_float, C.c_float, C.c_float]),
         "trisk_closure_synchronize": (C.c_int, [_p]),
         "trisk_closure_stream": (C.c_int, [_p, C.POINTER(_p)]),
+        "trisk_closure_expire_wait_once": (C.c_int, [_p, _i64]),
         "trisk_ensemble_create": (C.c_int, [_p, _p, _p, _p, _i32, C.POINTER(_p)]),
         "trisk_ensemble_create_precision": (C.c_int, [_p, _p, _p, _p, _i32, _i32, C.POINTER(_p)]),
         "trisk_ensemble_set_block": (C.c_int, [_p, _p]),

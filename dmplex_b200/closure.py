@@ -85,6 +85,12 @@ class ClosureMLP:
                                           C.byref(loss)))
         return g, loss.value
 
+    def expire_wait_once(self, tile: int) -> None:
+        """Test of the bounded tensor-core wait: the next forward call leaves tile `tile`'s first
+        tensor-core operation un-issued, so it returns TRISK_ERR_TIMEOUT (TriskError status 5)
+        after half a second; the closure stays usable."""
+        check(lib.trisk_closure_expire_wait_once(self._h, int(tile)))
+
     def train_step(self, X, T, lr: float, beta1: float = 0.9, beta2: float = 0.999, eps: float = 1e-8) -> float:
         """Gradients on the batch, then one Adam step; returns the batch loss."""
         _check_tensor(X, "torch.bfloat16", NIN)

@@ -6,15 +6,21 @@
 // 24 normalized features of an edge and returns two corrections (to the edge mass flux and
 // to the edge momentum tendency).
 //
-// One CTA = 4 warps = 128 threads; a tile = 128 edges, thread t owns row t. Shared-memory
-// operands use the no-swizzle "core matrix" layout (8 rows x 16 bytes, rows 16 bytes
-// apart). A buffer tiled as
+// A CTA = 4 warps = 128 threads; a tile = 128 edges, thread t owns row t (TMEM lane t).
+// Shared-memory operands use the no-swizzle "core matrix" layout (8 rows x 16 bytes, rows
+// 16 bytes apart). A buffer tiled as
 //     offset(r, c) = (c / 8) * CHUNK + (r / 8) * 128 + (r % 8) * 16 + (c % 8) * 2
 // is a K-major operand with rows r along M/N and columns c along K (SBO = 128, LBO =
 // CHUNK), and the same bytes are an MN-major operand with c along M/N and r along K
 // (SBO = CHUNK, LBO = 128). Forward GEMMs use the first view, backward GEMMs the second,
 // so no operand is ever transposed in memory.
 //
+// Inference (k_mlp_forward): a persistent grid, several CTAs per SM, 64 TMEM columns each.
+//   Z1 = X W1^T   M=128 N=64 K=32  (A = XH[:, 0:32], X padded with zeros; B = W1 K-major)
+//   H1 = gelu(Z1 + b1) -> bf16 -> XH[:, 0:64]  (over X: MMA 1 has finished reading it)
+//   Z2 = H1 W2^T  M=128 N=64 K=64  (same TMEM columns: Z1 has been read)
+//   Y  = bf16(gelu(Z2 + b2)) W3^T + b3 on the CUDA cores (N = 2)
+// Training (k_mlp_train): forward, backward and weight gradients of one tile per step:
 //   forward    Z1 = X W1^T       M=128 N=64 K=32   (A = HX[:, 64:96] K-major, B = W1 K-major)
 //              H1 = gelu(Z1 + b1) -> bf16 -> HX[:, 0:64]
 //              Z2 = H1 W2^T      M=128 N=64 K=64   (A = HX[:, 0:64], B = W2 K-major)
@@ -24,9 +30,16 @@
 //              dH1 = G * gelu'(Z1)                             -> DD[:, 64:128]
 //              DW += DD^T [H1 | X]   M=128 N=96 K=128 (A = DD MN-major, B = HX MN-major):
 //                   rows 0..63 x cols 0..63 = dW2, rows 64..127 x cols 64..87 = dW1
+//   Tensor memory: Z1 at 0, Z2 (then G) at 64, DW at 128..224 (256 columns, two CTAs per SM).
 //
-// Tensor memory: Z1 at 0, Z2 (then G) at 64, DW at 128..224 (training: 256 columns, two
-// CTAs per SM; inference: 128 columns, four CTAs per SM).
+// GELU is the tanh form of Hendrycks and Gimpel (2016), gelu(x) = x/2 (1 + tanh(sqrt(2/pi)
+// (x + 0.044715 x^3))), with tanh on the special-function unit (tanh.approx.f32); it is the
+// network's activation in training and inference alike, and the oracle's.
+//
+// Every tensor-core wait is bounded in time. A wait that gives up marks the CTA; at the next
+// CTA-wide barrier every thread sees the mark and the CTA leaves its tile loop, waits (again
+// bounded) for a tensor-core operation it committed and has not seen finish, frees its tensor
+// memory and reports TRISK_ERR_TIMEOUT through a status word the host reads.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -48,18 +61,16 @@ constexpr int W1_BYTES = 4 * W_CHUNK;    // 64 x 32
 constexpr int W2_BYTES = 8 * W_CHUNK;    // 64 x 64
 // + 64 B (mbarrier, TMEM address) + H2 (128 x 64 BF16) and dY (128 x 2 FP32) for training
 constexpr int SMEM_BYTES = HX_BYTES + DD_BYTES + W1_BYTES + W2_BYTES + 64 + TILE * NH * 2 + TILE * NOUT * 4;
-// Inference needs HX, W1, W2 and the barrier (36 KB) and 128 TMEM columns (Z1, Z2), so four
-// CTAs share an SM's 512 columns; its request is padded to 53 KB so that no fifth CTA, which
-// would wait in tcgen05.alloc for a whole CTA lifetime, becomes resident.
-constexpr int FWD_SMEM_BYTES = 53 * 1024;
-static_assert(HX_BYTES + W1_BYTES + W2_BYTES + 64 <= FWD_SMEM_BYTES, "inference shared memory");
-template <int TRAIN>
-struct MlpShape {
-  static constexpr uint32_t tmem_cols = TRAIN ? 256 : 128;
-  static constexpr int smem = TRAIN ? SMEM_BYTES : FWD_SMEM_BYTES;
-  static constexpr int ctas_per_sm = TRAIN ? 2 : 4;
-};
-constexpr int MBAR_SPIN_LIMIT = 1 << 20;
+constexpr uint32_t TRAIN_TMEM_COLS = 256;  // two CTAs per SM share its 512 columns
+// Inference: XH (X, then H1: 8 chunks), W1, W2 and the barrier, 64 TMEM columns; at most
+// seven CTAs fit an SM's shared memory, and seven (even eight) x 64 columns fit its TMEM, so
+// no CTA ever waits in tcgen05.alloc.
+constexpr int XH_BYTES = 8 * HX_CHUNK;
+constexpr int FWD_SMEM_BYTES = XH_BYTES + W1_BYTES + W2_BYTES + 64;
+constexpr uint32_t FWD_TMEM_COLS = 64;
+static_assert(FWD_SMEM_BYTES * 7 <= 220 * 1024, "seven inference CTAs per SM");
+// A bounded tensor-core wait gives up after this long (the operations take microseconds).
+constexpr long long MBAR_WAIT_NS = 500000000LL;
 
 // FP32 master parameters and their BF16 tensor-core copies (one contiguous block each).
 struct Params {
@@ -104,9 +115,17 @@ __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::aft
 __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
-// Waits for the mbarrier phase with a bounded number of tries; false after the bound.
+__device__ __forceinline__ long long global_ns() {
+  long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Waits for the completion of the mbarrier phase of parity `phase`, for at most MBAR_WAIT_NS;
+// false if it gave up.
 __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase) {
-  for (int i = 0; i < MBAR_SPIN_LIMIT; ++i) {
+  long long start = 0;
+  for (uint32_t i = 0;; ++i) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
@@ -115,8 +134,12 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase) {
         : "r"(mbar), "r"(phase)
         : "memory");
     if (done) return true;
+    if ((i & 255) == 0) {
+      const long long now = global_ns();
+      if (i == 0) start = now;
+      else if (now - start > MBAR_WAIT_NS) return false;
+    }
   }
-  return false;
 }
 
 // 16 consecutive FP32 columns of this thread's TMEM lane
@@ -132,9 +155,25 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
   for (int k = 0; k < 16; ++k) v[k] = __uint_as_float(r[k]);
 }
 
-__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+__device__ __forceinline__ float tanh_approx(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+// gelu(x) = x/2 (1 + tanh(u)), u = sqrt(2/pi) (x + 0.044715 x^3) (Hendrycks and Gimpel 2016)
+constexpr float GELU_C0 = 0.7978845608028654f;   // sqrt(2/pi)
+constexpr float GELU_C1 = 0.035677408136300125f;  // 0.044715 sqrt(2/pi)
+__device__ __forceinline__ float gelu(float x) {
+  const float u = x * fmaf(GELU_C1, x * x, GELU_C0);
+  const float h = 0.5f * x;
+  return fmaf(h, tanh_approx(u), h);
+}
+// d gelu / dx = (1 + t)/2 + x/2 (1 - t^2) du/dx,  du/dx = sqrt(2/pi) (1 + 3 * 0.044715 x^2)
 __device__ __forceinline__ float gelu_grad(float x) {
-  return 0.5f * (1.0f + erff(x * 0.70710678118654752f)) + x * 0.39894228040143268f * expf(-0.5f * x * x);
+  const float x2 = x * x;
+  const float t = tanh_approx(x * fmaf(GELU_C1, x2, GELU_C0));
+  const float du = fmaf(3.0f * GELU_C1, x2, GELU_C0);
+  return fmaf(0.5f * x * fmaf(-t, t, 1.0f), du, fmaf(0.5f, t, 0.5f));
 }
 __device__ __forceinline__ float bf(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
 
@@ -144,58 +183,24 @@ __device__ __forceinline__ uint32_t tile_off(int r, int c, int chunk) {
 
 // 8 consecutive columns (c0 multiple of 8) of row r as one 16-byte store
 __device__ __forceinline__ void store8(unsigned char* base, int r, int c0, int chunk, const float* v) {
-  __align__(16) __nv_bfloat16 t[8];
-#pragma unroll
-  for (int k = 0; k < 8; ++k) t[k] = __float2bfloat16_rn(v[k]);
-  *reinterpret_cast<uint4*>(base + tile_off(r, c0, chunk)) = *reinterpret_cast<const uint4*>(t);
+  uint4 q;
+  __nv_bfloat162 p0 = __floats2bfloat162_rn(v[0], v[1]), p1 = __floats2bfloat162_rn(v[2], v[3]),
+                 p2 = __floats2bfloat162_rn(v[4], v[5]), p3 = __floats2bfloat162_rn(v[6], v[7]);
+  q.x = *reinterpret_cast<uint32_t*>(&p0);
+  q.y = *reinterpret_cast<uint32_t*>(&p1);
+  q.z = *reinterpret_cast<uint32_t*>(&p2);
+  q.w = *reinterpret_cast<uint32_t*>(&p3);
+  *reinterpret_cast<uint4*>(base + tile_off(r, c0, chunk)) = q;
 }
 
 struct Status {
   int error;  // 1: a bounded tensor-core wait gave up
 };
-// Forward (TRAIN = 0) writes Y; training (TRAIN = 1) also accumulates the gradients of the
-// mean squared error (1/n) sum_rows sum_k (y_k - t_k)^2 into grad (FP32, zeroed by the
-// caller) and the squared-error sum into *loss. Column 88 of HX (the first padding column
-// of the input chunk) holds 1 for valid rows, so the weight-gradient MMA also returns the
-// bias gradients: DW[j][88] = sum_rows dH2[:, j] = db2[j], DW[64 + i][88] = db1[i]. W1's
-// padded input columns are 0, so the forward product ignores it.
-constexpr int ONES_COL = 64 + NIN;
 
-template <int TRAIN>
-__global__ void __launch_bounds__(TILE, MlpShape<TRAIN>::ctas_per_sm) k_mlp(const __nv_bfloat16* __restrict__ X, int64_t n,
-                                                  const ParamsBF16* __restrict__ wbf, const Params* __restrict__ p,
-                                                  const float* __restrict__ target, float* __restrict__ Y,
-                                                  Params* __restrict__ grad, float* loss, float inv_n,
-                                                  Status* status) {
-  extern __shared__ __align__(1024) unsigned char smem[];
-  constexpr uint32_t TMEM_COLS = MlpShape<TRAIN>::tmem_cols;
-  unsigned char* HX = smem;
-  unsigned char* DD = smem + HX_BYTES;  // training only
-  unsigned char* W1s = DD + (TRAIN ? DD_BYTES : 0);
-  unsigned char* W2s = W1s + W1_BYTES;
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(W2s + W2_BYTES);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(W2s + W2_BYTES + 16);
-  __nv_bfloat16* sH2 = reinterpret_cast<__nv_bfloat16*>(W2s + W2_BYTES + 64);  // 128 x 64 (training)
-  float* sDY = reinterpret_cast<float*>(W2s + W2_BYTES + 64 + TILE * NH * 2);   // 128 x 2 (training)
-  __shared__ float sb1[NH], sb2[NH], sw3[NOUT * NH], sb3[NOUT];
-  __shared__ int s_abort;
-
-  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
-  const int64_t ntiles = (n + TILE - 1) / TILE;
-  if ((int64_t)blockIdx.x >= ntiles) return;
-
-  if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                 "r"(TMEM_COLS)
-                 : "memory");
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-  }
-  if (t == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar)) : "memory");
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    s_abort = 0;
-  }
-  // weights: W1 (64 x 32, inputs padded with 0) and W2 (64 x 64) as K-major B operands
+// W1 (64 x 32, inputs padded with 0) and W2 (64 x 64) as K-major B operands; biases and W3
+__device__ __forceinline__ void load_weights(unsigned char* W1s, unsigned char* W2s, float* sb1, float* sb2,
+                                             float* sw3, float* sb3, const ParamsBF16* __restrict__ wbf,
+                                             const Params* __restrict__ p, int t) {
   for (int idx = t; idx < NH * 4; idx += TILE) {
     const int r = idx >> 2, c0 = (idx & 3) * 8;
     *reinterpret_cast<uint4*>(W1s + tile_off(r, c0, W_CHUNK)) =
@@ -212,26 +217,227 @@ __global__ void __launch_bounds__(TILE, MlpShape<TRAIN>::ctas_per_sm) k_mlp(cons
   }
   for (int idx = t; idx < NOUT * NH; idx += TILE) sw3[idx] = __bfloat162float(wbf->W3[idx]);
   if (t < NOUT) sb3[t] = p->b3[t];
+}
+
+// The bounded tensor-core waits of a CTA. wait() records a give-up in the CTA's shared abort
+// word; every thread reads that word only right after a CTA-wide barrier, so all threads
+// leave the tile loop together. `last` and `issued` (the parity of the last wait and whether
+// an operation was committed to it) are the same in every thread.
+struct MmaWaits {
+  uint32_t mb;
+  volatile int* abort;
+  uint32_t phase = 0, last = 0;
+  bool issued = false;
+  __device__ MmaWaits(uint32_t mbar, int* abort_word) : mb(mbar), abort(abort_word) {}
+  __device__ __forceinline__ void wait(bool committed) {
+    last = phase;
+    if (!mbar_wait(mb, phase)) *abort = 1;
+    phase ^= 1;
+    issued = committed;
+    fence_after();
+  }
+  __device__ __forceinline__ bool aborted() const { return *abort != 0; }
+  // after an abort: wait (bounded) for the committed operation whose completion was not seen,
+  // so that the tensor memory it writes is no longer in use when it is freed
+  __device__ __forceinline__ void drain() {
+    if (*abort && issued) mbar_wait(mb, last);
+  }
+};
+
+// Inference: Y (n x 2) = MLP(X) over a persistent grid. expire_tile >= 0 names a tile whose
+// first tensor-core operation is not issued, so its bounded wait runs out (the test of the
+// give-up path); -1 in normal use.
+__global__ void __launch_bounds__(TILE) k_mlp_forward(const __nv_bfloat16* __restrict__ X, int64_t n,
+                                                      const ParamsBF16* __restrict__ wbf,
+                                                      const Params* __restrict__ p, float* __restrict__ Y,
+                                                      Status* status, int64_t expire_tile) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  unsigned char* XH = smem;  // X (chunks 0..3), then H1 (chunks 0..7)
+  unsigned char* W1s = smem + XH_BYTES;
+  unsigned char* W2s = W1s + W1_BYTES;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(W2s + W2_BYTES);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(W2s + W2_BYTES + 16);
+  __shared__ __align__(16) float sb1[NH], sb2[NH], sw3[NOUT * NH];
+  __shared__ float sb3[NOUT];
+  __shared__ int s_abort;
+
+  const int t = threadIdx.x, warp = t >> 5;
+  const int64_t ntiles = (n + TILE - 1) / TILE;
+  if ((int64_t)blockIdx.x >= ntiles) return;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(FWD_TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (t == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    s_abort = 0;
+  }
+  load_weights(W1s, W2s, sb1, sb2, sw3, sb3, wbf, p, t);
   fence_async_smem();
   fence_before();
   __syncthreads();
   fence_after();
   const uint32_t tmem = *tmem_slot;
   const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
-  const uint32_t mb = smem_u32(mbar);
+  const uint32_t xh = smem_u32(XH), w1 = smem_u32(W1s), w2 = smem_u32(W2s);
+  const uint32_t ID = idesc_bf16(128, 64, 0, 0);
+  MmaWaits waits(smem_u32(mbar), &s_abort);
+  auto sync_for_mma = [&]() {  // shared-memory writes -> visible to the tensor core
+    fence_async_smem();
+    fence_before();
+    __syncthreads();
+    fence_after();
+  };
+  const float4* b1v = reinterpret_cast<const float4*>(sb1);
+  const float4* b2v = reinterpret_cast<const float4*>(sb2);
+  const float4* w3a = reinterpret_cast<const float4*>(sw3);
+  const float4* w3b = reinterpret_cast<const float4*>(sw3 + NH);
+
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int64_t row = tile * TILE + t;
+    const bool valid = row < n;
+    {  // X -> XH chunks 0..2 (24 features), chunk 3 = 0 (W1's padding columns are 0 as well)
+      uint4 q[3] = {make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0)};
+      if (valid) {
+        const uint4* src = reinterpret_cast<const uint4*>(X + row * NIN);
+        q[0] = src[0];
+        q[1] = src[1];
+        q[2] = src[2];
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) *reinterpret_cast<uint4*>(XH + tile_off(t, 8 * c, HX_CHUNK)) = q[c];
+      *reinterpret_cast<uint4*>(XH + tile_off(t, 24, HX_CHUNK)) = make_uint4(0, 0, 0, 0);
+    }
+    sync_for_mma();
+    if (waits.aborted()) break;
+    const bool issue = tile != expire_tile;
+    if (t == 0 && issue) {  // Z1 = X W1^T
+#pragma unroll
+      for (int kk = 0; kk < 2; ++kk)
+        mma_bf16(tmem, sdesc(xh + 2 * kk * HX_CHUNK, HX_CHUNK, 128), sdesc(w1 + 2 * kk * W_CHUNK, W_CHUNK, 128), ID,
+                 kk);
+      mma_commit(waits.mb);
+    }
+    waits.wait(issue);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {  // H1 = gelu(Z1 + b1) -> XH chunks 0..7 (MMA 1 has read X)
+      float v[16];
+      tmem_ld16(lane_base + 16 * c, v);
+#pragma unroll
+      for (int k4 = 0; k4 < 4; ++k4) {
+        const float4 b = b1v[4 * c + k4];
+        v[4 * k4 + 0] = gelu(v[4 * k4 + 0] + b.x);
+        v[4 * k4 + 1] = gelu(v[4 * k4 + 1] + b.y);
+        v[4 * k4 + 2] = gelu(v[4 * k4 + 2] + b.z);
+        v[4 * k4 + 3] = gelu(v[4 * k4 + 3] + b.w);
+      }
+      store8(XH, t, 16 * c, HX_CHUNK, v);
+      store8(XH, t, 16 * c + 8, HX_CHUNK, v + 8);
+    }
+    sync_for_mma();  // also: every thread has read Z1, which Z2 overwrites
+    if (waits.aborted()) break;
+    if (t == 0) {  // Z2 = H1 W2^T
+#pragma unroll
+      for (int kk = 0; kk < 4; ++kk)
+        mma_bf16(tmem, sdesc(xh + 2 * kk * HX_CHUNK, HX_CHUNK, 128), sdesc(w2 + 2 * kk * W_CHUNK, W_CHUNK, 128), ID,
+                 kk);
+      mma_commit(waits.mb);
+    }
+    waits.wait(true);
+    float y0 = sb3[0], y1 = sb3[1];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {  // Y = bf16(gelu(Z2 + b2)) W3^T + b3, FP32 accumulation
+      float v[16];
+      tmem_ld16(lane_base + 16 * c, v);
+#pragma unroll
+      for (int k4 = 0; k4 < 4; ++k4) {
+        const float4 b = b2v[4 * c + k4], wa = w3a[4 * c + k4], wb = w3b[4 * c + k4];
+        const __nv_bfloat162 h01 = __floats2bfloat162_rn(gelu(v[4 * k4 + 0] + b.x), gelu(v[4 * k4 + 1] + b.y));
+        const __nv_bfloat162 h23 = __floats2bfloat162_rn(gelu(v[4 * k4 + 2] + b.z), gelu(v[4 * k4 + 3] + b.w));
+        const float h0 = __low2float(h01), h1 = __high2float(h01), h2 = __low2float(h23), h3 = __high2float(h23);
+        y0 += h0 * wa.x;
+        y1 += h0 * wb.x;
+        y0 += h1 * wa.y;
+        y1 += h1 * wb.y;
+        y0 += h2 * wa.z;
+        y1 += h2 * wb.z;
+        y0 += h3 * wa.w;
+        y1 += h3 * wb.w;
+      }
+    }
+    if (valid) *reinterpret_cast<float2*>(Y + row * NOUT) = make_float2(y0, y1);
+    fence_before();
+    __syncthreads();  // the next tile rewrites XH, and its MMA 1 overwrites Z2
+    fence_after();
+    if (waits.aborted()) break;
+  }
+  waits.drain();
+  if (waits.aborted() && t == 0) atomicExch(&status->error, 1);
+  fence_before();
+  __syncthreads();
+  fence_after();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(FWD_TMEM_COLS)
+                 : "memory");
+}
+
+// Training accumulates the gradients of the mean squared error (1/n) sum_rows sum_k
+// (y_k - t_k)^2 into grad (FP32, zeroed by the caller) and the squared-error sum into *loss.
+// Column 88 of HX (the first padding column of the input chunk) holds 1 for valid rows, so
+// the weight-gradient MMA also returns the bias gradients: DW[j][88] = sum_rows dH2[:, j] =
+// db2[j], DW[64 + i][88] = db1[i]. W1's padded input columns are 0, so the forward product
+// ignores it.
+constexpr int ONES_COL = 64 + NIN;
+
+__global__ void __launch_bounds__(TILE, 2) k_mlp_train(const __nv_bfloat16* __restrict__ X, int64_t n,
+                                                       const ParamsBF16* __restrict__ wbf,
+                                                       const Params* __restrict__ p,
+                                                       const float* __restrict__ target, Params* __restrict__ grad,
+                                                       float* loss, float inv_n, Status* status) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  unsigned char* HX = smem;
+  unsigned char* DD = smem + HX_BYTES;
+  unsigned char* W1s = DD + DD_BYTES;
+  unsigned char* W2s = W1s + W1_BYTES;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(W2s + W2_BYTES);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(W2s + W2_BYTES + 16);
+  __nv_bfloat16* sH2 = reinterpret_cast<__nv_bfloat16*>(W2s + W2_BYTES + 64);  // 128 x 64
+  float* sDY = reinterpret_cast<float*>(W2s + W2_BYTES + 64 + TILE * NH * 2);   // 128 x 2
+  __shared__ float sb1[NH], sb2[NH], sw3[NOUT * NH], sb3[NOUT];
+  __shared__ int s_abort;
+
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const int64_t ntiles = (n + TILE - 1) / TILE;
+  if ((int64_t)blockIdx.x >= ntiles) return;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(TRAIN_TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (t == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    s_abort = 0;
+  }
+  load_weights(W1s, W2s, sb1, sb2, sw3, sb3, wbf, p, t);
+  fence_async_smem();
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
   const uint32_t hx = smem_u32(HX), dd = smem_u32(DD), w1 = smem_u32(W1s), w2 = smem_u32(W2s);
   const uint32_t ID_FWD = idesc_bf16(128, 64, 0, 0), ID_BWD = idesc_bf16(128, 64, 0, 1),
                  ID_WGRAD = idesc_bf16(128, 96, 1, 1);
-  uint32_t phase = 0;
+  MmaWaits waits(smem_u32(mbar), &s_abort);
   bool first_wgrad = true;
   float loss_local = 0.0f, gw3 = 0.0f, gb3 = 0.0f;  // thread t: dW3[t / 64][t % 64]; t < 2: db3[t]
-
-  auto wait_mma = [&]() {  // the whole CTA waits; one give-up aborts the remaining tiles
-    bool ok = mbar_wait(mb, phase);
-    phase ^= 1;
-    if (!ok) atomicExch(&s_abort, 1);
-    fence_after();
-  };
   auto sync_for_mma = [&]() {  // shared-memory writes -> visible to the tensor core
     fence_async_smem();
     fence_before();
@@ -240,7 +446,6 @@ __global__ void __launch_bounds__(TILE, MlpShape<TRAIN>::ctas_per_sm) k_mlp(cons
   };
 
   for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    if (s_abort) break;
     const int64_t row = tile * TILE + t;
     const bool valid = row < n;
     // X -> HX[:, 64:96]: 24 features as three 16-byte chunks, then [1 (valid rows), 0 x 7]
@@ -254,18 +459,19 @@ __global__ void __launch_bounds__(TILE, MlpShape<TRAIN>::ctas_per_sm) k_mlp(cons
       }
 #pragma unroll
       for (int c = 0; c < 3; ++c) *reinterpret_cast<uint4*>(HX + tile_off(t, 64 + 8 * c, HX_CHUNK)) = q[c];
-      float ones[8] = {TRAIN && valid ? 1.0f : 0.0f, 0, 0, 0, 0, 0, 0, 0};
+      float ones[8] = {valid ? 1.0f : 0.0f, 0, 0, 0, 0, 0, 0, 0};
       store8(HX, t, ONES_COL, HX_CHUNK, ones);
     }
     sync_for_mma();
+    if (waits.aborted()) break;
     if (t == 0) {  // Z1 = X W1^T
 #pragma unroll
       for (int kk = 0; kk < 2; ++kk)
         mma_bf16(tmem + 0, sdesc(hx + (8 + 2 * kk) * HX_CHUNK, HX_CHUNK, 128),
                  sdesc(w1 + 2 * kk * W_CHUNK, W_CHUNK, 128), ID_FWD, kk);
-      mma_commit(mb);
+      mma_commit(waits.mb);
     }
-    wait_mma();
+    waits.wait(true);
 #pragma unroll
     for (int c = 0; c < 4; ++c) {  // H1 = gelu(Z1 + b1) -> HX[:, 0:64]
       float v[16];
@@ -276,14 +482,15 @@ __global__ void __launch_bounds__(TILE, MlpShape<TRAIN>::ctas_per_sm) k_mlp(cons
       store8(HX, t, 16 * c + 8, HX_CHUNK, v + 8);
     }
     sync_for_mma();
+    if (waits.aborted()) break;
     if (t == 0) {  // Z2 = H1 W2^T
 #pragma unroll
       for (int kk = 0; kk < 4; ++kk)
         mma_bf16(tmem + 64, sdesc(hx + 2 * kk * HX_CHUNK, HX_CHUNK, 128), sdesc(w2 + 2 * kk * W_CHUNK, W_CHUNK, 128),
                  ID_FWD, kk);
-      mma_commit(mb);
+      mma_commit(waits.mb);
     }
-    wait_mma();
+    waits.wait(true);
     float y[NOUT] = {sb3[0], sb3[1]};
 #pragma unroll
     for (int c = 0; c < 4; ++c) {  // Y = bf16(gelu(Z2 + b2)) W3^T + b3, FP32 accumulation
@@ -295,18 +502,8 @@ __global__ void __launch_bounds__(TILE, MlpShape<TRAIN>::ctas_per_sm) k_mlp(cons
         const float h2 = bf(gelu(v[k] + sb2[j]));
         y[0] += h2 * sw3[j];
         y[1] += h2 * sw3[NH + j];
-        if (TRAIN) sH2[t * NH + j] = __float2bfloat16_rn(h2);
+        sH2[t * NH + j] = __float2bfloat16_rn(h2);
       }
-    }
-    if (!TRAIN) {
-      if (valid) {
-        Y[row * NOUT + 0] = y[0];
-        Y[row * NOUT + 1] = y[1];
-      }
-      fence_before();
-      __syncthreads();  // the next tile rewrites HX
-      fence_after();
-      continue;
     }
     // ---- backward ----
     float dy[NOUT];
@@ -330,12 +527,13 @@ __global__ void __launch_bounds__(TILE, MlpShape<TRAIN>::ctas_per_sm) k_mlp(cons
       store8(DD, t, 16 * c + 8, HX_CHUNK, v + 8);
     }
     sync_for_mma();  // also publishes sH2 and sDY
+    if (waits.aborted()) break;
     if (t == 0) {    // G = dH2 W2 (overwrites Z2)
 #pragma unroll
       for (int kk = 0; kk < 4; ++kk)
         mma_bf16(tmem + 64, sdesc(dd + 2 * kk * HX_CHUNK, HX_CHUNK, 128), sdesc(w2 + 2 * kk * 128, 128, W_CHUNK),
                  ID_BWD, kk);
-      mma_commit(mb);
+      mma_commit(waits.mb);
     }
     {  // meanwhile: dW3[o][j] += sum_rows dY[:, o] H2[:, j], db3 += sum_rows dY
       const int o = t / NH, j = t % NH;
@@ -348,7 +546,7 @@ __global__ void __launch_bounds__(TILE, MlpShape<TRAIN>::ctas_per_sm) k_mlp(cons
         gb3 += b;
       }
     }
-    wait_mma();
+    waits.wait(true);
 #pragma unroll
     for (int c = 0; c < 4; ++c) {  // dH1 = G * gelu'(Z1 + b1) -> DD[:, 64:128]
       float g[16], z[16];
@@ -360,61 +558,63 @@ __global__ void __launch_bounds__(TILE, MlpShape<TRAIN>::ctas_per_sm) k_mlp(cons
       store8(DD, t, 64 + 16 * c + 8, HX_CHUNK, g + 8);
     }
     sync_for_mma();
+    if (waits.aborted()) break;
     if (t == 0) {  // DW += DD^T [H1 | X | 1]
 #pragma unroll
       for (int kk = 0; kk < 8; ++kk)
         mma_bf16(tmem + 128, sdesc(dd + 2 * kk * 128, 128, HX_CHUNK), sdesc(hx + 2 * kk * 128, 128, HX_CHUNK),
                  ID_WGRAD, (first_wgrad && kk == 0) ? 0 : 1);
-      mma_commit(mb);
+      mma_commit(waits.mb);
     }
     first_wgrad = false;
-    wait_mma();
+    waits.wait(true);
     fence_before();
     __syncthreads();  // the next tile rewrites HX, DD, sH2 and sDY
     fence_after();
+    if (waits.aborted()) break;
   }
 
-  if (TRAIN) {
-    if (!s_abort && !first_wgrad) {  // row t of DW: dW2 and db2 (t < 64) or dW1 and db1
-      float v[16];
-      if (t < NH) {
+  waits.drain();
+  if (!waits.aborted() && !first_wgrad) {  // row t of DW: dW2 and db2 (t < 64) or dW1 and db1
+    float v[16];
+    if (t < NH) {
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          tmem_ld16(lane_base + 128 + 16 * c, v);
+      for (int c = 0; c < 4; ++c) {
+        tmem_ld16(lane_base + 128 + 16 * c, v);
 #pragma unroll
-          for (int k = 0; k < 16; ++k) atomicAdd(&grad->W2[t * NH + 16 * c + k], v[k]);
-        }
+        for (int k = 0; k < 16; ++k) atomicAdd(&grad->W2[t * NH + 16 * c + k], v[k]);
+      }
 #pragma unroll
-        for (int c = 0; c < 2; ++c) {
-          tmem_ld16(lane_base + 128 + 64 + 16 * c, v);
-          if (c == 1) atomicAdd(&grad->b2[t], v[ONES_COL - 64 - 16]);
-        }
-      } else {
+      for (int c = 0; c < 2; ++c) {
+        tmem_ld16(lane_base + 128 + 64 + 16 * c, v);
+        if (c == 1) atomicAdd(&grad->b2[t], v[ONES_COL - 64 - 16]);
+      }
+    } else {
 #pragma unroll
-        for (int c = 0; c < 2; ++c) {
-          tmem_ld16(lane_base + 128 + 64 + 16 * c, v);
+      for (int c = 0; c < 2; ++c) {
+        tmem_ld16(lane_base + 128 + 64 + 16 * c, v);
 #pragma unroll
-          for (int k = 0; k < 16; ++k) {
-            const int in = 16 * c + k;
-            if (in < NIN) atomicAdd(&grad->W1[(t - NH) * NIN + in], v[k]);
-            if (in == NIN) atomicAdd(&grad->b1[t - NH], v[k]);
-          }
+        for (int k = 0; k < 16; ++k) {
+          const int in = 16 * c + k;
+          if (in < NIN) atomicAdd(&grad->W1[(t - NH) * NIN + in], v[k]);
+          if (in == NIN) atomicAdd(&grad->b1[t - NH], v[k]);
         }
       }
-      atomicAdd(&grad->W3[t], gw3);
-      if (t < NOUT) atomicAdd(&grad->b3[t], gb3);
     }
-    float l = loss_local;
-#pragma unroll
-    for (int s = 16; s > 0; s >>= 1) l += __shfl_xor_sync(0xffffffffu, l, s);
-    if (lane == 0) atomicAdd(loss, l);
+    atomicAdd(&grad->W3[t], gw3);
+    if (t < NOUT) atomicAdd(&grad->b3[t], gb3);
   }
-  if (s_abort && t == 0) atomicExch(&status->error, 1);
+  float l = loss_local;
+#pragma unroll
+  for (int s = 16; s > 0; s >>= 1) l += __shfl_xor_sync(0xffffffffu, l, s);
+  if (lane == 0) atomicAdd(loss, l);
+  if (waits.aborted() && t == 0) atomicExch(&status->error, 1);
   fence_before();
   __syncthreads();
   fence_after();
   if (warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TRAIN_TMEM_COLS)
+                 : "memory");
 }
 
 // Adam on the FP32 master parameters; refreshes the BF16 copies.
@@ -462,7 +662,9 @@ struct TriskClosure {
   Status* status = nullptr;
   int64_t adam_step = 0;
   int64_t launches = 0;
-  int sms = 0;  // the device's SM count (persistent grids)
+  int sms = 0;              // the device's SM count (persistent grids)
+  int forward_per_sm = 1;   // resident inference CTAs per SM
+  int64_t expire_tile = -1;  // test of the bounded wait: see trisk_closure_expire_wait_once
   ~TriskClosure() {
     int prev = -1;
     cudaGetDevice(&prev);
@@ -491,17 +693,26 @@ void check_status(TriskClosure& c) {
   }
 }
 
-int mlp_grid(TriskClosure& c, int64_t n, int train) {
+// persistent grids: every resident CTA of the device, or one per tile when there are fewer
+int mlp_grid(const TriskClosure& c, int64_t n, int per_sm) {
   const int64_t tiles = (n + TILE - 1) / TILE;
-  const int64_t limit = (int64_t)c.sms * (train ? MlpShape<1>::ctas_per_sm : MlpShape<0>::ctas_per_sm);
-  return (int)std::max<int64_t>(1, std::min<int64_t>(tiles, limit));
+  return (int)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)c.sms * per_sm));
 }
 
-template <int TRAIN>
-void launch_mlp(TriskClosure& c, const __nv_bfloat16* X, int64_t n, const float* target, float* Y, float inv_n) {
+void launch_forward(TriskClosure& c, const __nv_bfloat16* X, int64_t n, float* Y, cudaStream_t stream) {
   if (n == 0) return;
-  k_mlp<TRAIN><<<mlp_grid(c, n, TRAIN), TILE, MlpShape<TRAIN>::smem, c.stream>>>(X, n, c.wbf, c.p, target, Y, c.g,
-                                                                                  c.loss, inv_n, c.status);
+  const int64_t expire = c.expire_tile;
+  c.expire_tile = -1;
+  k_mlp_forward<<<mlp_grid(c, n, c.forward_per_sm), TILE, FWD_SMEM_BYTES, stream>>>(X, n, c.wbf, c.p, Y, c.status,
+                                                                                     expire);
+  CUDA_CHECK(cudaGetLastError());
+  c.launches++;
+}
+
+void launch_train(TriskClosure& c, const __nv_bfloat16* X, int64_t n, const float* target, float inv_n) {
+  if (n == 0) return;
+  k_mlp_train<<<mlp_grid(c, n, 2), TILE, SMEM_BYTES, c.stream>>>(X, n, c.wbf, c.p, target, c.g, c.loss, inv_n,
+                                                                 c.status);
   CUDA_CHECK(cudaGetLastError());
   c.launches++;
 }
@@ -511,12 +722,7 @@ void launch_mlp(TriskClosure& c, const __nv_bfloat16* X, int64_t n, const float*
 namespace trisk {
 
 void closure_forward_on(TriskClosure* c, const void* X, int64_t n, float* Y, cudaStream_t stream) {
-  if (n == 0) return;
-  k_mlp<0><<<mlp_grid(*c, n, 0), TILE, MlpShape<0>::smem, stream>>>(static_cast<const __nv_bfloat16*>(X), n, c->wbf,
-                                                                     c->p, nullptr, Y, nullptr, nullptr, 0.0f,
-                                                                     c->status);
-  CUDA_CHECK(cudaGetLastError());
-  c->launches++;
+  launch_forward(*c, static_cast<const __nv_bfloat16*>(X), n, Y, stream);
 }
 
 void closure_check(TriskClosure* c) { check_status(*c); }
@@ -548,11 +754,15 @@ int trisk_closure_create(int32_t device, const float* params, TriskClosure** out
   else CUDA_CHECK(cudaMemset(c->p, 0, sizeof(Params)));
   k_refresh_bf16<<<(NH * NH + 255) / 256, 256, 0, c->stream>>>(c->p, c->wbf);
   CUDA_CHECK(cudaGetLastError());
-  CUDA_CHECK(cudaFuncSetAttribute(k_mlp<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, MlpShape<0>::smem));
-  CUDA_CHECK(cudaFuncSetAttribute(k_mlp<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, MlpShape<1>::smem));
+  CUDA_CHECK(cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, FWD_SMEM_BYTES));
+  CUDA_CHECK(cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
   int sms = 0;
   CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
   c->sms = sms;
+  int per_sm = 0;
+  CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mlp_forward, TILE, FWD_SMEM_BYTES));
+  // every resident CTA must find its tensor-memory columns free (512 per SM)
+  c->forward_per_sm = std::max(1, std::min<int>(per_sm, 512 / (int)FWD_TMEM_COLS));
   CUDA_CHECK(cudaStreamSynchronize(c->stream));
   *out = c.release();
   TRISK_API_END
@@ -590,7 +800,7 @@ int trisk_closure_forward(TriskClosure* closure, const void* X, int64_t n, float
   TriskClosure& c = *checked_c(closure);
   if (!X || !Y || n < 0) throw Error(TRISK_ERR_ARGUMENT, "bad argument");
   DeviceGuard guard(c.device);
-  launch_mlp<0>(c, static_cast<const __nv_bfloat16*>(X), n, nullptr, Y, 0.0f);
+  launch_forward(c, static_cast<const __nv_bfloat16*>(X), n, Y, c.stream);
   check_status(c);
   TRISK_API_END
 }
@@ -605,7 +815,7 @@ int trisk_closure_gradients(TriskClosure* closure, const void* X, const float* t
   DeviceGuard guard(c.device);
   CUDA_CHECK(cudaMemsetAsync(c.g, 0, sizeof(Params), c.stream));
   CUDA_CHECK(cudaMemsetAsync(c.loss, 0, sizeof(float), c.stream));
-  launch_mlp<1>(c, static_cast<const __nv_bfloat16*>(X), n, target, nullptr, 1.0f / (float)n);
+  launch_train(c, static_cast<const __nv_bfloat16*>(X), n, target, 1.0f / (float)n);
   if (grads) CUDA_CHECK(cudaMemcpyAsync(grads, c.g, sizeof(Params), cudaMemcpyDeviceToHost, c.stream));
   float l = 0;
   CUDA_CHECK(cudaMemcpyAsync(&l, c.loss, sizeof(float), cudaMemcpyDeviceToHost, c.stream));
@@ -633,6 +843,17 @@ int trisk_closure_synchronize(TriskClosure* closure) {
   TriskClosure& c = *checked_c(closure);
   DeviceGuard guard(c.device);
   check_status(c);
+  TRISK_API_END
+}
+
+// Test of the bounded tensor-core wait: the next inference launch of this closure leaves the
+// first tensor-core operation of `tile` un-issued, so that tile's wait runs out (after half a
+// second) and the call reports TRISK_ERR_TIMEOUT; later calls are unaffected.
+int trisk_closure_expire_wait_once(TriskClosure* closure, int64_t tile) {
+  TRISK_API_BEGIN
+  TriskClosure& c = *checked_c(closure);
+  if (tile < 0) throw Error(TRISK_ERR_ARGUMENT, "tile must be >= 0");
+  c.expire_tile = tile;
   TRISK_API_END
 }
 

@@ -206,9 +206,12 @@ __device__ __forceinline__ double energy_gradient(const DevTables& T, double ue,
   return ue * (double)gm[0] * (h0 * (double)gm[2] + h1 * (double)gm[3]);
 }
 
-// sums[2m] += <g, dq>, sums[2m + 1] += <g, g> for member m; block (32, 8): x members, y edges
+// Per-block partial sums of <g, dq> and <g, g> for member m: partials[(2m) gridDim.x + block]
+// and partials[(2m + 1) gridDim.x + block]; block (32, 8): x members, y edges. kg_sum_rows
+// then adds each row's partials in a fixed order, so the sums do not depend on the order in
+// which blocks finish.
 template <class R>
-__global__ void kg_work_sums(DevTables T, const R* y, const R* dq, const float* geom, int M, double* sums) {
+__global__ void kg_work_sums(DevTables T, const R* y, const R* dq, const float* geom, int M, double* partials) {
   __shared__ double s1[8][32], s2[8][32];
   const int m = blockIdx.y * 32 + threadIdx.x;
   double a = 0.0, b = 0.0;
@@ -230,9 +233,25 @@ __global__ void kg_work_sums(DevTables T, const R* y, const R* dq, const float* 
       a += s1[k][threadIdx.x];
       b += s2[k][threadIdx.x];
     }
-    atomicAdd(&sums[2 * m], a);
-    atomicAdd(&sums[2 * m + 1], b);
+    partials[(size_t)(2 * m) * gridDim.x + blockIdx.x] = a;
+    partials[(size_t)(2 * m + 1) * gridDim.x + blockIdx.x] = b;
   }
+}
+
+// out[row] = the sum of partials[row * ncols + 0 .. ncols - 1] in a fixed order (each thread
+// a fixed strided run, then a fixed tree): one block of 256 threads per row.
+__global__ void kg_sum_rows(const double* partials, int ncols, double* out) {
+  __shared__ double sm[256];
+  const double* p = partials + (size_t)blockIdx.x * ncols;
+  double s = 0.0;
+  for (int c = threadIdx.x; c < ncols; c += 256) s += p[c];
+  sm[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) sm[threadIdx.x] += sm[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[blockIdx.x] = sm[0];
 }
 
 template <class R>
@@ -251,10 +270,11 @@ __global__ void kg_work_project(DevTables T, const R* y, R* dq, const float* geo
   dq[r] = (R)((double)dq[r] - sums[2 * m] / gg * g);
 }
 
-// energy[m] += sum_i A_i h_i (K_i + g h_i / 2) over this block's cells (TRiSKShallowWater.jl:406-411)
+// partials[m gridDim.x + block] = sum_i A_i h_i (K_i + g h_i / 2) over this block's cells
+// (TRiSKShallowWater.jl:406-411); kg_sum_rows adds them per member in a fixed order.
 template <class R>
 __global__ void kg_energy(const R* y, const R* K, const double* area, int nc, int ne, int M, double g,
-                          double* energy) {
+                          double* partials) {
   __shared__ double sm[256];
   const int m = blockIdx.y;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -270,7 +290,7 @@ __global__ void kg_energy(const R* y, const R* K, const double* area, int nc, in
     if ((int)threadIdx.x < w) sm[threadIdx.x] += sm[threadIdx.x + w];
     __syncthreads();
   }
-  if (threadIdx.x == 0) atomicAdd(&energy[m], sm[0]);
+  if (threadIdx.x == 0) partials[(size_t)m * gridDim.x + blockIdx.x] = sm[0];
 }
 
 __global__ void kg_advance(int* counters, int n) {
@@ -304,7 +324,11 @@ struct ClosureSlot {
   bool every_stage = false;    // false: the network runs at stage 1 and its output is reused
   bool work_free = false;      // project the momentum correction to do no work (per member)
   double* sums = nullptr;      // 2 M: <g, dq>, <g, g> per member
+  double* partials = nullptr;  // 2 M x WORK_SUM_BLOCKS per-block partial sums of them
 };
+
+// blocks of kg_work_sums along the edges (the row length of its partial sums)
+constexpr int WORK_SUM_BLOCKS = 1024;
 
 struct TriskEnsemble {
   int device = 0;
@@ -316,7 +340,9 @@ struct TriskEnsemble {
   int grid[3] = {0, 0, 0};
   GroupSet G{};
   ClosureSlot cl[trisk::MAX_GROUPS];
-  double* energy = nullptr;  // per-member energies of the diagnostic
+  double* energy = nullptr;           // per-member energies of the diagnostic
+  double* energy_partials = nullptr;  // members x blocks partial sums of them
+  size_t energy_partials_size = 0;
   std::vector<TriskModel*> models;
   std::vector<void*> allocations;
   int* counters = nullptr;
@@ -426,13 +452,14 @@ void enqueue_closure(TriskEnsemble& e, int stage) {
       CUDA_CHECK(cudaGetLastError());
       if (c.work_free) {
         const R* ys = reinterpret_cast<const R*>(stage == 1 ? D.y : D.st);
-        CUDA_CHECK(cudaMemsetAsync(c.sums, 0, 2 * D.M * sizeof(double), e.stream));
-        const dim3 grid((unsigned)std::min<int64_t>(cdiv(D.T.ne, 8), 1024), (unsigned)cdiv(D.M, 32));
+        const int nx = (int)std::min<int64_t>(cdiv(D.T.ne, 8), WORK_SUM_BLOCKS);
+        const dim3 grid((unsigned)nx, (unsigned)cdiv(D.M, 32));
         kg_work_sums<R><<<grid, dim3(32, 8), 0, e.stream>>>(D.T, ys, reinterpret_cast<const R*>(c.dq), c.geom, D.M,
-                                                             c.sums);
+                                                             c.partials);
+        kg_sum_rows<<<(unsigned)(2 * D.M), 256, 0, e.stream>>>(c.partials, nx, c.sums);
         kg_work_project<R><<<nb, 256, 0, e.stream>>>(D.T, ys, reinterpret_cast<R*>(c.dq), c.geom, D.M, rows, c.sums);
         CUDA_CHECK(cudaGetLastError());
-        e.launches += 2;
+        e.launches += 3;
       }
     });
     e.launches += 3;
@@ -884,7 +911,10 @@ int trisk_ensemble_set_closure(TriskEnsemble* ens, int32_t group, TriskClosure* 
   c.norm.out_scale[1] = norm[2 * NFEAT + 1];
   c.every_stage = (flags & 1) != 0;
   c.work_free = (flags & 2) != 0;
-  if (c.work_free && !c.sums) c.sums = e.alloc<double>(2 * (size_t)D.M);
+  if (c.work_free && !c.sums) {
+    c.sums = e.alloc<double>(2 * (size_t)D.M);
+    c.partials = e.alloc<double>(2 * (size_t)D.M * WORK_SUM_BLOCKS);
+  }
   c.net = net;
   TRISK_API_END
 }
@@ -964,7 +994,11 @@ int trisk_ensemble_energy(TriskEnsemble* ens, int32_t group, double* energies) {
   const GroupDesc& D = e.G.g[group];
   const int M = D.M;
   if (!e.energy) e.energy = e.alloc<double>(e.max_members);
-  CUDA_CHECK(cudaMemsetAsync(e.energy, 0, M * sizeof(double), e.stream));
+  const int nblocks = (int)cdiv(m.nc, 256);
+  if (e.energy_partials_size < (size_t)nblocks * M) {  // grown on demand, kept for later calls
+    e.energy_partials_size = (size_t)nblocks * M;
+    e.energy_partials = e.alloc<double>(e.energy_partials_size);
+  }
   const int B = 128;
   with_modes_e(e.pv, e.ke, [&](auto pvc, auto kec) {
     constexpr int PV = decltype(pvc)::value, KE = decltype(kec)::value;
@@ -976,14 +1010,15 @@ int trisk_ensemble_energy(TriskEnsemble* ens, int32_t group, double* energies) {
       k_vertex<PV, KE, true, R><<<(unsigned)cdiv(m.nv * M, B), B, 0, e.stream>>>(D.T, W, u, h, M, 0);
       const int nbE = (int)cdiv(m.ne * M, B);
       k_flux<PV, KE, true, R><<<(unsigned)(nbE + cdiv(m.nc * M, B)), B, 0, e.stream>>>(D.T, W, u, h, M, nbE, 1);
-      kg_energy<R><<<dim3((unsigned)cdiv(m.nc, 256), (unsigned)M), 256, 0, e.stream>>>(
-          u, W.K, m.area_c, (int)m.nc, (int)m.ne, M, m.gravity, e.energy);
+      kg_energy<R><<<dim3((unsigned)nblocks, (unsigned)M), 256, 0, e.stream>>>(
+          u, W.K, m.area_c, (int)m.nc, (int)m.ne, M, m.gravity, e.energy_partials);
+      kg_sum_rows<<<(unsigned)M, 256, 0, e.stream>>>(e.energy_partials, nblocks, e.energy);
     });
   });
   CUDA_CHECK(cudaGetLastError());
   CUDA_CHECK(cudaMemcpyAsync(energies, e.energy, M * sizeof(double), cudaMemcpyDeviceToHost, e.stream));
   CUDA_CHECK(cudaStreamSynchronize(e.stream));
-  e.launches += 3;
+  e.launches += 4;
   TRISK_API_END
 }
 

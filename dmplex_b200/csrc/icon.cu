@@ -202,11 +202,15 @@ struct TriskIconModel {
   int* flag = nullptr;
   std::vector<void*> allocations;
   int64_t launches = 0;
+  cudaGraphExec_t graph = nullptr;  // one RK4 step at graph_dt
+  double graph_dt = 0.0;
+  int64_t graph_launches = 0;       // kernels in the graph
 
   ~TriskIconModel() {
     int prev = -1;
     cudaGetDevice(&prev);
     cudaSetDevice(device);
+    if (graph) cudaGraphExecDestroy(graph);
     if (caller_ev) cudaEventDestroy(caller_ev);
     if (stream) {
       cudaStreamSynchronize(stream);
@@ -260,6 +264,55 @@ void icon_tendency(TriskIconModel& m, const DevStage& S, int epi) {
     case EPI_STAGE3: ilaunch(m, k_icon_tend<EPI_STAGE3>, g, true, m.T, m.W, S, (int)nbE); break;
     default: ilaunch(m, k_icon_tend<EPI_STAGE4>, g, true, m.T, m.W, S, (int)nbE); break;
   }
+}
+
+// One RK4 step on the internal state m.y (RungeKutta.jl:18-29), the stage updates fused into
+// the last phase of every tendency.
+void icon_enqueue_step(TriskIconModel& m, double dt) {
+  DevStage S{};
+  S.y = m.y;
+  S.acc = m.acc;
+  S.st = m.st;
+  S.flag = m.flag;
+  S.sixth = dt / 6;
+  S.u = m.y;
+  S.h = m.y + m.ne;
+  S.c = dt / 2;
+  icon_tendency(m, S, EPI_STAGE1);
+  S.u = m.st;
+  S.h = m.st + m.ne;
+  icon_tendency(m, S, EPI_STAGE2);
+  S.c = dt;
+  icon_tendency(m, S, EPI_STAGE3);
+  icon_tendency(m, S, EPI_STAGE4);
+}
+
+// The step's 12 launches (20 with divergence damping) as one CUDA graph, captured again when
+// dt changes; replayed once per step.
+void icon_ensure_graph(TriskIconModel& m, double dt) {
+  if (m.graph && m.graph_dt == dt) return;
+  if (m.graph) {
+    cudaGraphExecDestroy(m.graph);
+    m.graph = nullptr;
+  }
+  const int64_t before = m.launches;
+  cudaGraph_t g = nullptr;
+  CUDA_CHECK(cudaStreamBeginCapture(m.stream, cudaStreamCaptureModeThreadLocal));
+  try {
+    icon_enqueue_step(m, dt);
+  } catch (...) {
+    cudaStreamEndCapture(m.stream, &g);
+    if (g) cudaGraphDestroy(g);
+    m.launches = before;
+    throw;
+  }
+  CUDA_CHECK(cudaStreamEndCapture(m.stream, &g));
+  m.graph_launches = m.launches - before;
+  m.launches = before;  // captured launches are counted when the graph is replayed
+  cudaError_t e = cudaGraphInstantiate(&m.graph, g, 0);
+  cudaGraphDestroy(g);
+  CUDA_CHECK(e);
+  m.graph_dt = dt;
 }
 
 TriskIconModel* checked_icon(TriskIconModel* m) {
@@ -439,23 +492,10 @@ int trisk_icon_rk4_step(TriskIconModel* model, double* y, double dt, int64_t nst
   if (nsteps < 0 || !std::isfinite(dt)) throw Error(TRISK_ERR_ARGUMENT, "bad dt or step count");
   DeviceGuard guard(m.device);
   icon_state_in(m, y, m.y);
-  DevStage S{};
-  S.y = m.y;
-  S.acc = m.acc;
-  S.st = m.st;
-  S.flag = m.flag;
-  S.sixth = dt / 6;
-  for (int64_t s = 0; s < nsteps; ++s) {  // RungeKutta.jl:18-29, stages fused into the tendency
-    S.u = m.y;
-    S.h = m.y + m.ne;
-    S.c = dt / 2;
-    icon_tendency(m, S, EPI_STAGE1);
-    S.u = m.st;
-    S.h = m.st + m.ne;
-    icon_tendency(m, S, EPI_STAGE2);
-    S.c = dt;
-    icon_tendency(m, S, EPI_STAGE3);
-    icon_tendency(m, S, EPI_STAGE4);
+  if (nsteps > 0) icon_ensure_graph(m, dt);
+  for (int64_t s = 0; s < nsteps; ++s) {
+    CUDA_CHECK(cudaGraphLaunch(m.graph, m.stream));
+    m.launches += m.graph_launches;
   }
   icon_state_out(m, y, m.y);
   icon_check_flag(m);

@@ -159,9 +159,32 @@ class ICONShallowWater:
         check(lib.trisk_icon_rk4_step(self._h, _state(y, self), float(dt), int(nsteps)))
         return y
 
+    def launch_count(self) -> int:
+        """Kernels launched so far (a replayed RK4 step counts its graph's kernels)."""
+        return int(lib.trisk_icon_launch_count(self._h))
+
+    def algorithmic_bytes(self) -> dict:
+        return algorithmic_bytes(self.tables)
+
     def total_mass(self, y) -> float:
         y = np.asarray(y)
         return float(self.grid.cell_areas @ y[self.ne:])
+
+
+def algorithmic_bytes(tables: dict) -> dict:
+    """The ICON path's byte model, in the form used for the TRiSK path: int32 indices (4 B) and
+    FP64 weights (8 B) as uploaded (vertex tables padded to 6 edges), every table read once per
+    tendency; the state N = 8 (ne + nc) bytes; per RK4 step 4 (T + 2N) + 15N (each tendency
+    reads its state and writes its tendency, plus the RK4 vector passes)."""
+    ne, nc, nv = tables["ne"], tables["nc"], tables["nv"]
+    damping = len(tables.get("divergence_damping", ())) > 0
+    per_edge = 4 * 4 + 8 * 4 + 4 * 2 + 8 * 2 + 8 + 4 * 2 + 8 * 2 + 8 + (8 if damping else 0)
+    per_cell = 4 * 3 + 8 * 3 + 8 * 3
+    per_vertex = (4 + 8) * 6
+    T = ne * per_edge + nc * per_cell + nv * per_vertex
+    N = 8 * (ne + nc)
+    return {"tables": T, "state": N, "tendency": T + 2 * N, "rk4_step": 4 * (T + 2 * N) + 15 * N,
+            "per_edge": per_edge, "per_cell": per_cell, "per_vertex": per_vertex}
 
 
 def _state(y, m):

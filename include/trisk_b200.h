@@ -443,6 +443,11 @@ int trisk_closure_gradients(TriskClosure* closure, const void* X, const float* t
 int trisk_closure_adam(TriskClosure* closure, float lr, float beta1, float beta2, float eps);
 int trisk_closure_synchronize(TriskClosure* closure);
 int trisk_closure_stream(TriskClosure* closure, void** stream);
+/* Test of the bounded tensor-core wait (no reference counterpart): the next inference call of
+ * this closure leaves the first tensor-core operation of tile `tile` (rows 128 tile ..) un-issued,
+ * so that tile's wait runs out after half a second and the call returns TRISK_ERR_TIMEOUT; the
+ * closure stays usable and later calls are unaffected. */
+int trisk_closure_expire_wait_once(TriskClosure* closure, int64_t tile);
 
 /* ---- allocation-free entry point ---------------------------------------------------
  * No counterpart in the reference: it exists for callers that must not have the library

@@ -39,12 +39,25 @@ def pack(p):
     return np.concatenate([np.asarray(p[name], dtype=np.float64).ravel() for name, _ in SHAPES])
 
 
+# GELU in the tanh form of Hendrycks and Gimpel (2016), the network's activation:
+# gelu(x) = x/2 (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3))). It differs from the erf form
+# x/2 (1 + erf(x / sqrt 2)) by at most 4.8e-4 (test_closure.py checks the bound).
+GELU_C0 = np.sqrt(2.0 / np.pi)
+GELU_C1 = 0.044715 * GELU_C0
+
+
 def gelu(x):
-    return 0.5 * x * (1.0 + erf(x / np.sqrt(2.0)))
+    return 0.5 * x * (1.0 + np.tanh(x * (GELU_C0 + GELU_C1 * x * x)))
 
 
 def gelu_grad(x):
-    return 0.5 * (1.0 + erf(x / np.sqrt(2.0))) + x * np.exp(-0.5 * x * x) / np.sqrt(2 * np.pi)
+    t = np.tanh(x * (GELU_C0 + GELU_C1 * x * x))
+    return 0.5 * (1.0 + t) + 0.5 * x * (1.0 - t * t) * (GELU_C0 + 3 * GELU_C1 * x * x)
+
+
+def gelu_erf(x):
+    """The erf form of GELU (Hendrycks and Gimpel 2016), for the bound above."""
+    return 0.5 * x * (1.0 + erf(x / np.sqrt(2.0)))
 
 
 def forward(flat, X, rounding=True):

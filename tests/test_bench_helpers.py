@@ -27,3 +27,22 @@ def test_mpas_algorithmic_bytes():
         state = ne + 2 * nc + nc                        # vn, rho, rho theta, w
         outputs = 3 * nc + 3 * nv + 3 * ne + ne + nc     # theta pi K, q_v zeta_v rho_v, q_e rho_e F_s, t_vn, t_w
         assert (b8 - b4) / 4 >= 8 * (state + outputs)
+
+
+def test_leg_summary_is_compact_and_keeps_errors():
+    """The key figures of every leg close the JSON line in a few hundred bytes; a failed leg
+    keeps its error there."""
+    import json
+
+    import bench
+    line = {"value": 1.3e9, "ms_per_step": 0.1238, "timing": {"spread": 0.01},
+            "roofline": {"frac": 1.03, "frac_on_implementation_bytes": 0.86, "step_frac": 1.04},
+            "e2e": {"value": 4.6e8},
+            "ensemble": {"value": 2.38e9, "gpu_seconds_per_simulated_day": 1.2, "frac": 0.41,
+                         "fp32_state": {"gpu_seconds_per_simulated_day": 0.98, "frac": 0.3}, "steps": [1] * 50},
+            "closure": {"error": "RuntimeError: boom"}, "icon": None}
+    s = bench.leg_summary(line)
+    assert s["headline"]["k_tend_frac_on_implementation_bytes"] == 0.86
+    assert s["ensemble"]["fp32_state_gpu_seconds_per_simulated_day"] == 0.98 and "steps" not in s["ensemble"]
+    assert s["closure"] == {"error": "RuntimeError: boom"} and s["icon"] is None
+    assert len(json.dumps(s)) < 1500

@@ -110,6 +110,25 @@ def test_icon_gpu_matches_oracle(require_gpu, gradient, nu):
     yd = torch.from_numpy(y).cuda()  # device state: same numbers
     m.rk4_step(yd, dt, 3)
     assert np.array_equal(yd.cpu().numpy(), b)
+    # each step is one replay of a CUDA graph of the step's launches (12, or 20 with damping),
+    # captured again when dt changes
+    before = m.launch_count()
+    a2 = a.copy()
+    m.rk4_step(a2, dt / 2, 2)
+    assert m.launch_count() - before == 2 * (20 if nu else 12)
+    assert np.array_equal(a2, o.rk4_step(a.copy(), dt / 2, 2))
+
+
+def test_icon_algorithmic_bytes():
+    """The ICON byte model: every uploaded table once per tendency (int32 indices, FP64 weights,
+    vertex tables 6 wide), and the RK4 step in the TRiSK path's form 4 (T + 2N) + 15N."""
+    g = tri_grid(3, 0.0)
+    t = icon.icon_tables(g)
+    b = icon.algorithmic_bytes(t)
+    assert b["tables"] == g.ne * 112 + g.nc * 60 + g.nv * 72
+    assert b["rk4_step"] == 4 * (b["tables"] + 2 * b["state"]) + 15 * b["state"]
+    t["divergence_damping"] = np.ones(g.ne)
+    assert icon.algorithmic_bytes(t)["tables"] == b["tables"] + 8 * g.ne
 
 
 @pytest.mark.gpu
