@@ -486,7 +486,7 @@ def run_ensemble_leg(local_rank, seed, days=1.0, state_bits=64):
     for gi, (g, m, members, nsteps, dt) in enumerate(info):
         for k, y in enumerate(w.ensemble_members(g, members, seed=seed + gi)):
             ens.set_member(gi, k, y)
-    tuned_ms = ens.autotune(5)  # phase block sizes; the states are left as they were
+    tuned_ms = ens.autotune(5)  # phase block sizes and slices; the states are left as they were
     stream = torch.cuda.ExternalStream(ens.stream(), device=local_rank)
     longest = max(x[3] for x in info)
     ens.run(3)  # warm-up (graph capture)
@@ -514,7 +514,7 @@ def run_ensemble_leg(local_rank, seed, days=1.0, state_bits=64):
             "gpu_seconds_per_simulated_day": ms * 1e-3 / days,
             "steps": taken, "dt_s": [round(x[4], 3) for x in info], "members": [x[2] for x in info],
             "gpu_launches": ens.launch_count() - launches0, "gbs": nbytes / (ms * 1e-3) / 1e9,
-            "block": ens.block(), "autotune_ms_per_step": tuned_ms,
+            "block": ens.block(), "members_per_slice": ens.slices(), "autotune_ms_per_step": tuned_ms,
             "frac": nbytes / (ms * 1e-3) / 1e9 / peak}
 
 

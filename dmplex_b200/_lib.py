@@ -185,6 +185,8 @@ def _load():
         "trisk_ensemble_bytes": (C.c_int, [_p, C.POINTER(_f64)]),
         "trisk_ensemble_energy": (C.c_int, [_p, _i32, _p]),
         "trisk_ensemble_set_closure": (C.c_int, [_p, _i32, _p, _p, _p, _i32]),
+        "trisk_ensemble_set_slices": (C.c_int, [_p, _p]),
+        "trisk_ensemble_get_slices": (C.c_int, [_p, _p]),
         "trisk_ensemble_closure_mask": (C.c_int, [_p, _i32, _p]),
         "trisk_ensemble_features": (C.c_int, [_p, _i32, _p, _p, _p]),
         "trisk_ensemble_closure_check": (C.c_int, [_p]),

@@ -1,12 +1,15 @@
-// Batched ensembles: many members, on meshes of several levels, advanced by one persistent
-// launch per phase. A group is a set of members that share one model's tables (same mesh,
-// same scheme); its state and work vectors are [entity][member], so the table entries a
-// warp reads serve all the members it holds, and one gathered index reads the members'
-// values as one contiguous run. The RK4 step of all groups (12 phase launches and a
-// counter update) is one CUDA graph; each group has its own dt and step count, and a group
-// that has taken its steps is skipped by later replays.
+// Batched ensembles: many members, on meshes of several levels, advanced by persistent
+// launches per phase. A group is a set of members that share one model's tables (same mesh,
+// same scheme). Its members are split into slices of consecutive members, each stored on its
+// own ([entity][slice member] state and work vectors, one slice after the other), so the table
+// entries a warp reads serve all the members it holds, one gathered index reads the members'
+// values as one contiguous run, and a slice's work vectors are small enough to stay in L2
+// from one phase to the next. The phases of a set of slices (a launch set) run back to back,
+// set after set; the RK4 step of all unfinished groups is one CUDA graph; each group has its
+// own dt and step count.
 #include <algorithm>
 #include <cstring>
+#include <map>
 #include <memory>
 
 #include <cuda_bf16.h>
@@ -17,15 +20,18 @@ using namespace trisk;
 
 namespace trisk {
 
-constexpr int MAX_GROUPS = 8;
+constexpr int MAX_GROUPS = 8;  // groups of an ensemble
+constexpr int MAX_SET = 8;     // slices of one launch set
 
+// One slice: members [m0, m0 + M) of a group.
 struct GroupDesc {
   DevTables T;
   DevWork W;
   double *y, *acc, *st;
   double dt;
-  int M;       // members
-  int nsteps;  // RK4 steps this group takes in a run
+  const int* counter;  // the group's steps taken (device)
+  int M;       // members of the slice
+  int nsteps;  // RK4 steps the group takes in a run
   int startV, nV;
   int startF, nEF, nCF;
   int startT, nET, nCT;
@@ -33,11 +39,10 @@ struct GroupDesc {
 };
 
 struct GroupSet {
-  GroupDesc g[MAX_GROUPS];
+  GroupDesc g[MAX_SET];
   int n;
   int totalV, totalF, totalT;
-  const int* counters;  // steps taken per group (device)
-  int* flag;            // non-finite state seen
+  int* flag;  // non-finite state seen
 };
 
 __device__ __forceinline__ int group_of(const GroupSet& G, int vb, int phase) {
@@ -66,7 +71,7 @@ __global__ void __launch_bounds__(256) kg_vertex(const GroupSet G, int first_sta
   for (int vb = blockIdx.x; vb < G.totalV; vb += gridDim.x) {
     const int gi = group_of(G, vb, 0);
     const GroupDesc& D = G.g[gi];
-    if (G.counters[gi] >= D.nsteps) continue;
+    if (*D.counter >= D.nsteps) continue;
     const R* u = as_r<R>(first_stage ? D.y : D.st);
     if (D.P == 2)
       vertex_body<PV, KE, true, R, false, 2>(D.T, work_as<R>(D.W), u, u + (size_t)D.T.ne * D.M, D.M, 0,
@@ -82,7 +87,7 @@ __global__ void __launch_bounds__(256) kg_flux(const GroupSet G, int first_stage
   for (int vb = blockIdx.x; vb < G.totalF; vb += gridDim.x) {
     const int gi = group_of(G, vb, 1);
     const GroupDesc& D = G.g[gi];
-    if (G.counters[gi] >= D.nsteps) continue;
+    if (*D.counter >= D.nsteps) continue;
     const R* u = as_r<R>(first_stage ? D.y : D.st);
     if (D.P == 2)
       flux_body<PV, KE, true, R, false, 2>(D.T, work_as<R>(D.W), u, u + (size_t)D.T.ne * D.M, D.M, D.nEF, want_K,
@@ -99,7 +104,7 @@ __global__ void __launch_bounds__(256, 4) kg_tend(const GroupSet G) {  // <= 64 
   for (int vb = blockIdx.x; vb < G.totalT; vb += gridDim.x) {
     const int gi = group_of(G, vb, 2);
     const GroupDesc& D = G.g[gi];
-    if (G.counters[gi] >= D.nsteps) continue;
+    if (*D.counter >= D.nsteps) continue;
     DevStageT<R> S{};
     S.y = as_r<R>(D.y);
     S.acc = as_r<R>(D.acc);
@@ -131,15 +136,17 @@ struct FeatureNorm {
   double out_scale[2];
 };
 
-// The network's 24 inputs of (edge, member) rows e * M + m, formed in FP64 as the stencil's
+// The network's 24 inputs of (edge, member) rows e * M + m of a slice, formed in FP64 as the stencil's
 // mean and differences so that their BF16 rounding keeps the local gradients: u_e; u at the
 // 10 TRiSK stencil edges minus u_e (0 for padded entries); the mean and the difference
 // (second cell minus first) of h at the two cells, of q at the two vertices and of K = B - g h
-// at the two cells; and 7 geometry values of the edge. Output row: row_map ? row_map[e] * M
-// + m (file edge numbering) : the internal row.
+// at the two cells; and 7 geometry values of the edge. Output row: row_map ? row_map[e] * Mg
+// + m0 + m (file edge numbering, the group's Mg members, the slice starting at member m0) :
+// the slice's internal row.
 template <class R>
 __global__ void kg_features(DevTables T, DevWorkT<R> W, const R* y, int M, const float* geom,
-                            const FeatureNorm N, __nv_bfloat16* X, const int32_t* row_map, int64_t rows) {
+                            const FeatureNorm N, __nv_bfloat16* X, const int32_t* row_map, int64_t rows, int Mg,
+                            int m0) {
   const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (r >= rows) return;
   int e, m;  // rows < 2^31 (checked when the ensemble is made)
@@ -168,7 +175,7 @@ __global__ void kg_features(DevTables T, DevWorkT<R> W, const R* y, int M, const
   f[16] = K1 - K0;
 #pragma unroll
   for (int k = 0; k < NGEOM; ++k) f[17 + k] = geom[(size_t)e * NGEOM + k];
-  const int64_t out = row_map ? (int64_t)row_map[e] * M + m : r;
+  const int64_t out = row_map ? (int64_t)row_map[e] * Mg + m0 + m : r;
   // the row's 48 bytes as three 16-byte stores (rows are 16-byte aligned)
   __align__(16) __nv_bfloat16 b[NFEAT];
 #pragma unroll
@@ -293,8 +300,23 @@ __global__ void kg_energy(const R* y, const R* K, const double* area, int nc, in
   if (threadIdx.x == 0) partials[(size_t)m * gridDim.x + blockIdx.x] = sm[0];
 }
 
-__global__ void kg_advance(int* counters, int n) {
-  if (threadIdx.x < n) counters[threadIdx.x] += 1;
+// the step counters of the groups in `mask`
+__global__ void kg_advance(int* counters, unsigned mask) {
+  if (threadIdx.x < MAX_GROUPS && ((mask >> threadIdx.x) & 1u)) counters[threadIdx.x] += 1;
+}
+
+// A group's state from slices of S_from members to slices of S_to members: member m of a
+// group of M members sits in slice m / S (members m0 = S (m / S) onwards, Ss = min(S, M - m0)
+// of them) at N m0 + j Ss + (m - m0) for state element j < N.
+template <class R>
+__global__ void kg_relayout(R* dst, const R* src, int64_t N, int M, int S_from, int S_to) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= N * M) return;
+  const int64_t j = t / M;
+  const int m = (int)(t - j * M);
+  const int a0 = (m / S_from) * S_from, b0 = (m / S_to) * S_to;
+  const int sa = min(S_from, M - a0), sb = min(S_to, M - b0);
+  dst[N * b0 + j * sb + (m - b0)] = src[N * a0 + j * sa + (m - a0)];
 }
 
 // y_group[j M + m] = y_file[n2o[j]]  and back
@@ -311,7 +333,9 @@ __global__ void kg_gather_member(double* dst, const R* src, const int32_t* o2n, 
 
 }  // namespace trisk
 
-// A group's learned closure: network, buffers of its (edge, member) rows and settings.
+// A group's learned closure: network, buffers of its (edge, member) rows and settings. The
+// rows of slice [m0, m0 + Ms) are rows ne m0 .. ne (m0 + Ms) - 1 of the buffers (e Ms + m
+// within the slice).
 struct ClosureSlot {
   TriskClosure* net = nullptr;
   __nv_bfloat16* X = nullptr;  // rows x 24 features
@@ -329,6 +353,33 @@ struct ClosureSlot {
 
 // blocks of kg_work_sums along the edges (the row length of its partial sums)
 constexpr int WORK_SUM_BLOCKS = 1024;
+// A slice's state and work vectors should stay in L2 (126 MB) beside the streaming tables:
+// the budget of the default slicing and of a launch set.
+constexpr double SLICE_L2_BUDGET = 96.0 * (1 << 20);
+
+// A user group: its members' buffers (every slice's, one after the other) and its slicing.
+struct EnsembleGroup {
+  TriskModel* m = nullptr;
+  int M = 0;                 // members
+  int S = 0;                 // members per slice (the last slice may have fewer)
+  double dt = 0;
+  int nsteps = 0;
+  int64_t taken = 0;         // steps taken, as the host counts them
+  double *y = nullptr, *acc = nullptr, *st = nullptr;
+  DevWork W{};
+  ClosureSlot cl;
+  double member_bytes = 0;   // state (y, acc, stage) and work vectors of one member
+};
+
+struct Slice {
+  int group, m0;
+  GroupDesc D;
+};
+
+struct EnsembleGraph {
+  cudaGraphExec_t exec = nullptr;
+  int64_t kernels = 0;
+};
 
 struct TriskEnsemble {
   int device = 0;
@@ -337,11 +388,13 @@ struct TriskEnsemble {
   bool fp32 = false;                // state and work vectors stored as float (arithmetic FP64)
   int pv = 0, ke = 0;
   int block[3] = {128, 128, 128};  // threads per block of the vertex, flux and tendency phases
-  int grid[3] = {0, 0, 0};
-  GroupSet G{};
-  ClosureSlot cl[trisk::MAX_GROUPS];
-  double* energy = nullptr;           // per-member energies of the diagnostic
-  double* energy_partials = nullptr;  // members x blocks partial sums of them
+  int occ[3] = {1, 1, 1};          // resident blocks per SM of the three phases
+  int sms = 1;
+  std::vector<EnsembleGroup> groups;
+  std::vector<Slice> slices;                 // every group's slices, group after group
+  std::map<unsigned, EnsembleGraph> graphs;  // one RK4 step of the groups in the mask
+  double* energy = nullptr;                  // per-member energies of the diagnostic
+  double* energy_partials = nullptr;         // members x blocks partial sums of them
   size_t energy_partials_size = 0;
   std::vector<TriskModel*> models;
   std::vector<void*> allocations;
@@ -350,16 +403,15 @@ struct TriskEnsemble {
   double* staging = nullptr;
   int64_t max_state = 0;
   int max_members = 0;
-  cudaGraphExec_t graph = nullptr;
   int64_t launches = 0;
-  int64_t graph_kernels = 0;
   double step_bytes = 0;
 
   ~TriskEnsemble() {
     int prev = -1;
     cudaGetDevice(&prev);
     cudaSetDevice(device);
-    if (graph) cudaGraphExecDestroy(graph);
+    for (auto& kv : graphs)
+      if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
     if (caller_ev) cudaEventDestroy(caller_ev);
     if (stream) {
       cudaStreamSynchronize(stream);
@@ -378,6 +430,10 @@ struct TriskEnsemble {
   size_t esize() const { return fp32 ? sizeof(float) : sizeof(double); }
   // a state or work vector of `count` elements of the storage type, kept as double*
   double* alloc_state(size_t count) { return reinterpret_cast<double*>(alloc<char>(count * esize())); }
+  // element `count` of a storage-type buffer kept as double*
+  double* at(double* p, int64_t count) const {
+    return p ? reinterpret_cast<double*>(reinterpret_cast<char*>(p) + count * (int64_t)esize()) : nullptr;
+  }
 };
 
 namespace {
@@ -411,10 +467,139 @@ void with_real(const TriskEnsemble& e, F&& f) {
     f(double{});
 }
 
+// The default members per slice of a group: the candidate M, M/2, M/4, ... that minimizes a
+// byte estimate per stage, (slices) T + M f max(0, 1 - B / (S f)): every slice streams the
+// tables T once, and the part of a slice's state and work vectors (f per member) beyond the
+// L2 budget B goes to DRAM and back.
+int default_slice(int M, double T, double f) {
+  int best = M;
+  double best_cost = INFINITY;
+  for (int S = M; S >= 1; S = S > 1 ? (S + 1) / 2 : 0) {
+    const double slices = std::ceil((double)M / S);
+    const double cost = slices * T + (double)M * f * std::max(0.0, 1.0 - SLICE_L2_BUDGET / (S * f));
+    if (cost < best_cost * 0.999) {
+      best_cost = cost;
+      best = S;
+    }
+    if (S == 1) break;
+  }
+  return best;
+}
+
+// The slices of every group for its current S: descriptors pointing into the group's buffers.
+void build_slices(TriskEnsemble& e) {
+  e.slices.clear();
+  for (int g = 0; g < (int)e.groups.size(); ++g) {
+    EnsembleGroup& G = e.groups[g];
+    const TriskModel& m = *G.m;
+    for (int m0 = 0; m0 < G.M; m0 += G.S) {
+      Slice sl{};
+      sl.group = g;
+      sl.m0 = m0;
+      GroupDesc& D = sl.D;
+      const int Ms = std::min(G.S, G.M - m0);
+      D.T = m.T;
+      D.M = Ms;
+      D.dt = G.dt;
+      D.nsteps = G.nsteps;
+      D.counter = e.counters + g;
+      D.y = e.at(G.y, m.N * m0);
+      D.acc = e.at(G.acc, m.N * m0);
+      D.st = e.at(G.st, m.N * m0);
+      D.W.K = e.at(G.W.K, m.nc * m0);
+      D.W.B = e.at(G.W.B, m.nc * m0);
+      D.W.F = e.at(G.W.F, m.ne * m0);
+      D.W.qe = e.at(G.W.qe, m.ne * m0);
+      D.W.zv = e.at(G.W.zv, m.nv * m0);
+      D.W.hv = e.at(G.W.hv, m.nv * m0);
+      D.W.qv = e.at(G.W.qv, m.nv * m0);
+      D.W.Kv = e.at(G.W.Kv, m.nv * m0);
+      if (G.cl.net) {
+        D.W.dq = e.at(G.cl.dq, m.ne * m0);
+        D.W.dF = e.at(G.cl.dF, m.ne * m0);
+      }
+      D.P = Ms % 2 == 0 ? 2 : 1;
+      e.slices.push_back(sl);
+    }
+  }
+}
+
+void drop_graphs(TriskEnsemble& e) {
+  for (auto& kv : e.graphs)
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+  e.graphs.clear();
+}
+
+// Launch sets of the slices of the groups in `mask`: slices in order, a set taking slices
+// while their state and work vectors stay within the L2 budget (and at most MAX_SET of them);
+// each slice's virtual blocks per phase for the current block sizes.
+std::vector<GroupSet> launch_sets(TriskEnsemble& e, unsigned mask, std::vector<std::vector<int>>* members) {
+  std::vector<GroupSet> sets;
+  GroupSet cur{};
+  double bytes = 0;
+  auto close = [&]() {
+    if (cur.n) sets.push_back(cur);
+    cur = GroupSet{};
+    cur.flag = e.flag;
+    bytes = 0;
+  };
+  close();
+  if (members) members->clear();
+  std::vector<int> cur_members;
+  for (int k = 0; k < (int)e.slices.size(); ++k) {
+    const Slice& sl = e.slices[k];
+    if (!((mask >> sl.group) & 1u)) continue;
+    const EnsembleGroup& G = e.groups[sl.group];
+    const double b = G.member_bytes * sl.D.M;
+    if (cur.n == MAX_SET || (cur.n > 0 && bytes + b > SLICE_L2_BUDGET)) {
+      close();
+      if (members) members->push_back(cur_members);
+      cur_members.clear();
+    }
+    GroupDesc D = sl.D;
+    const TriskModel& m = *G.m;
+    const int64_t M = D.M;
+    D.nV = (int)cdiv(m.nv * M / D.P, e.block[0]);
+    D.nEF = (int)cdiv(m.ne * M / D.P, e.block[1]);
+    D.nCF = (int)cdiv(m.nc * M / D.P, e.block[1]);
+    D.nET = (int)cdiv(m.ne * M / D.P, e.block[2]);
+    D.nCT = (int)cdiv(m.nc * M / D.P, e.block[2]);
+    D.startV = cur.totalV;
+    D.startF = cur.totalF;
+    D.startT = cur.totalT;
+    cur.totalV += D.nV;
+    cur.totalF += D.nEF + D.nCF;
+    cur.totalT += D.nET + D.nCT;
+    cur.g[cur.n++] = D;
+    cur_members.push_back(k);
+    bytes += b;
+  }
+  if (cur.n) {
+    sets.push_back(cur);
+    if (members) members->push_back(cur_members);
+  }
+  return sets;
+}
+
+// Resident blocks per SM of the three phases for the current block sizes.
+void layout(TriskEnsemble& e) {
+  CUDA_CHECK(cudaDeviceGetAttribute(&e.sms, cudaDevAttrMultiProcessorCount, e.device));
+  with_modes_e(e.pv, e.ke, [&](auto pvc, auto kec) {
+    constexpr int PV = decltype(pvc)::value, KE = decltype(kec)::value;
+    with_real(e, [&](auto r) {
+      using R = decltype(r);
+      CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&e.occ[0], kg_vertex<PV, KE, R>, e.block[0], 0));
+      CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&e.occ[1], kg_flux<PV, KE, R>, e.block[1], 0));
+      CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&e.occ[2], kg_tend<PV, EPI_STAGE2, R>, e.block[2], 0));
+    });
+  });
+  drop_graphs(e);
+}
+
 template <typename... KArgs, typename... Args>
-void elaunch(TriskEnsemble& e, void (*kernel)(KArgs...), int phase, bool pdl, Args&&... args) {
+void elaunch(TriskEnsemble& e, void (*kernel)(KArgs...), int phase, int total, bool pdl, Args&&... args) {
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((unsigned)e.grid[phase]);
+  cfg.gridDim = dim3((unsigned)std::max(1, std::min(total, e.sms * std::max(e.occ[phase], 1))));
   cfg.blockDim = dim3((unsigned)e.block[phase]);
   cfg.stream = e.stream;
   cudaLaunchAttribute attr[1];
@@ -426,38 +611,42 @@ void elaunch(TriskEnsemble& e, void (*kernel)(KArgs...), int phase, bool pdl, Ar
   e.launches++;
 }
 
-// One RK4 step of every unfinished group. The first phase of a step and the counter update
-// wait for the full completion of the launch before them (no PDL): both depend on, or
-// change, the step counters the others read.
-// The closure of every group that has one, after the flux phase of `stage`: features and
-// the network (at stage 1, or at every stage), then the corrections of F and du.
-void enqueue_closure(TriskEnsemble& e, int stage) {
-  for (int g = 0; g < e.G.n; ++g) {
-    ClosureSlot& c = e.cl[g];
+// The closure of every slice of the set whose group has one, after the flux phase of `stage`:
+// features and the network (at stage 1, or at every stage), then the corrections of F and du.
+void enqueue_closure(TriskEnsemble& e, const std::vector<int>& set_slices, int stage) {
+  for (int k : set_slices) {
+    const Slice& sl = e.slices[k];
+    EnsembleGroup& G = e.groups[sl.group];
+    ClosureSlot& c = G.cl;
     if (!c.net) continue;
-    const GroupDesc& D = e.G.g[g];
-    const int64_t rows = (int64_t)D.T.ne * D.M;
-    const unsigned nb = (unsigned)cdiv(rows, 256);
     if (stage != 1 && !c.every_stage) continue;
+    const GroupDesc& D = sl.D;
+    const int64_t ne = D.T.ne;
+    const int64_t rows = ne * D.M;
+    const int64_t r0 = ne * sl.m0;  // the slice's first row
+    const unsigned nb = (unsigned)cdiv(rows, 256);
+    __nv_bfloat16* X = c.X + r0 * NFEAT;
+    float* Y = c.Y + 2 * r0;
     with_real(e, [&](auto r) {
       using R = decltype(r);
-      kg_features<R><<<nb, 256, 0, e.stream>>>(D.T, work_as<R>(D.W),
-                                               reinterpret_cast<const R*>(stage == 1 ? D.y : D.st), D.M, c.geom,
-                                               c.norm, c.X, nullptr, rows);
+      R* dF = reinterpret_cast<R*>(e.at(c.dF, r0));
+      R* dq = reinterpret_cast<R*>(e.at(c.dq, r0));
+      const R* ys = reinterpret_cast<const R*>(stage == 1 ? D.y : D.st);
+      kg_features<R><<<nb, 256, 0, e.stream>>>(D.T, work_as<R>(D.W), ys, D.M, c.geom, c.norm, X, nullptr, rows, G.M,
+                                               sl.m0);
       CUDA_CHECK(cudaGetLastError());
-      closure_forward_on(c.net, c.X, rows, c.Y, e.stream);
-      kg_closure_apply<R><<<nb, 256, 0, e.stream>>>(reinterpret_cast<R*>(c.dF), reinterpret_cast<R*>(c.dq), c.Y,
-                                                    c.member_on, rows, D.M, c.norm.out_scale[0],
+      closure_forward_on(c.net, X, rows, Y, e.stream);
+      kg_closure_apply<R><<<nb, 256, 0, e.stream>>>(dF, dq, Y, c.member_on + sl.m0, rows, D.M, c.norm.out_scale[0],
                                                     c.norm.out_scale[1]);
       CUDA_CHECK(cudaGetLastError());
       if (c.work_free) {
-        const R* ys = reinterpret_cast<const R*>(stage == 1 ? D.y : D.st);
-        const int nx = (int)std::min<int64_t>(cdiv(D.T.ne, 8), WORK_SUM_BLOCKS);
+        double* sums = c.sums + 2 * sl.m0;
+        double* partials = c.partials + 2 * (int64_t)sl.m0 * WORK_SUM_BLOCKS;
+        const int nx = (int)std::min<int64_t>(cdiv(ne, 8), WORK_SUM_BLOCKS);
         const dim3 grid((unsigned)nx, (unsigned)cdiv(D.M, 32));
-        kg_work_sums<R><<<grid, dim3(32, 8), 0, e.stream>>>(D.T, ys, reinterpret_cast<const R*>(c.dq), c.geom, D.M,
-                                                             c.partials);
-        kg_sum_rows<<<(unsigned)(2 * D.M), 256, 0, e.stream>>>(c.partials, nx, c.sums);
-        kg_work_project<R><<<nb, 256, 0, e.stream>>>(D.T, ys, reinterpret_cast<R*>(c.dq), c.geom, D.M, rows, c.sums);
+        kg_work_sums<R><<<grid, dim3(32, 8), 0, e.stream>>>(D.T, ys, dq, c.geom, D.M, partials);
+        kg_sum_rows<<<(unsigned)(2 * D.M), 256, 0, e.stream>>>(partials, nx, sums);
+        kg_work_project<R><<<nb, 256, 0, e.stream>>>(D.T, ys, dq, c.geom, D.M, rows, sums);
         CUDA_CHECK(cudaGetLastError());
         e.launches += 3;
       }
@@ -466,43 +655,45 @@ void enqueue_closure(TriskEnsemble& e, int stage) {
   }
 }
 
-bool any_closure(const TriskEnsemble& e) {
-  for (int g = 0; g < e.G.n; ++g)
-    if (e.cl[g].net) return true;
-  return false;
-}
-
-void enqueue_ensemble_step(TriskEnsemble& e) {
-  const bool closure = any_closure(e);
+// One RK4 step of the groups in `mask`: per stage, the three phases of every launch set in
+// turn. The first launch of a step waits for the full completion of the launch before it
+// (no PDL): the step counters it reads were just advanced.
+void enqueue_ensemble_step(TriskEnsemble& e, unsigned mask) {
+  std::vector<std::vector<int>> members;
+  const std::vector<GroupSet> sets = launch_sets(e, mask, &members);
   with_modes_e(e.pv, e.ke, [&](auto pvc, auto kec) {
     constexpr int PV = decltype(pvc)::value, KE = decltype(kec)::value;
     for (int stage = 1; stage <= 4; ++stage) {
-      with_real(e, [&](auto r) {
-        using R = decltype(r);
-        elaunch(e, kg_vertex<PV, KE, R>, 0, stage != 1, e.G, stage == 1 ? 1 : 0);
-        elaunch(e, kg_flux<PV, KE, R>, 1, true, e.G, stage == 1 ? 1 : 0, 0);
-        if (closure) enqueue_closure(e, stage);
-        switch (stage) {
-          case 1: elaunch(e, kg_tend<PV, EPI_STAGE1, R>, 2, true, e.G); break;
-          case 2: elaunch(e, kg_tend<PV, EPI_STAGE2, R>, 2, true, e.G); break;
-          case 3: elaunch(e, kg_tend<PV, EPI_STAGE3, R>, 2, true, e.G); break;
-          default: elaunch(e, kg_tend<PV, EPI_STAGE4, R>, 2, true, e.G); break;
-        }
-      });
+      for (size_t k = 0; k < sets.size(); ++k) {
+        const GroupSet& G = sets[k];
+        with_real(e, [&](auto r) {
+          using R = decltype(r);
+          elaunch(e, kg_vertex<PV, KE, R>, 0, G.totalV, !(stage == 1 && k == 0), G, stage == 1 ? 1 : 0);
+          elaunch(e, kg_flux<PV, KE, R>, 1, G.totalF, true, G, stage == 1 ? 1 : 0, 0);
+          enqueue_closure(e, members[k], stage);
+          switch (stage) {
+            case 1: elaunch(e, kg_tend<PV, EPI_STAGE1, R>, 2, G.totalT, true, G); break;
+            case 2: elaunch(e, kg_tend<PV, EPI_STAGE2, R>, 2, G.totalT, true, G); break;
+            case 3: elaunch(e, kg_tend<PV, EPI_STAGE3, R>, 2, G.totalT, true, G); break;
+            default: elaunch(e, kg_tend<PV, EPI_STAGE4, R>, 2, G.totalT, true, G); break;
+          }
+        });
+      }
     }
   });
-  kg_advance<<<1, 32, 0, e.stream>>>(e.counters, e.G.n);
+  kg_advance<<<1, 32, 0, e.stream>>>(e.counters, mask);
   CUDA_CHECK(cudaGetLastError());
   e.launches++;
 }
 
-void ensure_ensemble_graph(TriskEnsemble& e) {
-  if (e.graph) return;
+EnsembleGraph& ensure_graph(TriskEnsemble& e, unsigned mask) {
+  auto it = e.graphs.find(mask);
+  if (it != e.graphs.end()) return it->second;
   const int64_t before = e.launches;
   cudaGraph_t g = nullptr;
   CUDA_CHECK(cudaStreamBeginCapture(e.stream, cudaStreamCaptureModeThreadLocal));
   try {
-    enqueue_ensemble_step(e);
+    enqueue_ensemble_step(e, mask);
   } catch (...) {
     cudaStreamEndCapture(e.stream, &g);
     if (g) cudaGraphDestroy(g);
@@ -510,57 +701,38 @@ void ensure_ensemble_graph(TriskEnsemble& e) {
     throw;
   }
   CUDA_CHECK(cudaStreamEndCapture(e.stream, &g));
-  e.graph_kernels = e.launches - before;  // counted again at every replay
+  EnsembleGraph eg;
+  eg.kernels = e.launches - before;  // counted again at every replay
   e.launches = before;
-  cudaError_t err = cudaGraphInstantiate(&e.graph, g, 0);
+  cudaError_t err = cudaGraphInstantiate(&eg.exec, g, 0);
   cudaGraphDestroy(g);
   CUDA_CHECK(err);
+  return e.graphs[mask] = eg;
 }
 
-void drop_graph(TriskEnsemble& e) {
-  if (e.graph) {
-    cudaGraphExecDestroy(e.graph);
-    e.graph = nullptr;
+// `steps` RK4 steps: each replay advances every unfinished group by one step, so the host
+// knows which groups a replay advances and replays the graph of exactly those groups.
+void run_steps(TriskEnsemble& e, int64_t steps) {
+  while (steps > 0) {
+    unsigned mask = 0;
+    int64_t k = steps;
+    for (int g = 0; g < (int)e.groups.size(); ++g) {
+      const EnsembleGroup& G = e.groups[g];
+      if (G.taken < G.nsteps) {
+        mask |= 1u << g;
+        k = std::min<int64_t>(k, G.nsteps - G.taken);
+      }
+    }
+    if (!mask) break;  // every group has taken its steps
+    EnsembleGraph& eg = ensure_graph(e, mask);
+    for (int64_t s = 0; s < k; ++s) {
+      CUDA_CHECK(cudaGraphLaunch(eg.exec, e.stream));
+      e.launches += eg.kernels;
+    }
+    for (int g = 0; g < (int)e.groups.size(); ++g)
+      if ((mask >> g) & 1u) e.groups[g].taken += k;
+    steps -= k;
   }
-}
-
-// Virtual blocks of every group per phase for the current block sizes, and the persistent
-// grids (as many blocks as stay resident, never more than the work).
-void layout(TriskEnsemble& e) {
-  int sV = 0, sF = 0, sT = 0;
-  for (int g = 0; g < e.G.n; ++g) {
-    GroupDesc& D = e.G.g[g];
-    const TriskModel& m = *e.models[g];
-    const int64_t M = D.M;
-    D.nV = (int)cdiv(m.nv * M / D.P, e.block[0]);
-    D.nEF = (int)cdiv(m.ne * M / D.P, e.block[1]);
-    D.nCF = (int)cdiv(m.nc * M / D.P, e.block[1]);
-    D.nET = (int)cdiv(m.ne * M / D.P, e.block[2]);
-    D.nCT = (int)cdiv(m.nc * M / D.P, e.block[2]);
-    D.startV = sV;
-    D.startF = sF;
-    D.startT = sT;
-    sV += D.nV;
-    sF += D.nEF + D.nCF;
-    sT += D.nET + D.nCT;
-  }
-  e.G.totalV = sV;
-  e.G.totalF = sF;
-  e.G.totalT = sT;
-  int dev_sms = 0;
-  CUDA_CHECK(cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, e.device));
-  int occ[3] = {1, 1, 1};
-  with_modes_e(e.pv, e.ke, [&](auto pvc, auto kec) {
-    constexpr int PV = decltype(pvc)::value, KE = decltype(kec)::value;
-    with_real(e, [&](auto r) {
-      using R = decltype(r);
-      CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[0], kg_vertex<PV, KE, R>, e.block[0], 0));
-      CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[1], kg_flux<PV, KE, R>, e.block[1], 0));
-      CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[2], kg_tend<PV, EPI_STAGE2, R>, e.block[2], 0));
-    });
-  });
-  const int total[3] = {sV, sF, sT};
-  for (int p = 0; p < 3; ++p) e.grid[p] = std::max(1, std::min(total[p], dev_sms * std::max(occ[p], 1)));
 }
 
 TriskEnsemble* checked_e(TriskEnsemble* e) {
@@ -568,10 +740,46 @@ TriskEnsemble* checked_e(TriskEnsemble* e) {
   return e;
 }
 
-const GroupDesc& group_at(TriskEnsemble& e, int g, int member) {
-  if (g < 0 || g >= e.G.n) throw Error(TRISK_ERR_ARGUMENT, "group out of range");
-  if (member < 0 || member >= e.G.g[g].M) throw Error(TRISK_ERR_ARGUMENT, "member out of range");
-  return e.G.g[g];
+// the slice holding member `member` of group g
+const Slice& slice_of(TriskEnsemble& e, int g, int member) {
+  if (g < 0 || g >= (int)e.groups.size()) throw Error(TRISK_ERR_ARGUMENT, "group out of range");
+  if (member < 0 || member >= e.groups[g].M) throw Error(TRISK_ERR_ARGUMENT, "member out of range");
+  for (const Slice& sl : e.slices)
+    if (sl.group == g && member >= sl.m0 && member < sl.m0 + sl.D.M) return sl;
+  throw Error(TRISK_ERR_ARGUMENT, "member out of range");
+}
+
+EnsembleGroup& group_ref(TriskEnsemble& e, int g) {
+  if (g < 0 || g >= (int)e.groups.size()) throw Error(TRISK_ERR_ARGUMENT, "group out of range");
+  return e.groups[g];
+}
+
+// A group's state from slices of S_from members to S_to (through a temporary copy).
+void relayout_group(TriskEnsemble& e, EnsembleGroup& G, const double* from, int S_from, int S_to) {
+  const int64_t n = G.m->N * (int64_t)G.M;
+  with_real(e, [&](auto r) {
+    using R = decltype(r);
+    kg_relayout<R><<<(unsigned)cdiv(n, 256), 256, 0, e.stream>>>(reinterpret_cast<R*>(G.y),
+                                                                 reinterpret_cast<const R*>(from), G.m->N, G.M,
+                                                                 S_from, S_to);
+  });
+  CUDA_CHECK(cudaGetLastError());
+}
+
+// Changes group g to slices of S members, keeping every member's state.
+void reslice(TriskEnsemble& e, int g, int S) {
+  EnsembleGroup& G = e.groups[g];
+  if (S == G.S) return;
+  const int64_t n = G.m->N * (int64_t)G.M;
+  double* tmp = nullptr;
+  CUDA_CHECK(cudaMallocAsync((void**)&tmp, n * e.esize(), e.stream));
+  CUDA_CHECK(cudaMemcpyAsync(tmp, G.y, n * e.esize(), cudaMemcpyDeviceToDevice, e.stream));
+  relayout_group(e, G, tmp, G.S, S);
+  CUDA_CHECK(cudaFreeAsync(tmp, e.stream));
+  CUDA_CHECK(cudaStreamSynchronize(e.stream));
+  G.S = S;
+  build_slices(e);
+  drop_graphs(e);
 }
 
 }  // namespace
@@ -602,6 +810,8 @@ int trisk_ensemble_create_precision(TriskModel* const* models, const int32_t* me
   DeviceGuard guard(e->device);
   CUDA_CHECK(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
   CUDA_CHECK(cudaEventCreateWithFlags(&e->caller_ev, cudaEventDisableTiming));
+  e->counters = e->alloc<int>(MAX_GROUPS);
+  e->flag = e->alloc<int>(1);
   for (int g = 0; g < ngroups; ++g) {
     TriskModel* m = models[g];
     if (!m) throw Error(TRISK_ERR_ARGUMENT, "model is NULL");
@@ -612,38 +822,36 @@ int trisk_ensemble_create_precision(TriskModel* const* models, const int32_t* me
       throw Error(TRISK_ERR_ARGUMENT, "bad dt or step count");
     const int64_t M = members[g];
     if ((m->ne + m->nc) * M >= (1LL << 31)) throw Error(TRISK_ERR_UNSUPPORTED, "group too large");
-    GroupDesc& D = e->G.g[g];
-    D.T = m->T;
-    D.M = (int)M;
-    D.dt = dt[g];
-    D.nsteps = (int)nsteps[g];
-    D.W.K = e->alloc_state(m->nc * M);
-    D.W.B = e->alloc_state(m->nc * M);
-    D.W.F = e->alloc_state(m->ne * M);
-    D.W.qe = e->alloc_state(m->ne * M);
-    D.W.zv = e->alloc_state(m->nv * M);
-    D.W.hv = e->alloc_state(m->nv * M);
-    D.W.qv = e->alloc_state(m->nv * M);
-    D.W.Kv = e->alloc_state(m->nv * M);
-    D.y = e->alloc_state(m->N * M);
-    D.acc = e->alloc_state(m->N * M);
-    D.st = e->alloc_state(m->N * M);
-    CUDA_CHECK(cudaMemset(D.y, 0, m->N * M * e->esize()));
-    D.P = M % 2 == 0 ? 2 : 1;
+    EnsembleGroup G;
+    G.m = m;
+    G.M = (int)M;
+    G.dt = dt[g];
+    G.nsteps = (int)nsteps[g];
+    G.W.K = e->alloc_state(m->nc * M);
+    G.W.B = e->alloc_state(m->nc * M);
+    G.W.F = e->alloc_state(m->ne * M);
+    G.W.qe = e->alloc_state(m->ne * M);
+    G.W.zv = e->alloc_state(m->nv * M);
+    G.W.hv = e->alloc_state(m->nv * M);
+    G.W.qv = e->alloc_state(m->nv * M);
+    G.W.Kv = e->alloc_state(m->nv * M);
+    G.y = e->alloc_state(m->N * M);
+    G.acc = e->alloc_state(m->N * M);
+    G.st = e->alloc_state(m->N * M);
+    CUDA_CHECK(cudaMemset(G.y, 0, m->N * M * e->esize()));
+    G.member_bytes = (double)e->esize() * (3.0 * m->N + 2.0 * m->nc + 2.0 * m->ne + 4.0 * m->nv);
+    G.S = default_slice(G.M, m->table_bytes_unique, G.member_bytes);
+    e->groups.push_back(G);
     e->models.push_back(m);
     e->max_state = std::max(e->max_state, m->N);
     e->max_members = std::max(e->max_members, (int)M);
     const double Nb = (double)e->esize() * (double)m->N * M;
     e->step_bytes += 4 * (m->table_bytes_unique + 2 * Nb) + 15 * Nb;
   }
-  e->G.n = ngroups;
-  e->counters = e->alloc<int>(MAX_GROUPS);
-  e->flag = e->alloc<int>(1);
   e->staging = e->alloc<double>(e->max_state);
   CUDA_CHECK(cudaMemset(e->counters, 0, MAX_GROUPS * sizeof(int)));
   CUDA_CHECK(cudaMemset(e->flag, 0, sizeof(int)));
-  e->G.counters = e->counters;
-  e->G.flag = e->flag;
+  build_slices(*e);
   layout(*e);
   CUDA_CHECK(cudaDeviceSynchronize());
   *out = e.release();
@@ -656,7 +864,7 @@ int trisk_ensemble_set_member(TriskEnsemble* ens, int32_t group, int32_t member,
   TRISK_API_BEGIN
   TriskEnsemble& e = *checked_e(ens);
   if (!y) throw Error(TRISK_ERR_ARGUMENT, "NULL state");
-  const GroupDesc& D = group_at(e, group, member);
+  const Slice& sl = slice_of(e, group, member);
   TriskModel& m = *e.models[group];
   DeviceGuard guard(e.device);
   const double* src = y;
@@ -668,8 +876,8 @@ int trisk_ensemble_set_member(TriskEnsemble* ens, int32_t group, int32_t member,
   }
   with_real(e, [&](auto r) {
     using R = decltype(r);
-    kg_scatter_member<R><<<(unsigned)cdiv(m.N, 256), 256, 0, e.stream>>>(reinterpret_cast<R*>(D.y), src,
-                                                                         m.state_n2o, m.N, D.M, member);
+    kg_scatter_member<R><<<(unsigned)cdiv(m.N, 256), 256, 0, e.stream>>>(reinterpret_cast<R*>(sl.D.y), src,
+                                                                         m.state_n2o, m.N, sl.D.M, member - sl.m0);
   });
   CUDA_CHECK(cudaGetLastError());
   CUDA_CHECK(cudaStreamSynchronize(e.stream));
@@ -680,7 +888,7 @@ int trisk_ensemble_get_member(TriskEnsemble* ens, int32_t group, int32_t member,
   TRISK_API_BEGIN
   TriskEnsemble& e = *checked_e(ens);
   if (!y) throw Error(TRISK_ERR_ARGUMENT, "NULL state");
-  const GroupDesc& D = group_at(e, group, member);
+  const Slice& sl = slice_of(e, group, member);
   TriskModel& m = *e.models[group];
   DeviceGuard guard(e.device);
   const bool dev = is_device_pointer(y);
@@ -688,8 +896,8 @@ int trisk_ensemble_get_member(TriskEnsemble* ens, int32_t group, int32_t member,
   if (dev) order_after_caller(e.stream, e.caller_ev);
   with_real(e, [&](auto r) {
     using R = decltype(r);
-    kg_gather_member<R><<<(unsigned)cdiv(m.N, 256), 256, 0, e.stream>>>(dst, reinterpret_cast<const R*>(D.y),
-                                                                        m.state_o2n, m.N, D.M, member);
+    kg_gather_member<R><<<(unsigned)cdiv(m.N, 256), 256, 0, e.stream>>>(
+        dst, reinterpret_cast<const R*>(sl.D.y), m.state_o2n, m.N, sl.D.M, member - sl.m0);
   });
   CUDA_CHECK(cudaGetLastError());
   if (!dev) CUDA_CHECK(cudaMemcpyAsync(y, e.staging, m.N * sizeof(double), cudaMemcpyDeviceToHost, e.stream));
@@ -702,11 +910,7 @@ int trisk_ensemble_run_async(TriskEnsemble* ens, int64_t steps) {
   TriskEnsemble& e = *checked_e(ens);
   if (steps < 0) throw Error(TRISK_ERR_ARGUMENT, "steps must be non-negative");
   DeviceGuard guard(e.device);
-  ensure_ensemble_graph(e);
-  for (int64_t s = 0; s < steps; ++s) {
-    CUDA_CHECK(cudaGraphLaunch(e.graph, e.stream));
-    e.launches += e.graph_kernels;
-  }
+  run_steps(e, steps);
   TRISK_API_END
 }
 
@@ -732,7 +936,7 @@ int trisk_ensemble_steps(TriskEnsemble* ens, int64_t* steps_taken) {
   int c[MAX_GROUPS] = {0};
   CUDA_CHECK(cudaMemcpyAsync(c, e.counters, sizeof(c), cudaMemcpyDeviceToHost, e.stream));
   CUDA_CHECK(cudaStreamSynchronize(e.stream));
-  for (int g = 0; g < e.G.n; ++g) steps_taken[g] = std::min<int64_t>(c[g], e.G.g[g].nsteps);
+  for (int g = 0; g < (int)e.groups.size(); ++g) steps_taken[g] = std::min<int64_t>(c[g], e.groups[g].nsteps);
   TRISK_API_END
 }
 
@@ -742,6 +946,7 @@ int trisk_ensemble_reset(TriskEnsemble* ens) {
   DeviceGuard guard(e.device);
   CUDA_CHECK(cudaMemsetAsync(e.counters, 0, MAX_GROUPS * sizeof(int), e.stream));
   CUDA_CHECK(cudaStreamSynchronize(e.stream));
+  for (EnsembleGroup& G : e.groups) G.taken = 0;
   TRISK_API_END
 }
 
@@ -766,7 +971,6 @@ int trisk_ensemble_set_block(TriskEnsemble* ens, const int32_t block[3]) {
   CUDA_CHECK(cudaStreamSynchronize(e.stream));
   for (int p = 0; p < 3; ++p) e.block[p] = block[p];
   layout(e);
-  drop_graph(e);
   TRISK_API_END
 }
 
@@ -778,6 +982,27 @@ int trisk_ensemble_get_block(TriskEnsemble* ens, int32_t block[3]) {
   TRISK_API_END
 }
 
+int trisk_ensemble_set_slices(TriskEnsemble* ens, const int32_t* members_per_slice) {
+  TRISK_API_BEGIN
+  TriskEnsemble& e = *checked_e(ens);
+  if (!members_per_slice) throw Error(TRISK_ERR_ARGUMENT, "NULL argument");
+  for (int g = 0; g < (int)e.groups.size(); ++g)
+    if (members_per_slice[g] < 1 || members_per_slice[g] > e.groups[g].M)
+      throw Error(TRISK_ERR_ARGUMENT, "members per slice must be in 1..members of the group");
+  DeviceGuard guard(e.device);
+  CUDA_CHECK(cudaStreamSynchronize(e.stream));
+  for (int g = 0; g < (int)e.groups.size(); ++g) reslice(e, g, members_per_slice[g]);
+  TRISK_API_END
+}
+
+int trisk_ensemble_get_slices(TriskEnsemble* ens, int32_t* members_per_slice) {
+  TRISK_API_BEGIN
+  TriskEnsemble& e = *checked_e(ens);
+  if (!members_per_slice) throw Error(TRISK_ERR_ARGUMENT, "NULL argument");
+  for (int g = 0; g < (int)e.groups.size(); ++g) members_per_slice[g] = e.groups[g].S;
+  TRISK_API_END
+}
+
 int trisk_ensemble_autotune(TriskEnsemble* ens, int32_t steps, double* best_ms) {
   TRISK_API_BEGIN
   TriskEnsemble& e = *checked_e(ens);
@@ -785,31 +1010,54 @@ int trisk_ensemble_autotune(TriskEnsemble* ens, int32_t steps, double* best_ms) 
   DeviceGuard guard(e.device);
   CUDA_CHECK(cudaStreamSynchronize(e.stream));
   // Times `steps` RK4 steps of all groups for every combination of the three phases' block
-  // sizes and keeps the fastest. The members' states, the step counters and each group's
-  // step count are saved first and restored after every trial and at the end, so the
-  // ensemble continues as if nothing had run (every candidate computes the same numbers).
+  // sizes, then for the members per slice of each group in turn (S, S/2, S/4 ... and 2 S ..
+  // up to the group), and keeps the fastest. The members' states (in the slicing they had),
+  // the step counters and each group's step count are saved first and restored after every
+  // trial and at the end, so the ensemble continues as if nothing had run (every candidate
+  // computes the same numbers).
   static const int choices[] = {64, 128, 256};
-  std::vector<double*> saved(e.G.n);
-  std::vector<int> nsteps(e.G.n);
+  const int ng = (int)e.groups.size();
+  std::vector<double*> saved(ng);
+  std::vector<int> nsteps(ng), S0(ng);
+  std::vector<int64_t> taken(ng);
   std::vector<int> counters(MAX_GROUPS);
   CUDA_CHECK(cudaMemcpy(counters.data(), e.counters, MAX_GROUPS * sizeof(int), cudaMemcpyDeviceToHost));
-  for (int g = 0; g < e.G.n; ++g) {
-    const size_t bytes = (size_t)e.models[g]->N * e.G.g[g].M * e.esize();
+  for (int g = 0; g < ng; ++g) {
+    EnsembleGroup& G = e.groups[g];
+    const size_t bytes = (size_t)G.m->N * G.M * e.esize();
     saved[g] = reinterpret_cast<double*>(e.alloc<char>(bytes));  // freed with the ensemble
-    CUDA_CHECK(cudaMemcpyAsync(saved[g], e.G.g[g].y, bytes, cudaMemcpyDeviceToDevice, e.stream));
-    nsteps[g] = e.G.g[g].nsteps;
-    e.G.g[g].nsteps = steps + 2;  // every group takes part in every timed step
+    CUDA_CHECK(cudaMemcpyAsync(saved[g], G.y, bytes, cudaMemcpyDeviceToDevice, e.stream));
+    nsteps[g] = G.nsteps;
+    taken[g] = G.taken;
+    S0[g] = G.S;
+    G.nsteps = steps + 2;  // every group takes part in every timed step
   }
-  auto restore = [&]() {
-    for (int g = 0; g < e.G.n; ++g) {
-      const size_t bytes = (size_t)e.models[g]->N * e.G.g[g].M * e.esize();
-      CUDA_CHECK(cudaMemcpyAsync(e.G.g[g].y, saved[g], bytes, cudaMemcpyDeviceToDevice, e.stream));
-    }
+  auto restore = [&]() {  // the saved states in the current slicing, counters at zero
+    for (int g = 0; g < ng; ++g) relayout_group(e, e.groups[g], saved[g], S0[g], e.groups[g].S);
     CUDA_CHECK(cudaMemsetAsync(e.counters, 0, MAX_GROUPS * sizeof(int), e.stream));
+    for (EnsembleGroup& G : e.groups) G.taken = 0;
+  };
+  auto set_slicing = [&](int g, int S) {  // no state to keep: restore() rewrites it
+    e.groups[g].S = S;
+    build_slices(e);
+    drop_graphs(e);
   };
   cudaEvent_t e0, e1;
   CUDA_CHECK(cudaEventCreate(&e0));
   CUDA_CHECK(cudaEventCreate(&e1));
+  auto trial = [&]() {
+    restore();
+    build_slices(e);  // the step counts changed
+    drop_graphs(e);
+    run_steps(e, 2);  // warm-up (and the graph's capture)
+    CUDA_CHECK(cudaEventRecord(e0, e.stream));
+    run_steps(e, steps);
+    CUDA_CHECK(cudaEventRecord(e1, e.stream));
+    CUDA_CHECK(cudaEventSynchronize(e1));
+    float ms = 0;
+    CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+    return (double)ms;
+  };
   int best[3] = {e.block[0], e.block[1], e.block[2]};
   double best_t = INFINITY;
   try {
@@ -820,16 +1068,7 @@ int trisk_ensemble_autotune(TriskEnsemble* ens, int32_t steps, double* best_ms) 
           e.block[1] = b;
           e.block[2] = c;
           layout(e);
-          drop_graph(e);
-          restore();
-          ensure_ensemble_graph(e);
-          for (int s2 = 0; s2 < 2; ++s2) CUDA_CHECK(cudaGraphLaunch(e.graph, e.stream));  // warm-up
-          CUDA_CHECK(cudaEventRecord(e0, e.stream));
-          for (int s2 = 0; s2 < steps; ++s2) CUDA_CHECK(cudaGraphLaunch(e.graph, e.stream));
-          CUDA_CHECK(cudaEventRecord(e1, e.stream));
-          CUDA_CHECK(cudaEventSynchronize(e1));
-          float ms = 0;
-          CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+          const double ms = trial();
           if (ms < best_t) {
             best_t = ms;
             best[0] = a;
@@ -837,6 +1076,28 @@ int trisk_ensemble_autotune(TriskEnsemble* ens, int32_t steps, double* best_ms) 
             best[2] = c;
           }
         }
+    for (int p = 0; p < 3; ++p) e.block[p] = best[p];
+    layout(e);
+    for (int g = 0; g < ng; ++g) {
+      const int M = e.groups[g].M, start = e.groups[g].S;
+      int best_S = start;
+      std::vector<int> candidates;
+      for (int S = start / 2; S >= 1 && candidates.size() < 3; S /= 2) candidates.push_back(S);
+      for (int S = start * 2; candidates.size() < 6; S *= 2) {
+        candidates.push_back(std::min(S, M));
+        if (S >= M) break;
+      }
+      for (int S : candidates) {
+        if (S == start) continue;
+        set_slicing(g, S);
+        const double ms = trial();
+        if (ms < best_t) {
+          best_t = ms;
+          best_S = S;
+        }
+      }
+      set_slicing(g, best_S);
+    }
   } catch (...) {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -844,11 +1105,11 @@ int trisk_ensemble_autotune(TriskEnsemble* ens, int32_t steps, double* best_ms) 
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  for (int p = 0; p < 3; ++p) e.block[p] = best[p];
-  for (int g = 0; g < e.G.n; ++g) e.G.g[g].nsteps = nsteps[g];
-  layout(e);
-  drop_graph(e);
+  for (int g = 0; g < ng; ++g) e.groups[g].nsteps = nsteps[g];
+  build_slices(e);
+  drop_graphs(e);
   restore();
+  for (int g = 0; g < ng; ++g) e.groups[g].taken = taken[g];
   CUDA_CHECK(cudaMemcpyAsync(e.counters, counters.data(), MAX_GROUPS * sizeof(int), cudaMemcpyHostToDevice,
                              e.stream));
   CUDA_CHECK(cudaMemsetAsync(e.flag, 0, sizeof(int), e.stream));
@@ -869,36 +1130,34 @@ int trisk_ensemble_set_closure(TriskEnsemble* ens, int32_t group, TriskClosure* 
                                const double* norm, int32_t flags) {
   TRISK_API_BEGIN
   TriskEnsemble& e = *checked_e(ens);
-  if (group < 0 || group >= e.G.n) throw Error(TRISK_ERR_ARGUMENT, "group out of range");
+  EnsembleGroup& G = group_ref(e, group);
   DeviceGuard guard(e.device);
-  GroupDesc& D = e.G.g[group];
-  ClosureSlot& c = e.cl[group];
-  drop_graph(e);
+  CUDA_CHECK(cudaStreamSynchronize(e.stream));
+  ClosureSlot& c = G.cl;
   if (!net) {  // back to the plain step
     c.net = nullptr;
-    D.W.dq = D.W.dF = nullptr;
+    build_slices(e);
+    drop_graphs(e);
     return TRISK_OK;
   }
-  TriskModel& m = *e.models[group];
+  TriskModel& m = *G.m;
   if (m.pv != PVM_TRISK) throw Error(TRISK_ERR_UNSUPPORTED, "the closure's features need the TRiSK PV flux");
   if (closure_device(net) != e.device) throw Error(TRISK_ERR_ARGUMENT, "closure on another device");
   if (!geometry || !norm) throw Error(TRISK_ERR_ARGUMENT, "NULL argument");
-  const int64_t rows = m.ne * (int64_t)D.M;
+  const int64_t rows = m.ne * (int64_t)G.M;
   if (!c.X) {
     c.X = e.alloc<__nv_bfloat16>(rows * NFEAT);
     c.Y = e.alloc<float>(rows * 2);
     c.geom = e.alloc<float>(m.ne * NGEOM);
-    c.member_on = e.alloc<float>(D.M);
+    c.member_on = e.alloc<float>(G.M);
     c.dF = e.alloc_state(rows);
     c.dq = e.alloc_state(rows);
-    std::vector<float> on(D.M, 1.0f);
-    CUDA_CHECK(cudaMemcpy(c.member_on, on.data(), D.M * sizeof(float), cudaMemcpyHostToDevice));
+    std::vector<float> on(G.M, 1.0f);
+    CUDA_CHECK(cudaMemcpy(c.member_on, on.data(), G.M * sizeof(float), cudaMemcpyHostToDevice));
     CUDA_CHECK(cudaMemset(c.Y, 0, rows * 2 * sizeof(float)));
     CUDA_CHECK(cudaMemset(c.dF, 0, rows * e.esize()));
     CUDA_CHECK(cudaMemset(c.dq, 0, rows * e.esize()));
   }
-  D.W.dq = c.dq;
-  D.W.dF = c.dF;
   std::vector<float> g((size_t)m.ne * NGEOM);
   for (int64_t j = 0; j < m.ne; ++j)  // internal edge j = file edge edge_n2o[j]
     for (int k = 0; k < NGEOM; ++k) g[j * NGEOM + k] = geometry[(size_t)m.edge_n2o[j] * NGEOM + k];
@@ -912,22 +1171,24 @@ int trisk_ensemble_set_closure(TriskEnsemble* ens, int32_t group, TriskClosure* 
   c.every_stage = (flags & 1) != 0;
   c.work_free = (flags & 2) != 0;
   if (c.work_free && !c.sums) {
-    c.sums = e.alloc<double>(2 * (size_t)D.M);
-    c.partials = e.alloc<double>(2 * (size_t)D.M * WORK_SUM_BLOCKS);
+    c.sums = e.alloc<double>(2 * (size_t)G.M);
+    c.partials = e.alloc<double>(2 * (size_t)G.M * WORK_SUM_BLOCKS);
   }
   c.net = net;
+  build_slices(e);
+  drop_graphs(e);
   TRISK_API_END
 }
 
 int trisk_ensemble_closure_mask(TriskEnsemble* ens, int32_t group, const float* member_on) {
   TRISK_API_BEGIN
   TriskEnsemble& e = *checked_e(ens);
-  if (group < 0 || group >= e.G.n || !member_on) throw Error(TRISK_ERR_ARGUMENT, "bad argument");
-  ClosureSlot& c = e.cl[group];
+  if (!member_on) throw Error(TRISK_ERR_ARGUMENT, "bad argument");
+  EnsembleGroup& G = group_ref(e, group);
+  ClosureSlot& c = G.cl;
   if (!c.net) throw Error(TRISK_ERR_ARGUMENT, "the group has no closure");
   DeviceGuard guard(e.device);
-  CUDA_CHECK(cudaMemcpyAsync(c.member_on, member_on, e.G.g[group].M * sizeof(float), cudaMemcpyHostToDevice,
-                             e.stream));
+  CUDA_CHECK(cudaMemcpyAsync(c.member_on, member_on, G.M * sizeof(float), cudaMemcpyHostToDevice, e.stream));
   CUDA_CHECK(cudaStreamSynchronize(e.stream));
   TRISK_API_END
 }
@@ -938,13 +1199,12 @@ int trisk_ensemble_features(TriskEnsemble* ens, int32_t group, void* X, const do
                             const float* geometry) {
   TRISK_API_BEGIN
   TriskEnsemble& e = *checked_e(ens);
-  if (group < 0 || group >= e.G.n || !X || !norm || !geometry) throw Error(TRISK_ERR_ARGUMENT, "bad argument");
+  if (!X || !norm || !geometry) throw Error(TRISK_ERR_ARGUMENT, "bad argument");
+  EnsembleGroup& G = group_ref(e, group);
   if (reinterpret_cast<uintptr_t>(X) % 16) throw Error(TRISK_ERR_ARGUMENT, "X must be 16-byte aligned");
-  TriskModel& m = *e.models[group];
+  TriskModel& m = *G.m;
   if (m.pv != PVM_TRISK) throw Error(TRISK_ERR_UNSUPPORTED, "the closure's features need the TRiSK PV flux");
   DeviceGuard guard(e.device);
-  const GroupDesc& D = e.G.g[group];
-  const int M = D.M;
   FeatureNorm N{};
   for (int k = 0; k < NFEAT; ++k) {
     N.mean[k] = norm[k];
@@ -960,27 +1220,32 @@ int trisk_ensemble_features(TriskEnsemble* ens, int32_t group, void* X, const do
   CUDA_CHECK(cudaMemcpyAsync(geom, g.data(), g.size() * sizeof(float), cudaMemcpyHostToDevice, e.stream));
   CUDA_CHECK(cudaMemcpyAsync(map, m.edge_n2o.data(), m.ne * sizeof(int32_t), cudaMemcpyHostToDevice, e.stream));
   const int B = 128;
-  const int64_t rows = m.ne * (int64_t)M;
   order_after_caller(e.stream, e.caller_ev);  // X may still be read by the caller
-  with_modes_e(e.pv, e.ke, [&](auto pvc, auto kec) {
-    constexpr int PV = decltype(pvc)::value, KE = decltype(kec)::value;
-    with_real(e, [&](auto r) {
-      using R = decltype(r);
-      const R* u = reinterpret_cast<const R*>(D.y);
-      const R* h = u + (size_t)m.ne * M;
-      const DevWorkT<R> W = work_as<R>(D.W);
-      k_vertex<PV, KE, true, R><<<(unsigned)cdiv(m.nv * M, B), B, 0, e.stream>>>(D.T, W, u, h, M, 0);
-      const int nbE = (int)cdiv(m.ne * M, B);
-      k_flux<PV, KE, true, R><<<(unsigned)(nbE + cdiv(m.nc * M, B)), B, 0, e.stream>>>(D.T, W, u, h, M, nbE, 1);
-      kg_features<R><<<(unsigned)cdiv(rows, 256), 256, 0, e.stream>>>(D.T, W, u, M, geom, N,
-                                                                       static_cast<__nv_bfloat16*>(X), map, rows);
+  for (const Slice& sl : e.slices) {
+    if (sl.group != group) continue;
+    const GroupDesc& D = sl.D;
+    const int M = D.M;
+    const int64_t rows = m.ne * (int64_t)M;
+    with_modes_e(e.pv, e.ke, [&](auto pvc, auto kec) {
+      constexpr int PV = decltype(pvc)::value, KE = decltype(kec)::value;
+      with_real(e, [&](auto r) {
+        using R = decltype(r);
+        const R* u = reinterpret_cast<const R*>(D.y);
+        const R* h = u + (size_t)m.ne * M;
+        const DevWorkT<R> W = work_as<R>(D.W);
+        k_vertex<PV, KE, true, R><<<(unsigned)cdiv(m.nv * M, B), B, 0, e.stream>>>(D.T, W, u, h, M, 0);
+        const int nbE = (int)cdiv(m.ne * M, B);
+        k_flux<PV, KE, true, R><<<(unsigned)(nbE + cdiv(m.nc * M, B)), B, 0, e.stream>>>(D.T, W, u, h, M, nbE, 1);
+        kg_features<R><<<(unsigned)cdiv(rows, 256), 256, 0, e.stream>>>(
+            D.T, W, u, M, geom, N, static_cast<__nv_bfloat16*>(X), map, rows, G.M, sl.m0);
+      });
     });
-  });
-  CUDA_CHECK(cudaGetLastError());
+    CUDA_CHECK(cudaGetLastError());
+    e.launches += 3;
+  }
   CUDA_CHECK(cudaFreeAsync(geom, e.stream));
   CUDA_CHECK(cudaFreeAsync(map, e.stream));
   CUDA_CHECK(cudaStreamSynchronize(e.stream));
-  e.launches += 3;
   TRISK_API_END
 }
 
@@ -988,37 +1253,41 @@ int trisk_ensemble_features(TriskEnsemble* ens, int32_t group, void* X, const do
 int trisk_ensemble_energy(TriskEnsemble* ens, int32_t group, double* energies) {
   TRISK_API_BEGIN
   TriskEnsemble& e = *checked_e(ens);
-  if (group < 0 || group >= e.G.n || !energies) throw Error(TRISK_ERR_ARGUMENT, "bad argument");
-  TriskModel& m = *e.models[group];
+  if (!energies) throw Error(TRISK_ERR_ARGUMENT, "bad argument");
+  EnsembleGroup& G = group_ref(e, group);
+  TriskModel& m = *G.m;
   DeviceGuard guard(e.device);
-  const GroupDesc& D = e.G.g[group];
-  const int M = D.M;
   if (!e.energy) e.energy = e.alloc<double>(e.max_members);
   const int nblocks = (int)cdiv(m.nc, 256);
-  if (e.energy_partials_size < (size_t)nblocks * M) {  // grown on demand, kept for later calls
-    e.energy_partials_size = (size_t)nblocks * M;
+  if (e.energy_partials_size < (size_t)nblocks * G.M) {  // grown on demand, kept for later calls
+    e.energy_partials_size = (size_t)nblocks * G.M;
     e.energy_partials = e.alloc<double>(e.energy_partials_size);
   }
   const int B = 128;
-  with_modes_e(e.pv, e.ke, [&](auto pvc, auto kec) {
-    constexpr int PV = decltype(pvc)::value, KE = decltype(kec)::value;
-    with_real(e, [&](auto r) {
-      using R = decltype(r);
-      const R* u = reinterpret_cast<const R*>(D.y);
-      const R* h = u + (size_t)m.ne * M;
-      const DevWorkT<R> W = work_as<R>(D.W);
-      k_vertex<PV, KE, true, R><<<(unsigned)cdiv(m.nv * M, B), B, 0, e.stream>>>(D.T, W, u, h, M, 0);
-      const int nbE = (int)cdiv(m.ne * M, B);
-      k_flux<PV, KE, true, R><<<(unsigned)(nbE + cdiv(m.nc * M, B)), B, 0, e.stream>>>(D.T, W, u, h, M, nbE, 1);
-      kg_energy<R><<<dim3((unsigned)nblocks, (unsigned)M), 256, 0, e.stream>>>(
-          u, W.K, m.area_c, (int)m.nc, (int)m.ne, M, m.gravity, e.energy_partials);
-      kg_sum_rows<<<(unsigned)M, 256, 0, e.stream>>>(e.energy_partials, nblocks, e.energy);
+  for (const Slice& sl : e.slices) {
+    if (sl.group != group) continue;
+    const GroupDesc& D = sl.D;
+    const int M = D.M;
+    with_modes_e(e.pv, e.ke, [&](auto pvc, auto kec) {
+      constexpr int PV = decltype(pvc)::value, KE = decltype(kec)::value;
+      with_real(e, [&](auto r) {
+        using R = decltype(r);
+        const R* u = reinterpret_cast<const R*>(D.y);
+        const R* h = u + (size_t)m.ne * M;
+        const DevWorkT<R> W = work_as<R>(D.W);
+        k_vertex<PV, KE, true, R><<<(unsigned)cdiv(m.nv * M, B), B, 0, e.stream>>>(D.T, W, u, h, M, 0);
+        const int nbE = (int)cdiv(m.ne * M, B);
+        k_flux<PV, KE, true, R><<<(unsigned)(nbE + cdiv(m.nc * M, B)), B, 0, e.stream>>>(D.T, W, u, h, M, nbE, 1);
+        kg_energy<R><<<dim3((unsigned)nblocks, (unsigned)M), 256, 0, e.stream>>>(
+            u, W.K, m.area_c, (int)m.nc, (int)m.ne, M, m.gravity, e.energy_partials);
+        kg_sum_rows<<<(unsigned)M, 256, 0, e.stream>>>(e.energy_partials, nblocks, e.energy + sl.m0);
+      });
     });
-  });
-  CUDA_CHECK(cudaGetLastError());
-  CUDA_CHECK(cudaMemcpyAsync(energies, e.energy, M * sizeof(double), cudaMemcpyDeviceToHost, e.stream));
+    CUDA_CHECK(cudaGetLastError());
+    e.launches += 4;
+  }
+  CUDA_CHECK(cudaMemcpyAsync(energies, e.energy, G.M * sizeof(double), cudaMemcpyDeviceToHost, e.stream));
   CUDA_CHECK(cudaStreamSynchronize(e.stream));
-  e.launches += 4;
   TRISK_API_END
 }
 
@@ -1026,8 +1295,8 @@ int trisk_ensemble_closure_check(TriskEnsemble* ens) {
   TRISK_API_BEGIN
   TriskEnsemble& e = *checked_e(ens);
   DeviceGuard guard(e.device);
-  for (int g = 0; g < e.G.n; ++g)
-    if (e.cl[g].net) closure_check(e.cl[g].net);
+  for (EnsembleGroup& G : e.groups)
+    if (G.cl.net) closure_check(G.cl.net);
   TRISK_API_END
 }
 

@@ -1,4 +1,4 @@
-"""Batched ensembles: many members on meshes of several levels in one persistent launch.
+"""Batched ensembles: many members on meshes of several levels, persistent launches per phase.
 
 There is no ensemble in the reference (it runs one model per process); each member here
 follows rk4_step! (src/TimeSteppers/RungeKutta.jl:18-29) on its group's model bit for bit.
@@ -49,8 +49,8 @@ class Ensemble:
         return y
 
     def autotune(self, steps: int = 10) -> float:
-        """Picks the fastest phase block sizes for these groups (states are left as they
-        were); returns ms per RK4 step."""
+        """Picks the fastest phase block sizes and members per slice for these groups (states
+        are left as they were); returns ms per RK4 step."""
         best = C.c_double()
         check(lib.trisk_ensemble_autotune(self._h, int(steps), C.byref(best)))
         return best.value
@@ -65,6 +65,20 @@ class Ensemble:
         if b.shape != (3,):
             raise ValueError("three block sizes")
         check(lib.trisk_ensemble_set_block(self._h, b.ctypes.data))
+
+    def slices(self) -> list:
+        """Members per slice of every group: a slice's members are stored together and its
+        three phases run back to back, so its work vectors stay in L2."""
+        b = np.zeros(len(self.groups), dtype=np.int32)
+        check(lib.trisk_ensemble_get_slices(self._h, b.ctypes.data))
+        return b.tolist()
+
+    def set_slices(self, members_per_slice) -> None:
+        """Re-slices every group (the members' states are kept)."""
+        b = np.ascontiguousarray(members_per_slice, dtype=np.int32)
+        if b.shape != (len(self.groups),):
+            raise ValueError("one slice size per group")
+        check(lib.trisk_ensemble_set_slices(self._h, b.ctypes.data))
 
     def run_async(self, steps: int) -> None:
         check(lib.trisk_ensemble_run_async(self._h, int(steps)))

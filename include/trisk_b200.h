@@ -356,8 +356,10 @@ int64_t trisk_mpas_launch_count(TriskMpas* ops);
  * trisk_shallow_water.jl:71-111); each member's arithmetic is that of rk4_step!
  * (RungeKutta.jl:18-29) on its group's model, bit for bit. A group = `members[g]` states
  * that share models[g]'s device tables (same mesh and scheme; all groups one scheme and
- * device), with its own dt[g] and step count nsteps[g]. Up to 8 groups. One RK4 step of
- * all unfinished groups is one CUDA graph of persistent kernels; the models must outlive
+ * device), with its own dt[g] and step count nsteps[g]. Up to 8 groups. A group's members
+ * are split into slices of consecutive members stored together; the three phases of a set of
+ * slices run back to back, set after set, so a slice's work vectors stay in L2. One RK4 step
+ * of all unfinished groups is one CUDA graph of persistent kernels; the models must outlive
  * the ensemble. */
 typedef struct TriskEnsemble TriskEnsemble;
 int trisk_ensemble_create(TriskModel* const* models, const int32_t* members, const double* dt,
@@ -373,7 +375,8 @@ void trisk_ensemble_destroy(TriskEnsemble* ensemble);
 /* Member state y = [u; h] in file numbering, host or device memory. */
 int trisk_ensemble_set_member(TriskEnsemble* ensemble, int32_t group, int32_t member, const double* y);
 int trisk_ensemble_get_member(TriskEnsemble* ensemble, int32_t group, int32_t member, double* y);
-/* Enqueues `steps` graph replays; a group stops advancing once it has taken nsteps[g]. */
+/* Advances every group by `steps` RK4 steps, or until it has taken nsteps[g]: one graph
+ * replay per step, each replay of the groups still running. */
 int trisk_ensemble_run_async(TriskEnsemble* ensemble, int64_t steps);
 int trisk_ensemble_synchronize(TriskEnsemble* ensemble);
 int trisk_ensemble_steps(TriskEnsemble* ensemble, int64_t* steps_taken); /* per group */
@@ -384,11 +387,17 @@ int64_t trisk_ensemble_launch_count(TriskEnsemble* ensemble);
  * [64, 256]; default 128 each). */
 int trisk_ensemble_set_block(TriskEnsemble* ensemble, const int32_t block[3]);
 int trisk_ensemble_get_block(TriskEnsemble* ensemble, int32_t block[3]);
+/* Members per slice of every group (ngroups values; the last slice of a group may have
+ * fewer). The default minimizes a byte estimate: tables streamed once per slice against the
+ * part of a slice's state and work vectors beyond a 96 MB L2 budget. Setting them keeps the
+ * members' states; results are the same bit for bit for every slicing. */
+int trisk_ensemble_set_slices(TriskEnsemble* ensemble, const int32_t* members_per_slice);
+int trisk_ensemble_get_slices(TriskEnsemble* ensemble, int32_t* members_per_slice);
 /* Autotuner of the batched path (no reference counterpart): times `steps` RK4 steps of all
- * groups for every combination of the phase block sizes {64, 128, 256}, keeps the fastest
- * and restores the members' states, step counters and step counts, so results are unchanged;
- * best_ms gets the time per step. Each call keeps one copy of the states until the ensemble
- * is destroyed. */
+ * groups for every combination of the phase block sizes {64, 128, 256}, then for each group
+ * a few members-per-slice values around the current one, keeps the fastest and restores the
+ * members' states, step counters and step counts, so results are unchanged; best_ms gets the
+ * time per step. Each call keeps one copy of the states until the ensemble is destroyed. */
 int trisk_ensemble_autotune(TriskEnsemble* ensemble, int32_t steps, double* best_ms);
 /* Algorithmic bytes of one RK4 step of all groups: sum 4 (T + 2 M N) + 15 M N. */
 int trisk_ensemble_bytes(TriskEnsemble* ensemble, double* step_bytes);

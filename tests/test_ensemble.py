@@ -15,14 +15,22 @@ def member_states(g, count, seed):
     return w.ensemble_members(g, count, seed, degree=6)
 
 
-@pytest.mark.parametrize("pv,ke", [("trisk", "cell"), ("gassmann", "vertex"), ("gassmann_mean", "mixed")])
-def test_ensemble_matches_single_models(require_gpu, pv, ke):
+@pytest.mark.parametrize("pv,ke,slices", [("trisk", "cell", None), ("gassmann", "vertex", None),
+                                          ("gassmann_mean", "mixed", None), ("trisk", "cell", [2, 1, 2]),
+                                          ("gassmann", "vertex", [3, 2, 1])])
+def test_ensemble_matches_single_models(require_gpu, pv, ke, slices):
+    """Every member of three groups of uneven meshes and step counts equals the single-model
+    RK4 step bit for bit, with the default slicing and with groups split into slices of one to
+    three members (launch sets of several slices, odd and even slice sizes)."""
     si = w.si_parameters()
     levels, members, nsteps = (3, 4, 5), (5, 3, 2), (7, 5, 3)
     grids = [trisk_grid(n, True) for n in levels]
     models = [d.TRiSKShallowWater(g, pv_flux=pv, kinetic_energy=ke, **si) for g in grids]
     dts = [w.courant_dt(g) for g in grids]
     ens = d.Ensemble([(m, k, dt, s) for m, k, dt, s in zip(models, members, dts, nsteps)])
+    if slices:
+        ens.set_slices(slices)
+        assert ens.slices() == slices
     states = [member_states(g, k, seed) for g, k, seed in zip(grids, members, (1, 2, 3))]
     for gi, group in enumerate(states):
         for k, y in enumerate(group):
@@ -30,7 +38,10 @@ def test_ensemble_matches_single_models(require_gpu, pv, ke):
     for gi, group in enumerate(states):  # set/get round trip before stepping
         for k, y in enumerate(group):
             assert np.array_equal(ens.get_member(gi, k), y)
-    ens.run(max(nsteps) + 2)
+    ens.run(2)
+    if slices:  # re-slicing in the middle of a run keeps every member's state
+        ens.set_slices([1, 3, 1])
+    ens.run(max(nsteps))
     assert ens.steps_taken() == list(nsteps)
     for gi, group in enumerate(states):
         for k, y in enumerate(group):
@@ -68,8 +79,8 @@ def test_ensemble_reset_and_launches(require_gpu):
         ens.set_member(0, k, y)
     ens.run(1)  # captures the graph
     before = ens.launch_count()
-    ens.run(3)
-    assert ens.launch_count() - before == 3 * 13
+    ens.run(3)  # one step is left: one replay of 12 phase launches and the counter update
+    assert ens.launch_count() - before == 13
     assert ens.steps_taken() == [2]
     ens.reset()
     assert ens.steps_taken() == [0]
@@ -246,17 +257,14 @@ def test_closure_energy_monitor_is_deterministic(require_gpu, work_free):
         on = np.ones(M, dtype=np.float32)
         e0 = ens.energy(0)
         energies, masks = [e0], []
-        threshold = None
-        for _ in range(4):
+        for check in range(4):
             ens.run(10)
             e = ens.energy(0)
             energies.append(e)
-            drift = np.abs(e - e0) / np.abs(e0)
-            if threshold is None:
-                threshold = np.median(drift)   # a threshold that switches about half the members off
-            newly = (drift > threshold) & (on > 0)
-            on[newly] = 0.0
-            ens.closure_mask(0, on)
+            if check == 0:  # the members drifting more than the median fall back to the plain step
+                drift = np.abs(e - e0) / np.abs(e0)
+                on[drift > np.median(drift)] = 0.0
+                ens.closure_mask(0, on)
             masks.append(on.copy())
         ens.closure_check()
         return energies, masks, [ens.get_member(0, k) for k in range(M)]
