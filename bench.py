@@ -602,6 +602,23 @@ def run_closure_leg(local_rank, members=128, seed=7):
     per_member = out["closure_gpu_seconds_per_simulated_day"] / members
     out["closure_gpu_seconds_per_member_day"] = per_member
     out["gpu_seconds_ratio_hexagon8_over_closure_hexagon6"] = per_day8 / per_member
+    # plain FP64 hexagon 7 (dt 75 s), 32 members: the second plain level of the equal-error figure
+    g7 = d.TRiSKGrid(d.create_hexagon_mesh(7, centroidal=True))
+    m7 = d.TRiSKShallowWater(g7, pv_flux="trisk", kinetic_energy="cell", device=local_rank, **si)
+    e7 = d.Ensemble([(m7, 32, 75.0, 1152)])
+    for k, y in enumerate(w.ensemble_members(g7, 32, seed=seed, degree=8, rms_range=(100.0, 100.0))):
+        e7.set_member(0, k, y)
+    e7.run(2)
+    e7.reset()
+    s7 = torch.cuda.ExternalStream(e7.stream(), device=local_rank)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(s7)
+    e7.run_async(96)
+    b.record(s7)
+    e7.synchronize()
+    out["plain_hexagon7_fp64_gpu_seconds_per_member_day"] = a.elapsed_time(b) / 1e3 / 96 * 1152 / 32
+    del e7
+    out["measured_errors"] = optional_leg(closure_errors, local_rank, g6, g7, g8, net, norm, out)
     if os.path.exists(CLOSURE_SUMMARY):
         with open(CLOSURE_SUMMARY) as f:
             s = json.load(f)
@@ -612,8 +629,46 @@ def run_closure_leg(local_rank, members=128, seed=7):
                 "state_bits": s[k].get("state_bits", 64)}
             for k in ("plain_coarse", "plain_coarse_fp32", "closure_coarse", "closure_coarse_no_fallback",
                       "closure_every_stage_no_fallback", "closure_mass_flux_only_no_fallback") if k in s}
-        out["errors_source"] = "dmplex_b200/data/closure_hexagon6.json (python -m dmplex_b200.closure_pipeline)"
+        out["errors_source"] = ("errors_vs_coarse_grained_hexagon8: the committed 10-day experiment "
+                                "(dmplex_b200/data/closure_hexagon6.json, python -m dmplex_b200.closure_pipeline); "
+                                "measured_errors: computed in this run")
     return out
+
+
+def closure_errors(local_rank, g6, g7, g8, net, norm, costs, seeds=(2001, 2002), days=2):
+    """The north-star comparison measured here: fine hexagon-8 runs (dt 20 s) from held-out
+    seeds, coarse-grained to hexagon 6 every day, judge plain FP64 hexagon 6 (dt 150 s) and 7
+    (dt 75 s, coarse-grained to hexagon 6 for the comparison) and the closure on hexagon 6 (FP32
+    state, energy-drift fallback); then the GPU seconds per member-day the plain method needs
+    at the closure's h error, interpolated log-linearly between the two plain levels, against
+    the closure's own (costs: the large-ensemble timings of the closure leg)."""
+    from dmplex_b200 import closure_pipeline as cp
+    _, _, _, daily, fine_s = cp.fine_snapshots(g8, g6, list(seeds), days, 0, dt_fine=20.0, device=local_rank,
+                                               spinup_days=0.0, record_days=True)
+    init = daily[0]
+    runs = {"plain_hexagon6_fp64": cp.run_coarse(g6, init, days, 150.0, daily, device=local_rank),
+            "closure_hexagon6": cp.run_coarse(g6, init, days, 150.0, daily, net, norm, device=local_rank,
+                                              state_bits=32),
+            "plain_hexagon7_fp64": cp.plain_level_errors(g8, g6, g7, list(seeds), days, 75.0, daily,
+                                                         device=local_rank)}
+    err = {k: [float(np.mean(x)) for x in r["h_l2"]] for k, r in runs.items()}
+    zeta = {k: [float(np.mean(x)) for x in r["zeta_l2"]] for k, r in runs.items()}
+    c6 = costs["plain_fp64_gpu_seconds_per_simulated_day"] / costs["members"]
+    c7 = costs["plain_hexagon7_fp64_gpu_seconds_per_member_day"]
+    cc = costs["closure_gpu_seconds_per_member_day"]
+    last = days - 1
+    plain_at = cp.equal_error_cost({6: err["plain_hexagon6_fp64"][last], 7: err["plain_hexagon7_fp64"][last]},
+                                   {6: c6, 7: c7}, err["closure_hexagon6"][last])
+    return {"seeds": list(seeds), "days": days, "h_l2_per_day_m": err, "zeta_l2_per_day": zeta,
+            "fallback_members": runs["closure_hexagon6"]["fallback_members"],
+            "diverged_on_day": runs["closure_hexagon6"]["diverged_on_day"],
+            "gpu_seconds_per_member_day": {"plain_hexagon6_fp64": c6, "plain_hexagon7_fp64": c7, "closure_hexagon6": cc},
+            "summary": {"day": days, "h_plain6": err["plain_hexagon6_fp64"][last],
+                        "h_plain7": err["plain_hexagon7_fp64"][last], "h_closure": err["closure_hexagon6"][last],
+                        "plain_gpu_s_per_member_day_at_closure_error": plain_at,
+                        "closure_gpu_s_per_member_day": cc,
+                        "plain_over_closure_at_equal_error": plain_at / cc if cc > 0 else None},
+            "fine_gpu_seconds": fine_s}
 
 
 def _pick(d, *keys, digits=4):

@@ -102,6 +102,16 @@ class TriskCoefficients(C.Structure):
                 ("pv_flux", _i32), ("alpha", _f64), ("gravity", _f64)] + [(n, _p) for n in COEFFICIENT_POINTERS]
 
 
+class TriskHalo(C.Structure):
+    _fields_ = [("ne_owned", _i64), ("nc_owned", _i64), ("nneighbors", _i32), ("pad_", _i32),
+                ("send_offsets", _p), ("send_index", _p), ("recv_offsets", _p), ("recv_index", _p)]
+
+
+# int (*)(void* user, const double* send, int64_t nsend, double* recv, int64_t nrecv, void* stream)
+EXCHANGE_FN = C.CFUNCTYPE(C.c_int, _p, _p, _i64, _p, _i64, _p)
+EXCHANGE_HOST, EXCHANGE_DEVICE, EXCHANGE_DEVICE_GRAPH = 0, 1, 2
+
+
 def _load():
     if not os.path.exists(LIB_PATH):
         raise ImportError(f"{LIB_PATH} is missing: build it with `make -C dmplex_b200` (or __graft_entry__.build())")
@@ -168,6 +178,7 @@ def _load():
         "trisk_closure_synchronize": (C.c_int, [_p]),
         "trisk_closure_stream": (C.c_int, [_p, C.POINTER(_p)]),
         "trisk_closure_expire_wait_once": (C.c_int, [_p, _i64]),
+        "trisk_closure_info": (C.c_int, [_p, C.POINTER(_i32), C.POINTER(_i32)]),
         "trisk_ensemble_create": (C.c_int, [_p, _p, _p, _p, _i32, C.POINTER(_p)]),
         "trisk_ensemble_create_precision": (C.c_int, [_p, _p, _p, _p, _i32, _i32, C.POINTER(_p)]),
         "trisk_ensemble_set_block": (C.c_int, [_p, _p]),
@@ -185,6 +196,14 @@ def _load():
         "trisk_ensemble_bytes": (C.c_int, [_p, C.POINTER(_f64)]),
         "trisk_ensemble_energy": (C.c_int, [_p, _i32, _p]),
         "trisk_ensemble_set_closure": (C.c_int, [_p, _i32, _p, _p, _p, _i32]),
+        "trisk_dist_create": (C.c_int, [C.POINTER(TriskCoefficients), C.POINTER(TriskConfig), C.POINTER(TriskHalo),
+                                        C.POINTER(_p)]),
+        "trisk_dist_destroy": (None, [_p]),
+        "trisk_dist_set_exchange": (C.c_int, [_p, EXCHANGE_FN, _p, _i32]),
+        "trisk_dist_tendency": (C.c_int, [_p, _p, _p]),
+        "trisk_dist_rk4_step": (C.c_int, [_p, _p, _f64, _i64]),
+        "trisk_dist_stream": (C.c_int, [_p, C.POINTER(_p)]),
+        "trisk_dist_launch_count": (_i64, [_p]),
         "trisk_ensemble_set_slices": (C.c_int, [_p, _p]),
         "trisk_ensemble_get_slices": (C.c_int, [_p, _p]),
         "trisk_ensemble_closure_mask": (C.c_int, [_p, _i32, _p]),
@@ -201,7 +220,7 @@ def _load():
         fn.restype = res
         fn.argtypes = args
     for which, cls in enumerate((TriskGrid, TriskCoefficients, TriskConfig, TriskPlex, TriskIconTables,
-                                  TriskMpasTables, TriskMpasFields)):
+                                  TriskMpasTables, TriskMpasFields, TriskHalo)):
         if lib.trisk_struct_size(which) != C.sizeof(cls):
             raise ImportError(f"{cls.__name__}: binding size {C.sizeof(cls)} != library size "
                               f"{lib.trisk_struct_size(which)}")

@@ -85,6 +85,12 @@ class ClosureMLP:
                                           C.byref(loss)))
         return g, loss.value
 
+    def info(self) -> dict:
+        """The inference kernel's launch shape: CTAs per SM of its persistent grid, and SMs."""
+        per_sm, sms = C.c_int32(), C.c_int32()
+        check(lib.trisk_closure_info(self._h, C.byref(per_sm), C.byref(sms)))
+        return {"forward_ctas_per_sm": per_sm.value, "sms": sms.value}
+
     def expire_wait_once(self, tile: int) -> None:
         """Test of the bounded tensor-core wait: the next forward call leaves tile `tile`'s first
         tensor-core operation un-issued, so it returns TRISK_ERR_TIMEOUT (TriskError status 5)

@@ -337,6 +337,50 @@ def run_coarse(gc, Y_init, days, dt, daily_truth, mlp=None, norm=None, drift_per
             "state_bits": state_bits}
 
 
+def plain_level_errors(gf, gc, gm, seeds, days, dt, daily_truth, device=0, state_bits=64):
+    """Plain runs on an intermediate mesh gm (between the coarse gc and the fine gf) from the
+    fine initial states coarse-grained to gm, judged like the coarse runs: every day the gm
+    state is coarse-grained to gc and compared with the coarse-grained fine run (daily_truth,
+    on gc). Returns h and vorticity L2 errors per day (members as columns) and the GPU seconds
+    per member-day of the gm runs."""
+    import torch
+    si = w.si_parameters()
+    mm = TRiSKShallowWater(gm, pv_flux=PV, kinetic_energy=KE, device=device, **si)
+    to_m, m_to_c = CoarseGrainer(gf, gm), CoarseGrainer(gm, gc)
+    steps_day = int(round(86400 / dt))
+    S = len(seeds)
+    ens = Ensemble([(mm, S, 86400 / steps_day, steps_day * days)], state_bits=state_bits)
+    for k, seed in enumerate(seeds):
+        ens.set_member(0, k, np.ascontiguousarray(to_m(w.synthetic_state(gf, seed=seed))))
+    Vc = relative_vorticity_matrix(model_tables(gc, pv_flux=PV, kinetic_energy=KE, **si))
+    stream = torch.cuda.ExternalStream(ens.stream(), device=device)
+    errs_h, errs_z, gpu_ms = [], [], 0.0
+    for day in range(1, days + 1):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        ens.run_async(steps_day)
+        b.record(stream)
+        ens.synchronize()
+        gpu_ms += a.elapsed_time(b)
+        Y = np.stack([m_to_c(ens.get_member(0, k)) for k in range(S)], axis=1)
+        eh, ez = l2_errors(gc, Vc, Y, daily_truth[day].cpu().numpy())
+        errs_h.append(eh.tolist())
+        errs_z.append(ez.tolist())
+    return {"h_l2": errs_h, "zeta_l2": errs_z, "gpu_seconds_per_member_day": gpu_ms / 1e3 / (S * days),
+            "cells": int(gm.nc), "dt": 86400 / steps_day, "members": S, "state_bits": state_bits}
+
+
+def equal_error_cost(errors: dict, costs: dict, target: float) -> float:
+    """GPU seconds per member-day the plain method needs to reach the h error `target`:
+    log-linear interpolation (or extrapolation) of cost against error between the two plain
+    levels, errors = {level: h error}, costs = {level: GPU seconds per member-day}."""
+    (l1, e1), (l2, e2) = sorted(errors.items())
+    if e1 <= 0 or e2 <= 0 or e1 == e2 or target <= 0:
+        return float("nan")
+    slope = np.log(costs[l2] / costs[l1]) / np.log(e2 / e1)
+    return float(costs[l1] * (target / e1) ** slope)
+
+
 def calibrate(gf, gc, mlp, norm, seeds=(501, 502), days=2, coarse_dt=150.0, fine_dt=20.0,
               scales=(0.0, 0.05, 0.1, 0.2, 0.4, 1.0), device=0, log=print, work_free=False):
     """A-posteriori choice of the momentum correction's scale: coarse runs with the closure

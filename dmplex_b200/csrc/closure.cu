@@ -297,21 +297,28 @@ __global__ void __launch_bounds__(TILE) k_mlp_forward(const __nv_bfloat16* __res
   const float4* w3a = reinterpret_cast<const float4*>(sw3);
   const float4* w3b = reinterpret_cast<const float4*>(sw3 + NH);
 
+  // row t of tile `tile` (24 features as three 16-byte loads; zeros past the last row)
+  auto load_row = [&](int64_t tile, uint4 (&q)[3]) {
+    q[0] = q[1] = q[2] = make_uint4(0, 0, 0, 0);
+    const int64_t row = tile * TILE + t;
+    if (tile < ntiles && row < n) {
+      const uint4* src = reinterpret_cast<const uint4*>(X + row * NIN);
+      q[0] = __ldcs(src);
+      q[1] = __ldcs(src + 1);
+      q[2] = __ldcs(src + 2);
+    }
+  };
+  uint4 xq[3];
+  load_row(blockIdx.x, xq);
   for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int64_t row = tile * TILE + t;
     const bool valid = row < n;
-    {  // X -> XH chunks 0..2 (24 features), chunk 3 = 0 (W1's padding columns are 0 as well)
-      uint4 q[3] = {make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0)};
-      if (valid) {
-        const uint4* src = reinterpret_cast<const uint4*>(X + row * NIN);
-        q[0] = src[0];
-        q[1] = src[1];
-        q[2] = src[2];
-      }
+    // X -> XH chunks 0..2, chunk 3 = 0 (W1's padding columns are 0 as well); then the next
+    // tile's row is loaded while this tile runs through the tensor cores and the epilogues
 #pragma unroll
-      for (int c = 0; c < 3; ++c) *reinterpret_cast<uint4*>(XH + tile_off(t, 8 * c, HX_CHUNK)) = q[c];
-      *reinterpret_cast<uint4*>(XH + tile_off(t, 24, HX_CHUNK)) = make_uint4(0, 0, 0, 0);
-    }
+    for (int c = 0; c < 3; ++c) *reinterpret_cast<uint4*>(XH + tile_off(t, 8 * c, HX_CHUNK)) = xq[c];
+    *reinterpret_cast<uint4*>(XH + tile_off(t, 24, HX_CHUNK)) = make_uint4(0, 0, 0, 0);
+    load_row(tile + gridDim.x, xq);
     sync_for_mma();
     if (waits.aborted()) break;
     const bool issue = tile != expire_tile;
@@ -369,7 +376,7 @@ __global__ void __launch_bounds__(TILE) k_mlp_forward(const __nv_bfloat16* __res
         y1 += h3 * wb.w;
       }
     }
-    if (valid) *reinterpret_cast<float2*>(Y + row * NOUT) = make_float2(y0, y1);
+    if (valid) __stcs(reinterpret_cast<float2*>(Y + row * NOUT), make_float2(y0, y1));
     fence_before();
     __syncthreads();  // the next tile rewrites XH, and its MMA 1 overwrites Z2
     fence_after();
@@ -663,7 +670,8 @@ struct TriskClosure {
   int64_t adam_step = 0;
   int64_t launches = 0;
   int sms = 0;              // the device's SM count (persistent grids)
-  int forward_per_sm = 1;   // resident inference CTAs per SM
+  int forward_per_sm = 1;   // resident inference CTAs per SM (the grid's multiple of the SMs)
+  int forward_occupancy = 0;  // what the occupancy query returned
   int64_t expire_tile = -1;  // test of the bounded wait: see trisk_closure_expire_wait_once
   ~TriskClosure() {
     int prev = -1;
@@ -756,11 +764,19 @@ int trisk_closure_create(int32_t device, const float* params, TriskClosure** out
   CUDA_CHECK(cudaGetLastError());
   CUDA_CHECK(cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, FWD_SMEM_BYTES));
   CUDA_CHECK(cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+  // all of the unified L1/shared storage as shared memory, so that seven inference CTAs (and
+  // two training CTAs) are resident per SM; without the preference the occupancy query, and
+  // the launch, can settle on a carveout that holds one
+  CUDA_CHECK(cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  cudaSharedmemCarveoutMaxShared));
+  CUDA_CHECK(cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  cudaSharedmemCarveoutMaxShared));
   int sms = 0;
   CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
   c->sms = sms;
   int per_sm = 0;
   CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mlp_forward, TILE, FWD_SMEM_BYTES));
+  c->forward_occupancy = per_sm;
   // every resident CTA must find its tensor-memory columns free (512 per SM)
   c->forward_per_sm = std::max(1, std::min<int>(per_sm, 512 / (int)FWD_TMEM_COLS));
   CUDA_CHECK(cudaStreamSynchronize(c->stream));
@@ -843,6 +859,15 @@ int trisk_closure_synchronize(TriskClosure* closure) {
   TriskClosure& c = *checked_c(closure);
   DeviceGuard guard(c.device);
   check_status(c);
+  TRISK_API_END
+}
+
+// Launch shape of the inference kernel: CTAs per SM of its persistent grid, and SMs.
+int trisk_closure_info(TriskClosure* closure, int32_t* forward_ctas_per_sm, int32_t* sms) {
+  TRISK_API_BEGIN
+  TriskClosure& c = *checked_c(closure);
+  if (forward_ctas_per_sm) *forward_ctas_per_sm = c.forward_per_sm;
+  if (sms) *sms = c.sms;
   TRISK_API_END
 }
 

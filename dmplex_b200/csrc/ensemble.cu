@@ -353,9 +353,11 @@ struct ClosureSlot {
 
 // blocks of kg_work_sums along the edges (the row length of its partial sums)
 constexpr int WORK_SUM_BLOCKS = 1024;
-// A slice's state and work vectors should stay in L2 (126 MB) beside the streaming tables:
-// the budget of the default slicing and of a launch set.
-constexpr double SLICE_L2_BUDGET = 96.0 * (1 << 20);
+// A slice's gathered stage state and work vectors should stay in L2 beside the streaming
+// tables. The L2 is 126 MB, but each of the two dies' halves caches what its own SMs read, so
+// data every SM reads sees about half of it (the single-model path thrashes beyond a working
+// set of ~60 MB): the budget of the default slicing and of a launch set.
+constexpr double SLICE_L2_BUDGET = 48.0 * (1 << 20);
 
 // A user group: its members' buffers (every slice's, one after the other) and its slicing.
 struct EnsembleGroup {
@@ -368,7 +370,7 @@ struct EnsembleGroup {
   double *y = nullptr, *acc = nullptr, *st = nullptr;
   DevWork W{};
   ClosureSlot cl;
-  double member_bytes = 0;   // state (y, acc, stage) and work vectors of one member
+  double member_bytes = 0;   // gathered stage state and work vectors of one member
 };
 
 struct Slice {
@@ -839,7 +841,7 @@ int trisk_ensemble_create_precision(TriskModel* const* models, const int32_t* me
     G.acc = e->alloc_state(m->N * M);
     G.st = e->alloc_state(m->N * M);
     CUDA_CHECK(cudaMemset(G.y, 0, m->N * M * e->esize()));
-    G.member_bytes = (double)e->esize() * (3.0 * m->N + 2.0 * m->nc + 2.0 * m->ne + 4.0 * m->nv);
+    G.member_bytes = (double)e->esize() * (1.0 * m->N + 2.0 * m->nc + 2.0 * m->ne + 4.0 * m->nv);
     G.S = default_slice(G.M, m->table_bytes_unique, G.member_bytes);
     e->groups.push_back(G);
     e->models.push_back(m);

@@ -53,6 +53,9 @@ enum Epilogue { EPI_TENDENCY = 0, EPI_STAGE1 = 1, EPI_STAGE2 = 2, EPI_STAGE3 = 3
 struct DevTables {
   int32_t nc, ne, nv;
   int32_t ldc, lde, ldv;  // padded entity counts of the [k][entity] tables
+  // Owned entities: internal edges < ne_own and cells < nc_own (all of them, except on one
+  // rank's part of a distributed model, whose ghosts follow and get zero tendencies).
+  int32_t ne_own, nc_own;
   double gravity;
   // Table entries below keep_end (a prefix of the one packed table block) are loaded with
   // an L2 evict-last policy, so they stay in L2 from one launch to the next; nullptr: none.
@@ -505,6 +508,7 @@ __device__ __forceinline__ void tend_body(const DevTables& T, const DevWorkT<R>&
       du = s - ((double)W.B[(size_t)ec1 * M + mm] - (double)W.B[(size_t)ec0 * M + mm]) * invd;
     }
     if (CL) du += (double)W.dq[o];  // learned momentum correction
+    if (e >= T.ne_own) du = 0.0;     // a ghost edge (TRiSKShallowWater.jl:389-393)
     epilogue<EPI, R>(S, o, du);
   } else {
     int i, mm;
@@ -528,7 +532,7 @@ __device__ __forceinline__ void tend_body(const DevTables& T, const DevWorkT<R>&
 #pragma unroll
     for (int k = 0; k < CW; ++k) s += dv[k] * f[k];
     const size_t o = (size_t)i * M + mm;
-    epilogue<EPI, R>(S, (size_t)T.ne * M + o, -s);
+    epilogue<EPI, R>(S, (size_t)T.ne * M + o, i >= T.nc_own ? 0.0 : -s);  // ghost cells: 0
   }
 }
 

@@ -75,6 +75,7 @@ int32_t trisk_struct_size(int32_t which) {
     case 4: return (int32_t)sizeof(TriskIconTables);
     case 5: return (int32_t)sizeof(TriskMpasTables);
     case 6: return (int32_t)sizeof(TriskMpasFields);
+    case 7: return (int32_t)sizeof(TriskHalo);
     default: return -1;
   }
 }

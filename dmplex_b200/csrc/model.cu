@@ -21,6 +21,13 @@ __global__ void k_gather(double* __restrict__ dst, const double* __restrict__ sr
   if (j < n) dst[j] = src[idx[j]];
 }
 
+// dst[idx[j]] = src[j], j < n
+__global__ void k_scatter(double* __restrict__ dst, const double* __restrict__ src, const int32_t* __restrict__ idx,
+                          int64_t n) {
+  const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (j < n) dst[idx[j]] = src[j];
+}
+
 constexpr int RED_BLOCK = 256, RED_PER_THREAD = 8;
 
 // MODE 0: a b   MODE 1: (a b)(c + g b / 2)   MODE 2: (a b)(c c)
@@ -436,11 +443,24 @@ Grid grid_from_abi(const TriskGrid* g) {
 // cells' edge lists, vertices by first appearance in the edges' vertex pairs (the same
 // rule as hilbert_order, src/Topology/Ordering.jl:54-82). The permutation is integer and
 // exact; every table row keeps its order, so per-entity sums are unchanged bit for bit.
+// Internal numbering: cells along the Hilbert curve of their centroids (the owned cells of a
+// distributed model's part first, then its ghosts), edges by first appearance in the cells'
+// edge lists (owned edges first), vertices by first appearance in the edges.
 void build_numbering(TriskModel& m, const Coefficients& C, const std::vector<V3>* centroids) {
   const int64_t nc = C.nc, ne = C.ne, nv = C.nv;
+  const int64_t nc_own = m.nc_own, ne_own = m.ne_own;
   std::vector<int64_t> cperm(nc);
   for (int64_t i = 0; i < nc; ++i) cperm[i] = i;
-  if (centroids) cperm = hilbert_sort(*centroids, 16);
+  if (centroids && nc_own == nc) {
+    cperm = hilbert_sort(*centroids, 16);
+  } else if (centroids) {  // owned cells, then ghost cells, each along the curve
+    for (int part = 0; part < 2; ++part) {
+      const int64_t lo = part ? nc_own : 0, hi = part ? nc : nc_own;
+      std::vector<V3> c(centroids->begin() + lo, centroids->begin() + hi);
+      const std::vector<int64_t> p = hilbert_sort(c, 16);
+      for (int64_t j = 0; j < hi - lo; ++j) cperm[lo + j] = lo + p[j];
+    }
+  }
   m.cell_n2o.assign(nc, 0);
   m.cell_o2n.assign(nc, -1);
   for (int64_t j = 0; j < nc; ++j) {
@@ -461,6 +481,15 @@ void build_numbering(TriskModel& m, const Coefficients& C, const std::vector<V3>
   }
   for (int64_t e = 0; e < ne; ++e)
     if (m.edge_o2n[e] < 0) m.edge_o2n[e] = next++;
+  if (ne_own < ne) {  // owned edges first, each kind in the order above
+    std::vector<int64_t> order(ne);
+    for (int64_t e = 0; e < ne; ++e) order[m.edge_o2n[e]] = e;
+    int32_t owned = 0, ghost = (int32_t)ne_own;
+    for (int64_t j = 0; j < ne; ++j) {
+      const int64_t e = order[j];
+      m.edge_o2n[e] = e < ne_own ? owned++ : ghost++;
+    }
+  }
   m.edge_n2o.assign(ne, 0);
   for (int64_t e = 0; e < ne; ++e) m.edge_n2o[m.edge_o2n[e]] = (int32_t)e;
   m.vert_o2n.assign(nv, -1);
@@ -582,6 +611,8 @@ void upload(TriskModel& m, const Coefficients& C) {
   T.nc = (int32_t)nc;
   T.ne = (int32_t)ne;
   T.nv = (int32_t)nv;
+  T.nc_own = (int32_t)m.nc_own;
+  T.ne_own = (int32_t)m.ne_own;
   T.ldc = (int32_t)ldc;
   T.lde = (int32_t)lde;
   T.ldv = (int32_t)ldv;
@@ -641,6 +672,8 @@ void finish_create(TriskModel& m, const Coefficients& C, const std::vector<V3>* 
   m.nc = C.nc;
   m.ne = C.ne;
   m.nv = C.nv;
+  if (m.nc_own < 0) m.nc_own = m.nc;
+  if (m.ne_own < 0) m.ne_own = m.ne;
   m.N = C.ne + C.nc;
   m.pv = C.pv_flux;
   m.alpha = C.alpha;
@@ -1187,5 +1220,258 @@ int trisk_profile_phases(TriskModel* model, double* y, double dt, int64_t nsteps
   for (int p = 0; p < 3; ++p) ms[p] = acc[p] / (4.0 * nsteps);
   TRISK_API_END
 }
+
+// ---- one rank's part of a distributed model ------------------------------------------
+}  // extern "C"
+
+struct TriskDist {
+  std::unique_ptr<TriskModel> m;
+  int64_t nsend = 0, nrecv = 0;
+  int32_t* send_idx = nullptr;  // internal state indices of the sent owned entries (device)
+  int32_t* recv_idx = nullptr;  // ... of the received ghost entries
+  double* send_dev = nullptr;
+  double* recv_dev = nullptr;
+  double* send_host = nullptr;  // pinned, for TRISK_EXCHANGE_HOST
+  double* recv_host = nullptr;
+  TriskExchangeFn fn = nullptr;
+  void* user = nullptr;
+  int mode = TRISK_EXCHANGE_HOST;
+  cudaGraphExec_t graph = nullptr;  // one RK4 step (TRISK_EXCHANGE_DEVICE_GRAPH)
+  double graph_dt = NAN;
+  int64_t graph_launches = 0;
+  ~TriskDist() {
+    if (!m) return;
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(m->device);
+    cudaStreamSynchronize(m->stream);
+    if (graph) cudaGraphExecDestroy(graph);
+    if (send_host) cudaFreeHost(send_host);
+    if (recv_host) cudaFreeHost(recv_host);
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+namespace {
+
+TriskDist* checked_dist(TriskDist* d) {
+  if (!d || !d->m) throw Error(TRISK_ERR_ARGUMENT, "distributed model is NULL");
+  return d;
+}
+
+// Ghost values of the state vector `base` (internal numbering) from their owners: pack the
+// sent entries, the caller's exchange, unpack the received ones (exchange!, Halo.jl:80-99).
+void dist_exchange(TriskDist& d, double* base) {
+  TriskModel& m = *d.m;
+  if (d.nsend == 0 && d.nrecv == 0) return;
+  if (!d.fn) throw Error(TRISK_ERR_ARGUMENT, "the part has neighbours but no exchange function");
+  if (d.nsend > 0) {
+    k_gather<<<(unsigned)cdiv(d.nsend, 256), 256, 0, m.stream>>>(d.send_dev, base, d.send_idx, d.nsend);
+    CUDA_CHECK(cudaGetLastError());
+    m.launches++;
+  }
+  int status;
+  if (d.mode == TRISK_EXCHANGE_HOST) {
+    if (d.nsend > 0)
+      CUDA_CHECK(cudaMemcpyAsync(d.send_host, d.send_dev, d.nsend * sizeof(double), cudaMemcpyDeviceToHost,
+                                 m.stream));
+    CUDA_CHECK(cudaStreamSynchronize(m.stream));
+    status = d.fn(d.user, d.send_host, d.nsend, d.recv_host, d.nrecv, nullptr);
+    if (status == TRISK_OK && d.nrecv > 0)
+      CUDA_CHECK(cudaMemcpyAsync(d.recv_dev, d.recv_host, d.nrecv * sizeof(double), cudaMemcpyHostToDevice,
+                                 m.stream));
+  } else {
+    status = d.fn(d.user, d.send_dev, d.nsend, d.recv_dev, d.nrecv, (void*)m.stream);
+  }
+  if (status != TRISK_OK) throw Error(status, "the exchange function failed");
+  if (d.nrecv > 0) {
+    k_scatter<<<(unsigned)cdiv(d.nrecv, 256), 256, 0, m.stream>>>(base, d.recv_dev, d.recv_idx, d.nrecv);
+    CUDA_CHECK(cudaGetLastError());
+    m.launches++;
+  }
+}
+
+// One RK4 step of the part (RungeKutta.jl:18-29): every tendency exchanges its stage state
+// first; the ghosts' tendencies are zero (k_tend), so their stage values stay the exchanged ones.
+void dist_enqueue_step(TriskDist& d, double dt) {
+  TriskModel& m = *d.m;
+  DevStage S{};
+  S.y = m.y;
+  S.acc = m.acc;
+  S.st = m.st;
+  S.flag = m.flag;
+  S.sixth = dt / 6;
+  S.u = m.y;
+  S.h = m.y + m.ne;
+  S.c = dt / 2;
+  dist_exchange(d, m.y);
+  enqueue_tendency(m, S, EPI_STAGE1);
+  S.u = m.st;
+  S.h = m.st + m.ne;
+  dist_exchange(d, m.st);
+  enqueue_tendency(m, S, EPI_STAGE2);
+  S.c = dt;
+  dist_exchange(d, m.st);
+  enqueue_tendency(m, S, EPI_STAGE3);
+  dist_exchange(d, m.st);
+  enqueue_tendency(m, S, EPI_STAGE4);
+}
+
+void dist_ensure_graph(TriskDist& d, double dt) {
+  TriskModel& m = *d.m;
+  if (d.graph && d.graph_dt == dt) return;
+  if (d.graph) {
+    cudaGraphExecDestroy(d.graph);
+    d.graph = nullptr;
+  }
+  const int64_t before = m.launches;
+  cudaGraph_t g = nullptr;
+  CUDA_CHECK(cudaStreamBeginCapture(m.stream, cudaStreamCaptureModeThreadLocal));
+  try {
+    dist_enqueue_step(d, dt);
+  } catch (...) {
+    cudaStreamEndCapture(m.stream, &g);
+    if (g) cudaGraphDestroy(g);
+    m.launches = before;
+    throw;
+  }
+  CUDA_CHECK(cudaStreamEndCapture(m.stream, &g));
+  d.graph_launches = m.launches - before;
+  m.launches = before;
+  cudaError_t e = cudaGraphInstantiate(&d.graph, g, 0);
+  cudaGraphDestroy(g);
+  CUDA_CHECK(e);
+  d.graph_dt = dt;
+}
+
+// 1-based local state indices of one side of the halo -> internal indices (device)
+int32_t* halo_indices(TriskModel& m, const int64_t* offsets, const int64_t* index, int32_t nnb, bool owned_side,
+                      int64_t& count) {
+  if (nnb > 0 && (!offsets || !index)) throw Error(TRISK_ERR_ARGUMENT, "halo lists are NULL");
+  count = nnb > 0 ? offsets[nnb] : 0;
+  if (nnb > 0 && offsets[0] != 0) throw Error(TRISK_ERR_ARGUMENT, "halo offsets must start at 0");
+  for (int32_t k = 0; k < nnb; ++k)
+    if (offsets[k + 1] < offsets[k]) throw Error(TRISK_ERR_ARGUMENT, "halo offsets must not decrease");
+  std::vector<int32_t> out((size_t)std::max<int64_t>(count, 1));
+  for (int64_t j = 0; j < count; ++j) {
+    const int64_t x = index[j] - 1;
+    if (x < 0 || x >= m.N) throw Error(TRISK_ERR_TABLE, "halo index out of range");
+    const bool edge = x < m.ne;
+    const int64_t local = edge ? x : x - m.ne;
+    const bool is_owned = edge ? local < m.ne_own : local < m.nc_own;
+    if (is_owned != owned_side)
+      throw Error(TRISK_ERR_TABLE, owned_side ? "a sent halo entry is not owned" : "a received halo entry is owned");
+    out[j] = edge ? m.edge_o2n[local] : (int32_t)(m.ne + m.cell_o2n[local]);
+  }
+  int32_t* dev = m.alloc<int32_t>(out.size());
+  CUDA_CHECK(cudaMemcpy(dev, out.data(), out.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  return dev;
+}
+
+}  // namespace
+
+extern "C" {
+
+int trisk_dist_create(const TriskCoefficients* local, const TriskConfig* cfg, const TriskHalo* halo,
+                      TriskDist** out) {
+  TRISK_API_BEGIN
+  if (!out || !cfg || !halo || !local) throw Error(TRISK_ERR_ARGUMENT, "NULL argument");
+  *out = nullptr;
+  Coefficients C = coefficients_from_abi(local);
+  if (halo->ne_owned < 0 || halo->ne_owned > C.ne || halo->nc_owned < 0 || halo->nc_owned > C.nc)
+    throw Error(TRISK_ERR_ARGUMENT, "owned counts out of range");
+  if (halo->nneighbors < 0) throw Error(TRISK_ERR_ARGUMENT, "negative neighbour count");
+  auto d = std::make_unique<TriskDist>();
+  d->m = std::make_unique<TriskModel>();
+  TriskModel& m = *d->m;
+  m.device = cfg->device;
+  m.ne_own = halo->ne_owned;
+  m.nc_own = halo->nc_owned;
+  std::vector<V3> centroids;
+  const bool reorder = cfg->reorder && cfg->cell_positions;
+  if (reorder) {
+    centroids.resize(C.nc);
+    std::memcpy(centroids.data(), cfg->cell_positions, C.nc * sizeof(V3));
+  }
+  finish_create(m, C, reorder ? &centroids : nullptr, cfg);
+  DeviceGuard guard(m.device);
+  d->send_idx = halo_indices(m, halo->send_offsets, halo->send_index, halo->nneighbors, true, d->nsend);
+  d->recv_idx = halo_indices(m, halo->recv_offsets, halo->recv_index, halo->nneighbors, false, d->nrecv);
+  d->send_dev = m.alloc<double>(std::max<int64_t>(d->nsend, 1));
+  d->recv_dev = m.alloc<double>(std::max<int64_t>(d->nrecv, 1));
+  CUDA_CHECK(cudaMallocHost((void**)&d->send_host, std::max<int64_t>(d->nsend, 1) * sizeof(double)));
+  CUDA_CHECK(cudaMallocHost((void**)&d->recv_host, std::max<int64_t>(d->nrecv, 1) * sizeof(double)));
+  *out = d.release();
+  TRISK_API_END
+}
+
+void trisk_dist_destroy(TriskDist* dist) { delete dist; }
+
+int trisk_dist_set_exchange(TriskDist* dist, TriskExchangeFn fn, void* user, int32_t mode) {
+  TRISK_API_BEGIN
+  TriskDist& d = *checked_dist(dist);
+  if (mode < TRISK_EXCHANGE_HOST || mode > TRISK_EXCHANGE_DEVICE_GRAPH)
+    throw Error(TRISK_ERR_ARGUMENT, "unknown exchange mode");
+  d.fn = fn;
+  d.user = user;
+  d.mode = mode;
+  if (d.graph) {
+    cudaGraphExecDestroy(d.graph);
+    d.graph = nullptr;
+  }
+  TRISK_API_END
+}
+
+int trisk_dist_tendency(TriskDist* dist, const double* y, double* dy) {
+  TRISK_API_BEGIN
+  TriskDist& d = *checked_dist(dist);
+  TriskModel& m = *d.m;
+  if (!y || !dy) throw Error(TRISK_ERR_ARGUMENT, "NULL state");
+  DeviceGuard guard(m.device);
+  state_in(m, y, m.y);
+  dist_exchange(d, m.y);
+  DevStage S{};
+  S.u = m.y;
+  S.h = m.y + m.ne;
+  S.dy = m.dy;
+  S.flag = m.flag;
+  enqueue_tendency(m, S, EPI_TENDENCY);
+  state_out(m, dy, m.dy);
+  CUDA_CHECK(cudaStreamSynchronize(m.stream));
+  TRISK_API_END
+}
+
+int trisk_dist_rk4_step(TriskDist* dist, double* y, double dt, int64_t nsteps) {
+  TRISK_API_BEGIN
+  TriskDist& d = *checked_dist(dist);
+  TriskModel& m = *d.m;
+  if (!y) throw Error(TRISK_ERR_ARGUMENT, "NULL state");
+  if (nsteps < 0 || !std::isfinite(dt)) throw Error(TRISK_ERR_ARGUMENT, "bad dt or step count");
+  DeviceGuard guard(m.device);
+  if (nsteps == 0) return TRISK_OK;
+  state_in(m, y, m.y);
+  if (d.mode == TRISK_EXCHANGE_DEVICE_GRAPH) {
+    dist_ensure_graph(d, dt);
+    for (int64_t s = 0; s < nsteps; ++s) {
+      CUDA_CHECK(cudaGraphLaunch(d.graph, m.stream));
+      m.launches += d.graph_launches;
+    }
+  } else {
+    for (int64_t s = 0; s < nsteps; ++s) dist_enqueue_step(d, dt);
+  }
+  state_out(m, y, m.y);
+  check_flag(m);
+  TRISK_API_END
+}
+
+int trisk_dist_stream(TriskDist* dist, void** stream) {
+  TRISK_API_BEGIN
+  TriskDist& d = *checked_dist(dist);
+  if (!stream) throw Error(TRISK_ERR_ARGUMENT, "NULL argument");
+  *stream = (void*)d.m->stream;
+  TRISK_API_END
+}
+
+int64_t trisk_dist_launch_count(TriskDist* dist) { return dist && dist->m ? dist->m->launches : -1; }
 
 }  // extern "C"

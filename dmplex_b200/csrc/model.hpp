@@ -73,6 +73,7 @@ struct TriskModel {
   int pv = 0, ke = 0;  // pv: the kernels' PvMode (PVM_GASSMANN_DERIVED when the table allows it)
   double alpha = 1.0, gravity = 1.0;
   int64_t nc = 0, ne = 0, nv = 0, N = 0;
+  int64_t nc_own = -1, ne_own = -1;  // owned cells and edges come first (-1: all are owned)
   int block[3] = {128, 128, 128};  // threads per block of k_vertex, k_flux, k_tend
   bool use_graph = true, use_pdl = true, identity = true;
   trisk::Coefficients C;  // file numbering, 0-based (kept for export)

@@ -16,17 +16,22 @@ the owned entities first; the state [u; h] is exchanged once per tendency (one m
 neighbour: its edges, then its cells) and the tendencies of ghosts are zeroed, so the owned
 values are those of the undivided model bit for bit.
 
-The local tendency runs on the rank's GPU through the library (a model built from the
-restricted tables with TRiSKShallowWater.from_coefficients); the exchange uses
-torch.distributed point-to-point messages (NCCL between GPUs, or gloo through host memory).
+The rank's part runs in the library (trisk_dist_*: its tendency and RK4 steps with the stage
+updates fused, the ghost tendencies zeroed in the tendency kernel, the halo packed and unpacked
+by gather kernels), which calls back into HaloExchange once per tendency for the exchange
+itself: torch.distributed point-to-point messages, on the library's stream with NCCL between
+GPUs, or through host memory with gloo.
 """
 from __future__ import annotations
 
+import ctypes as C
 import math
 
 import numpy as np
 
-from .model import TRiSKShallowWater, model_tables
+from . import _lib
+from ._lib import check, lib
+from .model import _alpha, _coefficients_struct, _pv_code, _state, model_tables
 
 # ------------------------------------------------------------------ partition (Partition.jl)
 
@@ -253,19 +258,144 @@ def local_coefficients(coeffs: dict, dist: TRiSKDistribution) -> dict:
     return out
 
 
-class _Centers:  # what TRiSKShallowWater.from_coefficients reads for its Hilbert order
-    def __init__(self, centers):
-        self.centers = centers
+def halo_lists(dist: TRiSKDistribution):
+    """The state halo of `dist` as the library's TriskHalo arrays: CSR offsets and 1-based
+    local state indices, neighbour after neighbour in dist.state_neighbors' order."""
+    def csr(lists):
+        offsets = np.zeros(len(lists) + 1, dtype=np.int64)
+        offsets[1:] = np.cumsum([len(x) for x in lists])
+        index = np.concatenate(lists).astype(np.int64) + 1 if lists else np.zeros(0, np.int64)
+        return offsets, np.ascontiguousarray(index)
+    so, si = csr(dist.state_send)
+    ro, ri = csr(dist.state_recv)
+    return so, si, ro, ri
+
+
+class HaloExchange:
+    """The exchange the library calls once per tendency (exchange!, Halo.jl:80-99): `send`
+    holds the packed owned values for every neighbour in turn, `recv` gets the neighbours'
+    values of my ghosts in the same order. One message pair per neighbour through
+    torch.distributed; host arrays (gloo), or device tensors on `stream` (NCCL)."""
+
+    def __init__(self, dist: TRiSKDistribution, group=None):
+        self.group = group
+        self.peers = list(dist.state_neighbors)
+        self.send_counts = [len(x) for x in dist.state_send]
+        self.recv_counts = [len(x) for x in dist.state_recv]
+
+    def __call__(self, send, recv, stream=None) -> None:
+        import torch
+        import torch.distributed as tdist
+        ops = []
+        a = b = 0
+        ctx = torch.cuda.stream(torch.cuda.ExternalStream(stream)) if stream else _nullcontext()
+        with ctx:
+            for q, ns, nr in zip(self.peers, self.send_counts, self.recv_counts):
+                peer = tdist.get_global_rank(self.group, q) if self.group is not None else q
+                if ns:
+                    ops.append(tdist.P2POp(tdist.isend, send[a:a + ns], peer, self.group))
+                if nr:
+                    ops.append(tdist.P2POp(tdist.irecv, recv[b:b + nr], peer, self.group))
+                a, b = a + ns, b + nr
+            if ops:
+                for req in tdist.batch_isend_irecv(ops):
+                    req.wait()
+
+
+class _nullcontext:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        return False
+
+
+class _CudaBuffer:
+    """A device buffer given by the library as a torch tensor (no copy)."""
+
+    def __init__(self, address: int, n: int):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f8", "data": (address, False), "version": 3}
+
+
+class _DistModel:
+    """The library's part of a distributed model (trisk_dist_*) with its exchange callback."""
+
+    def __init__(self, coefficients, dist, centers, exchange: HaloExchange, device_exchange: bool, *, gravity,
+                 omega, pv_flux, kinetic_energy, device):
+        pv, alpha = _pv_code(pv_flux), _alpha(kinetic_energy)
+        cs, self._keep = _coefficients_struct(coefficients, pv, alpha, gravity)
+        cfg = _lib.TriskConfig()
+        cfg.pv_flux, cfg.reorder, cfg.alpha, cfg.gravity, cfg.omega = pv, 1, alpha, gravity, omega
+        cfg.device, cfg.use_graph, cfg.use_pdl, cfg.block = device, 1, 1, 0
+        pos = np.ascontiguousarray(centers, dtype=np.float64)
+        self._keep.append(pos)
+        cfg.cell_positions = pos.ctypes.data
+        so, si, ro, ri = halo_lists(dist)
+        self._keep += [so, si, ro, ri]
+        halo = _lib.TriskHalo()
+        halo.ne_owned, halo.nc_owned = dist.edges.n_owned, dist.cells.n_owned
+        halo.nneighbors = len(dist.state_neighbors)
+        halo.send_offsets, halo.send_index = so.ctypes.data, si.ctypes.data
+        halo.recv_offsets, halo.recv_index = ro.ctypes.data, ri.ctypes.data
+        h = C.c_void_p()
+        check(lib.trisk_dist_create(C.byref(cs), C.byref(cfg), C.byref(halo), C.byref(h)))
+        self._h = h
+        self.exchange = exchange
+        self._error = None
+        self._callback = _lib.EXCHANGE_FN(self._exchange)  # kept alive with the model
+        mode = _lib.EXCHANGE_DEVICE if device_exchange else _lib.EXCHANGE_HOST
+        check(lib.trisk_dist_set_exchange(h, self._callback, None, mode))
+        self.state_size = len(dist.edges) + len(dist.cells)
+
+    def _exchange(self, user, send, nsend, recv, nrecv, stream):
+        try:
+            if stream:
+                import torch
+                s = torch.as_tensor(_CudaBuffer(send, nsend), device="cuda") if nsend else None
+                r = torch.as_tensor(_CudaBuffer(recv, nrecv), device="cuda") if nrecv else None
+            else:
+                import torch
+                s = torch.from_numpy(np.ctypeslib.as_array((C.c_double * max(nsend, 1)).from_address(send)))[:nsend]
+                r = torch.from_numpy(np.ctypeslib.as_array((C.c_double * max(nrecv, 1)).from_address(recv)))[:nrecv]
+            self.exchange(s, r, stream)
+            return 0
+        except Exception as exc:  # noqa: BLE001 - re-raised by _call once the library returns
+            self._error = exc
+            return 1
+
+    def _call(self, fn, *args):
+        status = fn(self._h, *args)
+        if self._error is not None:
+            err, self._error = self._error, None
+            raise err
+        check(status)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib.trisk_dist_destroy(self._h)
+            self._h = None
+
+    def tendency(self, dy, y):
+        self._call(lib.trisk_dist_tendency, _state(y, self), _state(dy, self))
+
+    def rk4_step(self, y, dt: float, nsteps: int):
+        self._call(lib.trisk_dist_rk4_step, _state(y, self), float(dt), int(nsteps))
+
+    def launch_count(self) -> int:
+        return int(lib.trisk_dist_launch_count(self._h))
 
 
 class DistributedShallowWater:
     """One rank's part of a TRiSK shallow-water model (TRiSKShallowWater(grid; comm, part)).
 
     group: a torch.distributed process group (None: the default group); part: the cell
-    partition (default: equal_area_partition). `engine`, if given, is called with the local
-    tables and returns the object whose tendency(y) -> dy (numpy) replaces the local GPU
-    model (the tests pass the CPU oracle). States are local [u; h] vectors, owned entities
-    first: numpy arrays, or CUDA float64 tensors for the GPU model.
+    partition (default: equal_area_partition). The rank's part runs in the library on GPU
+    `device`; its halo exchange is HaloExchange over the group (on the GPU with NCCL, through
+    host memory with gloo). `engine`, if given, is called with the local tables and returns
+    the object whose tendency(y) -> dy (numpy) replaces the library's part (the tests pass the
+    CPU oracle); the RK4 steps and the exchange are then done here, with the same HaloExchange
+    on numpy buffers. States are local [u; h] vectors, owned entities first: numpy arrays, or
+    CUDA float64 tensors.
     """
 
     def __init__(self, grid, *, gravity=1.0, omega=1.0, pv_flux="trisk", kinetic_energy="cell", part=None,
@@ -284,11 +414,12 @@ class DistributedShallowWater:
         self.coefficients = local_coefficients(self.global_coefficients, self.dist)
         self.ne, self.nc = len(self.dist.edges), len(self.dist.cells)
         self.state_size = self.ne + self.nc
+        self.exchange = HaloExchange(self.dist, group)
         if engine is None:
-            centers = _Centers(np.ascontiguousarray(grid.centers[self.dist.cells.global_ids]))
-            self.engine = TRiSKShallowWater.from_coefficients(self.coefficients, grid=centers, device=device,
-                                                              gravity=gravity, pv_flux=pv_flux,
-                                                              kinetic_energy=kinetic_energy)
+            backend = tdist.get_backend(group) if tdist.is_initialized() else "gloo"
+            self.engine = _DistModel(self.coefficients, self.dist, grid.centers[self.dist.cells.global_ids],
+                                     self.exchange, backend == "nccl", gravity=gravity, omega=omega,
+                                     pv_flux=pv_flux, kinetic_energy=kinetic_energy, device=device)
         else:
             self.engine = engine(self.coefficients)
 
@@ -322,55 +453,44 @@ class DistributedShallowWater:
         return out
 
     # ---------------------------------------------------------------- halo exchange
-    def exchange_state(self, y) -> None:
-        """Ghost values of the local state from their owners: one message per neighbour
-        (exchange_state!, TRiSKShallowWater.jl:201). A CUDA state goes through host memory
-        when the group's backend is gloo."""
-        if self.nranks == 1 or not self.dist.state_neighbors:
-            return
+    def exchange_state(self, y: np.ndarray) -> None:
+        """Ghost values of a numpy local state from their owners (exchange_state!,
+        TRiSKShallowWater.jl:201): the library's pack, exchange and unpack, restated on the
+        host for an injected engine."""
         import torch
-        import torch.distributed as tdist
-        is_t = hasattr(y, "data_ptr")
-        host = not is_t or (y.is_cuda and tdist.get_backend(self.group) == "gloo")
-        yt = torch.from_numpy(y) if not is_t else y
-        ops, recv_bufs = [], []
-        for q, send, recv in zip(self.dist.state_neighbors, self.dist.state_send, self.dist.state_recv):
-            si = torch.from_numpy(send).to(yt.device)
-            buf = yt.index_select(0, si)
-            rb = torch.empty(len(recv), dtype=yt.dtype, device=yt.device)
-            if host:
-                buf, rb = buf.cpu(), rb.cpu()
-            peer = tdist.get_global_rank(self.group, q) if self.group is not None else q
-            ops.append(tdist.P2POp(tdist.isend, buf, peer, self.group))
-            ops.append(tdist.P2POp(tdist.irecv, rb, peer, self.group))
-            recv_bufs.append((recv, rb))
-        for req in tdist.batch_isend_irecv(ops):
-            req.wait()
-        for recv, rb in recv_bufs:
-            ri = torch.from_numpy(recv).to(yt.device)
-            yt.index_copy_(0, ri, rb.to(yt.device))
+        send = np.concatenate(self.dist.state_send) if self.dist.state_send else np.zeros(0, np.int64)
+        recv = np.concatenate(self.dist.state_recv) if self.dist.state_recv else np.zeros(0, np.int64)
+        if len(send) == 0 and len(recv) == 0:
+            return
+        buf = torch.from_numpy(np.ascontiguousarray(y[send]))
+        out = torch.empty(len(recv), dtype=torch.float64)
+        self.exchange(buf, out)
+        y[recv] = out.numpy()
 
     # ---------------------------------------------------------------- tendency, RK4
     def tendency(self, dy, y):
         """tendency!(dy, y, m) of the local state (TRiSKShallowWater.jl:379-394): exchange,
-        local tendency, ghost tendencies zeroed."""
-        from .model import tendency as _tendency
+        local tendency, ghost tendencies zero."""
+        if isinstance(self.engine, _DistModel):
+            self.engine.tendency(dy, y)
+            return dy
         self.exchange_state(y)
-        if isinstance(self.engine, TRiSKShallowWater):
-            _tendency(dy, y, self.engine)
-        else:
-            dy[:] = self.engine.tendency(_to_numpy(y))
+        dy[:] = self.engine.tendency(_to_numpy(y))
         d = self.dist
         dy[d.edges.n_owned:self.ne] = 0.0
         dy[self.ne + d.cells.n_owned:] = 0.0
         return dy
 
     def rk4_step(self, y, dt: float, nsteps: int = 1):
-        """rk4_step! (RungeKutta.jl:18-29) with a distributed tendency; the stage sums keep
-        the reference's association, so owned values match the undivided model bit for bit."""
+        """rk4_step! (RungeKutta.jl:18-29) with a distributed tendency: in the library (stage
+        updates fused, graph-free because of the exchange), or here for an injected engine with
+        the stage sums in the reference's association; owned values match the undivided model
+        bit for bit."""
+        if isinstance(self.engine, _DistModel):
+            self.engine.rk4_step(y, dt, nsteps)
+            return y
         half, sixth = dt / 2, dt / 6
-        like = (lambda: y.clone()) if hasattr(y, "clone") else (lambda: y.copy())
-        k1, k2, k3, k4, st = like(), like(), like(), like(), like()
+        k1, k2, k3, k4, st = (y.copy() for _ in range(5))
         for _ in range(nsteps):
             self.tendency(k1, y)
             st[:] = y + half * k1

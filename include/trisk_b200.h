@@ -44,7 +44,8 @@ size_t trisk_last_error(char* buf, size_t len);
 int32_t trisk_abi_version(void);
 /* sizeof of the structs below, so a binding can check its layout */
 int32_t trisk_struct_size(int32_t which); /* 0 TriskGrid, 1 TriskCoefficients, 2 TriskConfig, 3 TriskPlex,
-                                          4 TriskIconTables, 5 TriskMpasTables, 6 TriskMpasFields */
+                                          4 TriskIconTables, 5 TriskMpasTables, 6 TriskMpasFields,
+                                          7 TriskHalo */
 
 /* ---- mesh generation (set-up, host) ------------------------------------------------
  * Replaces create_hexagon_mesh(n; centroidal)   src/Grids/Hexagonal.jl:11-17
@@ -351,6 +352,56 @@ int trisk_mpas_stream(TriskMpas* ops, void** stream);
 int trisk_mpas_synchronize(TriskMpas* ops);
 int64_t trisk_mpas_launch_count(TriskMpas* ops);
 
+/* ---- one rank's part of a distributed model -------------------------------------------
+ * Replaces TRiSKShallowWater(grid; comm, part)     src/FiniteVolumes/TRiSKShallowWater.jl:121-168
+ * with its TRiSKDistribution                      src/FiniteVolumes/TRiSKDistribution.jl:70-106
+ * and tendency! with exchange_state!              TRiSKShallowWater.jl:201,379-394
+ * (exchange!, src/Parallel/Halo.jl:80-99) and rk4_step! (RungeKutta.jl:18-29) on it.
+ * The model holds the rank's owned entities and its ghosts in local numbering, owned first:
+ * its tables are the global ones restricted to the local entities (TriskCoefficients in
+ * local numbering: local_table, TRiSKDistribution.jl:108-119). Before every tendency the ghost
+ * values of the stage state are exchanged once (one packed buffer of all neighbours); the
+ * ghosts' tendencies are zero, so owned values follow the undivided model bit for bit. */
+typedef struct {
+  int64_t ne_owned, nc_owned; /* local edges 1..ne_owned and cells 1..nc_owned are owned */
+  int32_t nneighbors, pad_;
+  /* neighbour k sends/receives the local state entries index[offsets[k] .. offsets[k+1]-1]
+   * (offsets 0-based, nneighbors + 1 of them; indices 1-based into the local [u; h]:
+   * edges 1..ne, cells ne+1..ne+nc). Sent entries are owned, received entries are ghosts. */
+  const int64_t* send_offsets;
+  const int64_t* send_index;
+  const int64_t* recv_offsets;
+  const int64_t* recv_index;
+} TriskHalo;
+/* The caller's exchange (the reference's MPI exchange!): fill recv (nrecv values, neighbour
+ * after neighbour in the halo's order) from the neighbours, sending them `send` (nsend values,
+ * in the same order). Returns 0, or a status the library passes on. */
+typedef int (*TriskExchangeFn)(void* user, const double* send, int64_t nsend, double* recv, int64_t nrecv,
+                               void* stream);
+enum {
+  TRISK_EXCHANGE_HOST = 0,   /* send/recv are host buffers; the device work before is finished */
+  TRISK_EXCHANGE_DEVICE = 1, /* device buffers; the callback orders its transfers on `stream`
+                                (a cudaStream_t), e.g. NCCL send/recv on that stream */
+  TRISK_EXCHANGE_DEVICE_GRAPH = 2 /* as DEVICE, and each RK4 step is captured once per dt as a
+                                     CUDA graph with the callback's stream work in it, so the
+                                     callback must enqueue only capturable work */
+};
+typedef struct TriskDist TriskDist;
+/* cfg: as trisk_model_create_from_coefficients (cell_positions, if given, are the local cells'
+ * centers for the internal numbering, which keeps owned entities first). */
+int trisk_dist_create(const TriskCoefficients* local, const TriskConfig* cfg, const TriskHalo* halo,
+                      TriskDist** out);
+void trisk_dist_destroy(TriskDist* dist);
+int trisk_dist_set_exchange(TriskDist* dist, TriskExchangeFn fn, void* user, int32_t mode);
+/* tendency! of the local state y (host or device; the ghost values used are the exchanged
+ * ones, y itself is not changed); dy's ghost entries are 0. */
+int trisk_dist_tendency(TriskDist* dist, const double* y, double* dy);
+/* rk4_step! nsteps times in place on the local state (host or device), the stage updates
+ * fused into the tendency phase as in trisk_rk4_step. */
+int trisk_dist_rk4_step(TriskDist* dist, double* y, double dt, int64_t nsteps);
+int trisk_dist_stream(TriskDist* dist, void** stream);
+int64_t trisk_dist_launch_count(TriskDist* dist);
+
 /* ---- batched ensembles ------------------------------------------------------------
  * No counterpart in the reference, which runs one model per process (examples/
  * trisk_shallow_water.jl:71-111); each member's arithmetic is that of rk4_step!
@@ -389,7 +440,7 @@ int trisk_ensemble_set_block(TriskEnsemble* ensemble, const int32_t block[3]);
 int trisk_ensemble_get_block(TriskEnsemble* ensemble, int32_t block[3]);
 /* Members per slice of every group (ngroups values; the last slice of a group may have
  * fewer). The default minimizes a byte estimate: tables streamed once per slice against the
- * part of a slice's state and work vectors beyond a 96 MB L2 budget. Setting them keeps the
+ * part of a slice's gathered state and work vectors beyond a 48 MB L2 budget. Setting them keeps the
  * members' states; results are the same bit for bit for every slicing. */
 int trisk_ensemble_set_slices(TriskEnsemble* ensemble, const int32_t* members_per_slice);
 int trisk_ensemble_get_slices(TriskEnsemble* ensemble, int32_t* members_per_slice);
@@ -452,6 +503,8 @@ int trisk_closure_gradients(TriskClosure* closure, const void* X, const float* t
 int trisk_closure_adam(TriskClosure* closure, float lr, float beta1, float beta2, float eps);
 int trisk_closure_synchronize(TriskClosure* closure);
 int trisk_closure_stream(TriskClosure* closure, void** stream);
+/* Launch shape of inference: the persistent grid's CTAs per SM (seven on a B200) and the SMs. */
+int trisk_closure_info(TriskClosure* closure, int32_t* forward_ctas_per_sm, int32_t* sms);
 /* Test of the bounded tensor-core wait (no reference counterpart): the next inference call of
  * this closure leaves the first tensor-core operation of tile `tile` (rows 128 tile ..) un-issued,
  * so that tile's wait runs out after half a second and the call returns TRISK_ERR_TIMEOUT; the

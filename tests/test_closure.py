@@ -64,6 +64,7 @@ def test_forward_and_gradients_match_oracle(require_gpu, n):
     p = co.init_params(7)
     p[co.NH * co.NIN:co.NH * co.NIN + co.NH] = 0.1  # nonzero b1
     mlp = cl.ClosureMLP(p.astype(np.float32))
+    assert mlp.info()["forward_ctas_per_sm"] >= 6  # the persistent grid fills the SMs
     Xd = torch.from_numpy(X.astype(np.float32)).to(torch.bfloat16).cuda().contiguous()
     Td = torch.from_numpy(T.astype(np.float32)).cuda().contiguous()
     pf = mlp.params().astype(np.float64)
