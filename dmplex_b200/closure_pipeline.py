@@ -216,9 +216,12 @@ def build_dataset(gc, Y0, dF, dQ, ens, device=0, sample=2_000_000):
     return X, Tn, norm
 
 
-def train(mlp: ClosureMLP, X, T, epochs=3, batch=65536, lr=1e-3, holdout=0.05, seed=0):
+def train(mlp: ClosureMLP, X, T, epochs=3, batch=65536, lr=1e-3, holdout=0.05, seed=0, input_noise=0.0):
     """Adam on random batches; returns per-epoch mean losses, the held-out loss and the
-    held-out loss of predicting zero (the coarse model without the closure)."""
+    held-out loss of predicting zero (the coarse model without the closure). input_noise > 0
+    adds Gaussian noise of that standard deviation to the normalized training inputs (not to
+    the held-out rows): a regularization towards states the coarse run visits but the
+    coarse-grained fine run does not."""
     import torch
     g = torch.Generator(device=X.device)
     g.manual_seed(seed)
@@ -236,7 +239,11 @@ def train(mlp: ClosureMLP, X, T, epochs=3, batch=65536, lr=1e-3, holdout=0.05, s
         for b in range(steps):
             idx = order[b * batch:(b + 1) * batch]
             rate = lr * 0.5 * (1 + np.cos(np.pi * k / total))  # cosine schedule
-            losses.append(mlp.train_step(X[idx].contiguous(), T[idx].contiguous(), rate))
+            xb = X[idx]
+            if input_noise > 0:
+                noise = torch.randn(xb.shape, device=X.device, generator=g, dtype=torch.float32)
+                xb = (xb.float() + input_noise * noise).to(torch.bfloat16)
+            losses.append(mlp.train_step(xb.contiguous(), T[idx].contiguous(), rate))
             k += 1
         history.append(float(np.mean(losses)))
     held = []
@@ -370,6 +377,27 @@ def plain_level_errors(gf, gc, gm, seeds, days, dt, daily_truth, device=0, state
             "cells": int(gm.nc), "dt": 86400 / steps_day, "members": S, "state_bits": state_bits}
 
 
+def member_day_cost(g, members, dt, state_bits=64, mlp=None, norm=None, steps=96, device=0, seed=3) -> float:
+    """GPU seconds per member and simulated day of a `members`-member ensemble on grid g at
+    time step dt (with the closure if mlp is given), from `steps` timed steps after a warm-up."""
+    import torch
+    si = w.si_parameters()
+    m = TRiSKShallowWater(g, pv_flux=PV, kinetic_energy=KE, device=device, **si)
+    ens = Ensemble([(m, members, dt, steps + 2)], state_bits=state_bits)
+    for k, y in enumerate(w.ensemble_members(g, members, seed=seed, degree=8, rms_range=(100.0, 100.0))):
+        ens.set_member(0, k, y)
+    if mlp is not None:
+        ens.set_closure(0, mlp, edge_geometry(g), norm)
+    ens.run(2)
+    stream = torch.cuda.ExternalStream(ens.stream(), device=device)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    ens.run_async(steps)
+    b.record(stream)
+    ens.synchronize()
+    return a.elapsed_time(b) / 1e3 / steps * (86400 / dt) / members
+
+
 def equal_error_cost(errors: dict, costs: dict, target: float) -> float:
     """GPU seconds per member-day the plain method needs to reach the h error `target`:
     log-linear interpolation (or extrapolation) of cost against error between the two plain
@@ -382,13 +410,15 @@ def equal_error_cost(errors: dict, costs: dict, target: float) -> float:
 
 
 def calibrate(gf, gc, mlp, norm, seeds=(501, 502), days=2, coarse_dt=150.0, fine_dt=20.0,
-              scales=(0.0, 0.05, 0.1, 0.2, 0.4, 1.0), device=0, log=print, work_free=False):
+              scales=(0.0, 0.05, 0.1, 0.2, 0.4, 1.0), device=0, log=print, work_free=False, daily=None):
     """A-posteriori choice of the momentum correction's scale: coarse runs with the closure
     (no fallback, mass-flux part unscaled) from validation seeds, none of them a training or
-    evaluation seed, against their coarse-grained fine runs; the scale with the smallest mean
-    h error over the days wins (a run that turns non-finite loses). Returns (scale, table)."""
-    _, _, _, daily, _ = fine_snapshots(gf, gc, list(seeds), days, 0, dt_fine=fine_dt, device=device,
-                                       spinup_days=0.0, record_days=True)
+    evaluation seed, against their coarse-grained fine runs (daily: those, if already made);
+    the scale with the smallest mean h error over the days wins (a run that turns non-finite
+    loses). Returns (scale, table)."""
+    if daily is None:
+        _, _, _, daily, _ = fine_snapshots(gf, gc, list(seeds), days, 0, dt_fine=fine_dt, device=device,
+                                           spinup_days=0.0, record_days=True)
     table = {}
     for sc in scales:
         r = run_coarse(gc, daily[0], days, coarse_dt, daily, mlp, norm, drift_per_day=np.inf, device=device,
@@ -402,11 +432,14 @@ def calibrate(gf, gc, mlp, norm, seeds=(501, 502), days=2, coarse_dt=150.0, fine
 
 def pipeline(fine_level=8, coarse_level=6, train_seeds=32, train_days=10, snapshots=2000, eval_seeds=4,
              eval_days=10, coarse_dt=150.0, window=1800.0, fine_dt=20.0, epochs=3, device=0, out_params=None,
-             target="tendency", log=print):
+             target="tendency", log=print, input_noise=(0.0,), calibrate_days=4,
+             scales=(0.0, 0.05, 0.1, 0.15, 0.2, 0.25, 0.3)):
     """The whole closure experiment; returns a JSON-able summary. target "tendency": the
     residual is the coarse model's missing tendency at the coarse-grained state; "window":
     the mean missing tendency over `window` seconds (window / fine_dt fine steps, window /
-    coarse_dt coarse steps)."""
+    coarse_dt coarse steps). One network is trained, calibrated and evaluated per value of
+    input_noise on the same data; the first is the summary's, the others follow under
+    "variants" (out_params gets the first)."""
     import torch
     if target not in ("tendency", "window"):
         raise ValueError("target must be 'tendency' or 'window'")
@@ -425,41 +458,60 @@ def pipeline(fine_level=8, coarse_level=6, train_seeds=32, train_days=10, snapsh
     del ens, Y1
     torch.cuda.empty_cache()
     log(f"dataset: {X.shape[0]} rows")
-    mlp = ClosureMLP(device=device, seed=0)
-    history, held, zero = train(mlp, X, T, epochs=epochs)
-    skill = output_skill(mlp, X, T)
-    log(f"training loss per epoch {history}, held-out {held:.4f} (without the closure {zero:.4f}), "
-        f"skill (mass flux, momentum) {skill}")
-    scale, table = calibrate(gf, gc, mlp, norm, coarse_dt=coarse_dt, fine_dt=fine_dt, device=device, log=log)
-    norm = np.array(norm, dtype=np.float64)
-    norm[2 * NFEAT + 1] *= scale  # the calibrated momentum scale is part of the saved closure
-    if out_params:
-        np.savez(out_params, params=mlp.params(), norm=norm, fine_level=fine_level, coarse_level=coarse_level,
-                 window=window if target == "window" else 0.0, target=target, momentum_scale=scale)
+    _, _, _, cal_daily, _ = fine_snapshots(gf, gc, [501, 502], calibrate_days, 0, dt_fine=fine_dt,
+                                           device=device, spinup_days=0.0, record_days=True)
+    eval_list = list(range(1001, 1001 + eval_seeds))
+    _, _, _, eval_daily, fine_eval_s = fine_snapshots(gf, gc, eval_list, eval_days, 0, dt_fine=fine_dt,
+                                                      device=device, spinup_days=0.0, record_days=True)
+    results = []
+    for noise in input_noise:
+        mlp = ClosureMLP(device=device, seed=0)
+        history, held, zero = train(mlp, X, T, epochs=epochs, input_noise=noise)
+        skill = output_skill(mlp, X, T)
+        log(f"input noise {noise}: training loss per epoch {history}, held-out {held:.4f} (without the closure "
+            f"{zero:.4f}), skill (mass flux, momentum) {skill}")
+        scale, table = calibrate(gf, gc, mlp, norm, days=calibrate_days, coarse_dt=coarse_dt, fine_dt=fine_dt,
+                                 scales=scales, device=device, log=log, daily=cal_daily)
+        vnorm = np.array(norm, dtype=np.float64)
+        vnorm[2 * NFEAT + 1] *= scale  # the calibrated momentum scale is part of the saved closure
+        if out_params and not results:
+            np.savez(out_params, params=mlp.params(), norm=vnorm, fine_level=fine_level, coarse_level=coarse_level,
+                     window=window if target == "window" else 0.0, target=target, momentum_scale=scale,
+                     input_noise=noise)
+        r = {"input_noise": noise, "train_loss": history, "heldout_loss": held, "heldout_loss_without_closure": zero,
+             "output_skill": skill, "calibrated_momentum_scale": scale, "calibration_mean_h_l2": table,
+             "calibration_days": calibrate_days}
+        r.update(evaluate(gf, gc, mlp, vnorm, eval_seeds, eval_days, coarse_dt, fine_dt, device, log,
+                          daily=eval_daily, fine_eval_seconds=fine_eval_s))
+        results.append(r)
     del X, T
     torch.cuda.empty_cache()
     summary = {
         "fine_level": fine_level, "coarse_level": coarse_level, "train_seeds": train_seeds,
         "train_days": train_days, "training_snapshots": int(Y0.shape[1]), "target": target,
         "window_seconds": delta if target == "window" else None,
-        "coarse_steps_per_window": coarse_steps if target == "window" else None, "epochs": epochs, "train_loss": history, "heldout_loss": held,
-        "heldout_loss_without_closure": zero, "output_skill": skill, "fine_training_gpu_seconds": fine_train_s,
-        "calibrated_momentum_scale": scale, "calibration_mean_h_l2": table,
+        "coarse_steps_per_window": coarse_steps if target == "window" else None, "epochs": epochs,
+        "fine_training_gpu_seconds": fine_train_s, "gelu": "tanh form (Hendrycks and Gimpel 2016)",
     }
-    summary.update(evaluate(gf, gc, mlp, norm, eval_seeds, eval_days, coarse_dt, fine_dt, device, log))
+    summary.update(results[0])
+    if len(results) > 1:
+        summary["variants"] = results[1:]
     summary["wall_seconds"] = time.perf_counter() - t_start
     return summary
 
 
 def evaluate(gf, gc, mlp, norm, eval_seeds=4, eval_days=10, coarse_dt=150.0, fine_dt=20.0, device=0, log=print,
-             work_free=False):
+             work_free=False, daily=None, fine_eval_seconds=None):
     """Coarse runs from the coarse-grained state of held-out seeds against the coarse-grained
-    fine run: plain (FP64 and FP32 state), and with FP32 state the closure with the energy-
-    drift fallback, without it, evaluated at every RK4 stage, and the mass-flux correction
-    alone."""
+    fine run (daily: that run's daily coarse-grained states, if already made): plain (FP64 and
+    FP32 state), and with FP32 state the closure with the energy-drift fallback, without it,
+    evaluated at every RK4 stage, and the mass-flux correction alone; then the equal-error
+    table."""
     eval_list = list(range(1001, 1001 + eval_seeds))
-    _, _, _, daily, fine_eval_s = fine_snapshots(gf, gc, eval_list, eval_days, 0, dt_fine=fine_dt, device=device,
-                                                 spinup_days=0.0, record_days=True)
+    fine_eval_s = fine_eval_seconds
+    if daily is None:
+        _, _, _, daily, fine_eval_s = fine_snapshots(gf, gc, eval_list, eval_days, 0, dt_fine=fine_dt,
+                                                     device=device, spinup_days=0.0, record_days=True)
     out = {"eval_seeds": eval_seeds, "eval_days": eval_days, "coarse_dt": coarse_dt, "fine_dt": fine_dt,
            "fine_gpu_seconds_per_member_day": fine_eval_s / (eval_seeds * eval_days)}
     init = daily[0]
@@ -481,7 +533,40 @@ def evaluate(gf, gc, mlp, norm, eval_seeds=4, eval_days=10, coarse_dt=150.0, fin
         log(f"{name}: h L2 per day {[round(float(np.mean(x)), 2) for x in r['h_l2']]}, vorticity "
             f"{[float('%.3g' % np.mean(x)) for x in r['zeta_l2']]}, fallback {r['fallback_members']}, "
             f"diverged on day {r['diverged_on_day']}")
+    out.update(equal_error_table(gf, gc, mlp, norm, eval_list, eval_days, coarse_dt, daily, out, device, log))
     return out
+
+
+def equal_error_table(gf, gc, mlp, norm, seeds, days, coarse_dt, daily, runs, device=0, log=print):
+    """The north star's comparison at equal h L2 error: plain FP64 runs one level finer than
+    the coarse mesh (dt halved) judged on the coarse mesh like the others, the GPU seconds per
+    member-day of large ensembles (128 coarse members, 32 finer ones; the closure with FP32
+    state), and per day the plain cost at the closure's error (log-linear between the two plain
+    levels) against the closure's cost."""
+    level = int(round(np.log2((gc.nc - 2) / 10) / 2))
+    gm = _grid(level + 1)
+    inter = plain_level_errors(gf, gc, gm, seeds, days, coarse_dt / 2, daily, device=device)
+    costs = {"plain_coarse_fp64": member_day_cost(gc, 128, coarse_dt, 64, device=device),
+             "plain_finer_fp64": member_day_cost(gm, 32, coarse_dt / 2, 64, device=device),
+             "closure_coarse_fp32": member_day_cost(gc, 128, coarse_dt, 32, mlp, norm, device=device)}
+    table = []
+    closure = runs.get("closure_coarse", {}).get("h_l2", [])
+    for d in range(min(days, len(closure))):
+        e6, e7 = float(np.mean(runs["plain_coarse"]["h_l2"][d])), float(np.mean(inter["h_l2"][d]))
+        ec = float(np.mean(closure[d]))
+        plain_at = equal_error_cost({level: e6, level + 1: e7},
+                                    {level: costs["plain_coarse_fp64"], level + 1: costs["plain_finer_fp64"]}, ec)
+        table.append({"day": d + 1, "h_plain_coarse": e6, "h_plain_finer": e7, "h_closure": ec,
+                      "plain_gpu_s_per_member_day_at_closure_error": plain_at,
+                      "plain_over_closure": plain_at / costs["closure_coarse_fp32"]})
+    log(f"plain hexagon {level + 1}: h L2 per day {[round(float(np.mean(x)), 2) for x in inter['h_l2']]}; "
+        f"costs (GPU s per member-day) {costs}")
+    for row in table:
+        log(f"day {row['day']}: h plain {row['h_plain_coarse']:.2f} / {row['h_plain_finer']:.2f}, closure "
+            f"{row['h_closure']:.2f}; plain at the closure's error {row['plain_gpu_s_per_member_day_at_closure_error']:.4g}"
+            f" GPU s per member-day, {row['plain_over_closure']:.3g} x the closure's")
+    return {"plain_finer": inter, "finer_level": level + 1, "gpu_seconds_per_member_day": costs,
+            "equal_error": table}
 
 
 def main():
@@ -506,10 +591,11 @@ def main():
     p.add_argument("--momentum-scale", type=float, default=None,
                    help="with --evaluate: the scale the saved closure's momentum output had at training "
                         "(when the file does not record it); the closure is then re-calibrated")
-    p.add_argument("--calibrate-days", type=int, default=2)
+    p.add_argument("--calibrate-days", type=int, default=4)
     p.add_argument("--work-free", action="store_true",
                    help="with --evaluate: the momentum correction does no work on each member's flow")
-    p.add_argument("--scales", default="0,0.05,0.1,0.2,0.4,1", help="momentum scales the calibration tries")
+    p.add_argument("--scales", default="0,0.05,0.1,0.15,0.2,0.25,0.3", help="momentum scales the calibration tries")
+    p.add_argument("--input-noise", default="0", help="comma-separated: one network per training-input noise level")
     a = p.parse_args()
     scales = tuple(float(x) for x in a.scales.split(","))
     if a.evaluate:
@@ -537,7 +623,10 @@ def main():
                           work_free=a.work_free))
     else:
         s = pipeline(a.fine, a.coarse, a.train_seeds, a.train_days, a.snapshots, a.eval_seeds, a.eval_days,
-                     a.coarse_dt, a.window, a.fine_dt, a.epochs, out_params=a.params, target=a.target)
+                     a.coarse_dt, a.window, a.fine_dt, a.epochs, out_params=a.params, target=a.target,
+                     input_noise=tuple(float(x) for x in a.input_noise.split(",")),
+                     calibrate_days=a.calibrate_days, scales=scales)
+        s["command"] = "python -m dmplex_b200.closure_pipeline " + " ".join(__import__("sys").argv[1:])
     with open(a.out, "w") as f:
         json.dump(s, f, indent=1)
     print(json.dumps({k: v for k, v in s.items() if not isinstance(v, dict)}))

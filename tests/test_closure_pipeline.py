@@ -91,3 +91,28 @@ def test_run_coarse_reports_errors(require_gpu):
     res = cp.run_coarse(gc, daily[0], 2, 300.0, daily)
     assert len(res["h_l2"]) == 2 and all(np.isfinite(res["h_l2"][-1]))
     assert res["h_l2"][1][0] > 0
+
+
+def test_equal_error_cost_interpolates_log_linearly():
+    """The plain method's cost at a target error, log-linear in (error, cost) between two levels:
+    exact at the levels, and one level's factor per halving of the error between them."""
+    errors, costs = {6: 20.0, 7: 5.0}, {6: 1.0, 7: 8.0}
+    assert cp.equal_error_cost(errors, costs, 20.0) == pytest.approx(1.0)
+    assert cp.equal_error_cost(errors, costs, 5.0) == pytest.approx(8.0)
+    assert cp.equal_error_cost(errors, costs, 10.0) == pytest.approx(8.0 ** 0.5)
+    assert np.isnan(cp.equal_error_cost({6: 1.0, 7: 1.0}, costs, 1.0))
+
+
+@pytest.mark.gpu
+def test_plain_level_errors_and_costs(require_gpu):
+    """An intermediate level judged on the coarse mesh: its errors against the coarse-grained
+    fine run are finite and below the coarse level's, and the cost of a member-day is positive
+    and grows with the level."""
+    gf, gm, gc = cp._grid(5), cp._grid(4), cp._grid(3)
+    _, _, _, daily, _ = cp.fine_snapshots(gf, gc, [7, 8], 1, 0, dt_fine=60.0, spinup_days=0.0, record_days=True)
+    coarse = cp.run_coarse(gc, daily[0], 1, 300.0, daily)
+    inter = cp.plain_level_errors(gf, gc, gm, [7, 8], 1, 150.0, daily)
+    assert np.isfinite(inter["h_l2"]).all() and np.mean(inter["h_l2"][0]) < np.mean(coarse["h_l2"][0])
+    c3 = cp.member_day_cost(gc, 8, 300.0, steps=8)
+    c4 = cp.member_day_cost(gm, 8, 150.0, steps=8)
+    assert 0 < c3 < c4
