@@ -10,9 +10,7 @@ from dmplex_b200 import closure_pipeline as cp
 from dmplex_b200 import workloads as w
 from dmplex_b200.coarsen import divergence_matrix
 
-pytestmark = pytest.mark.gpu
-
-
+@pytest.mark.gpu
 @pytest.mark.parametrize("tendency_targets", [True, False])
 def test_closure_pipeline_small(require_gpu, tendency_targets):
     import torch
@@ -84,6 +82,7 @@ def test_closure_pipeline_small(require_gpu, tendency_targets):
     assert np.all(power > 0) and np.all(power_free <= 0.05 * power), (power_free, power)
 
 
+@pytest.mark.gpu
 def test_run_coarse_reports_errors(require_gpu):
     gf, gc = cp._grid(4), cp._grid(3)
     _, _, _, daily, secs = cp.fine_snapshots(gf, gc, [7, 8], 2, 0, dt_fine=60.0, spinup_days=0.0, record_days=True)
