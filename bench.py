@@ -58,7 +58,11 @@ def parse():
     p.add_argument("--no-hexagon5", action="store_true", help="skip the hexagon-5 CPU/GPU leg")
     p.add_argument("--ensemble-days", type=float, default=1.0, help="simulated days of the ensemble leg")
     p.add_argument("--no-icon", action="store_true", help="skip the ICON triangle-model leg")
+    p.add_argument("--icon-level", type=int, default=8, help="triangle level of the ICON leg (8: 1.31 M cells)")
+    p.add_argument("--icon-steps", type=int, default=100, help="timed RK4 steps of the ICON leg")
     p.add_argument("--no-mpas", action="store_true", help="skip the 3-D MPAS-Gassmann operators leg")
+    p.add_argument("--mpas-level", type=int, default=7, help="hexagon level of the MPAS leg")
+    p.add_argument("--mpas-calls", type=int, default=50, help="timed calls of the MPAS leg")
     p.add_argument("--no-galewsky", action="store_true", help="skip the Galewsky-jet leg (hexagon 8, 6 days)")
     p.add_argument("--level", type=int, default=LEVEL, help="mesh level (7 is the benchmark workload)")
     p.add_argument("--block", default=None,
@@ -837,10 +841,11 @@ def run_b200(args, rank, world, local_rank):
         closure = optional_leg(run_closure_leg, local_rank)
     icon_leg = None
     if not args.no_icon:
-        icon_leg = optional_leg(run_icon_leg, local_rank)
+        icon_leg = optional_leg(run_icon_leg, local_rank, level=args.icon_level, steps=args.icon_steps)
     mpas_leg = None
     if not args.no_mpas:
-        mpas_leg = optional_leg(run_mpas_leg, local_rank)
+        mpas_leg = optional_leg(run_mpas_leg, local_rank, level=args.mpas_level, calls=args.mpas_calls,
+                                cpu_calls=1 if args.no_cpu_baseline else 3)
     galewsky = None
     if world == 1 and not args.no_galewsky:   # an end-to-end run, not a per-GPU rate: at N = 1 only
         galewsky = optional_leg(run_galewsky_leg, local_rank)

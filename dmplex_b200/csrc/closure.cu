@@ -671,7 +671,6 @@ struct TriskClosure {
   int64_t launches = 0;
   int sms = 0;              // the device's SM count (persistent grids)
   int forward_per_sm = 1;   // resident inference CTAs per SM (the grid's multiple of the SMs)
-  int forward_occupancy = 0;  // what the occupancy query returned
   int64_t expire_tile = -1;  // test of the bounded wait: see trisk_closure_expire_wait_once
   ~TriskClosure() {
     int prev = -1;
@@ -774,11 +773,23 @@ int trisk_closure_create(int32_t device, const float* params, TriskClosure** out
   int sms = 0;
   CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
   c->sms = sms;
-  int per_sm = 0;
-  CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mlp_forward, TILE, FWD_SMEM_BYTES));
-  c->forward_occupancy = per_sm;
-  // every resident CTA must find its tensor-memory columns free (512 per SM)
-  c->forward_per_sm = std::max(1, std::min<int>(per_sm, 512 / (int)FWD_TMEM_COLS));
+  // Resident inference CTAs per SM from the kernel's resources: shared memory (dynamic,
+  // static and the per-CTA reservation), registers (allocated per warp in units of 256),
+  // threads, and tensor memory (512 columns). The runtime's occupancy query reports one CTA
+  // for this kernel, which leaves most of each SM idle, so it is not used.
+  cudaFuncAttributes fa{};
+  CUDA_CHECK(cudaFuncGetAttributes(&fa, k_mlp_forward));
+  int smem_sm = 0, reserved = 0, regs_sm = 0, threads_sm = 0;
+  CUDA_CHECK(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device));
+  CUDA_CHECK(cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, device));
+  CUDA_CHECK(cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, device));
+  CUDA_CHECK(cudaDeviceGetAttribute(&threads_sm, cudaDevAttrMaxThreadsPerMultiProcessor, device));
+  const int by_smem = smem_sm / (FWD_SMEM_BYTES + (int)fa.sharedSizeBytes + reserved);
+  const int warp_regs = ((fa.numRegs * 32 + 255) / 256) * 256;
+  const int by_regs = regs_sm / std::max(1, warp_regs * (TILE / 32));
+  const int by_threads = threads_sm / TILE;
+  const int per_sm = std::min(std::min(by_smem, by_regs), std::min(by_threads, 512 / (int)FWD_TMEM_COLS));
+  c->forward_per_sm = std::max(1, per_sm);
   CUDA_CHECK(cudaStreamSynchronize(c->stream));
   *out = c.release();
   TRISK_API_END
