@@ -164,3 +164,25 @@ def test_bounded_wait_gives_up_and_the_closure_stays_usable(require_gpu):
     assert torch.equal(before, after)
     Yo, _ = co.forward(mlp.params().astype(np.float64), X)
     assert _rel(after.cpu().numpy(), Yo) <= 1e-2
+
+
+@pytest.mark.gpu
+def test_forward_large_batch_rows_are_independent(require_gpu):
+    """4,194,304 rows (201 MB of features, more than the L2) through the persistent inference
+    grid: every row equals the same row computed in a small batch, bit for bit (each row is one
+    thread's, whatever tile and CTA it falls in), and a sample matches the oracle."""
+    import torch
+    import dmplex_b200.closure as cl
+    n = 4_194_304
+    g = torch.Generator(device="cuda")
+    g.manual_seed(11)
+    Xd = torch.randn((n, co.NIN), device="cuda", generator=g).to(torch.bfloat16).contiguous()
+    mlp = cl.ClosureMLP(co.init_params(2).astype(np.float32))
+    Y = mlp.forward(Xd)
+    for start in (0, 1_000_003, n - 777):
+        part = mlp.forward(Xd[start:start + 777].contiguous())
+        assert torch.equal(part, Y[start:start + 777])
+    idx = torch.arange(0, n, 4099, device="cuda")
+    Xs = Xd[idx].float().cpu().numpy().astype(np.float64)
+    Yo, _ = co.forward(mlp.params().astype(np.float64), Xs)
+    assert _rel(Y[idx].cpu().numpy(), Yo) <= 1e-2
