@@ -14,6 +14,7 @@
 
 #include <cuda_bf16.h>
 
+#include "closure_mlp.cuh"
 #include "model.hpp"
 
 using namespace trisk;
@@ -136,19 +137,15 @@ struct FeatureNorm {
   double out_scale[2];
 };
 
-// The network's 24 inputs of (edge, member) rows e * M + m of a slice, formed in FP64 as the stencil's
-// mean and differences so that their BF16 rounding keeps the local gradients: u_e; u at the
-// 10 TRiSK stencil edges minus u_e (0 for padded entries); the mean and the difference
-// (second cell minus first) of h at the two cells, of q at the two vertices and of K = B - g h
-// at the two cells; and 7 geometry values of the edge. Output row: row_map ? row_map[e] * Mg
-// + m0 + m (file edge numbering, the group's Mg members, the slice starting at member m0) :
-// the slice's internal row.
+// The network's 24 inputs of (edge, member) row r = e * M + m of a slice, formed in FP64 as the
+// stencil's mean and differences so that their BF16 rounding keeps the local gradients: u_e;
+// u at the 10 TRiSK stencil edges minus u_e (0 for padded entries); the mean and the
+// difference (second cell minus first) of h at the two cells, of q at the two vertices and of
+// K = B - g h at the two cells; and 7 geometry values of the edge; normalized (x - mean) scale
+// and rounded to BF16, as the row's 48 bytes.
 template <class R>
-__global__ void kg_features(DevTables T, DevWorkT<R> W, const R* y, int M, const float* geom,
-                            const FeatureNorm N, __nv_bfloat16* X, const int32_t* row_map, int64_t rows, int Mg,
-                            int m0) {
-  const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (r >= rows) return;
+__device__ __forceinline__ void feature_row(const DevTables& T, const DevWorkT<R>& W, const R* y, int M,
+                                            const float* geom, const FeatureNorm& N, int64_t r, uint4 (&q)[3]) {
   int e, m;  // rows < 2^31 (checked when the ensemble is made)
   split<true>((int)r, M, e, m);
   const R* u = y;
@@ -175,30 +172,84 @@ __global__ void kg_features(DevTables T, DevWorkT<R> W, const R* y, int M, const
   f[16] = K1 - K0;
 #pragma unroll
   for (int k = 0; k < NGEOM; ++k) f[17 + k] = geom[(size_t)e * NGEOM + k];
-  const int64_t out = row_map ? (int64_t)row_map[e] * Mg + m0 + m : r;
-  // the row's 48 bytes as three 16-byte stores (rows are 16-byte aligned)
   __align__(16) __nv_bfloat16 b[NFEAT];
 #pragma unroll
   for (int k = 0; k < NFEAT; ++k) b[k] = __float2bfloat16_rn((float)((f[k] - N.mean[k]) * N.scale[k]));
-  uint4* dst = reinterpret_cast<uint4*>(X + out * NFEAT);
   const uint4* src = reinterpret_cast<const uint4*>(b);
+  q[0] = src[0];
+  q[1] = src[1];
+  q[2] = src[2];
+}
+
+// The features of a slice's rows into X. Output row: row_map ? row_map[e] * Mg + m0 + m (file
+// edge numbering, the group's Mg members, the slice starting at member m0) : the slice's row.
+template <class R>
+__global__ void kg_features(DevTables T, DevWorkT<R> W, const R* y, int M, const float* geom,
+                            const FeatureNorm N, __nv_bfloat16* X, const int32_t* row_map, int64_t rows, int Mg,
+                            int m0) {
+  const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (r >= rows) return;
+  uint4 q[3];
+  feature_row<R>(T, W, y, M, geom, N, r, q);
+  int e, m;
+  split<true>((int)r, M, e, m);
+  const int64_t out = row_map ? (int64_t)row_map[e] * Mg + m0 + m : r;
+  uint4* dst = reinterpret_cast<uint4*>(X + out * NFEAT);  // rows are 16-byte aligned
 #pragma unroll
-  for (int c = 0; c < NFEAT / 8; ++c) dst[c] = src[c];
+  for (int c = 0; c < NFEAT / 8; ++c) dst[c] = q[c];
 }
 
 // dF = on[m] sF y0 (mass flux: added to F in the flux-form continuity equation only, so
 // mass stays conserved and the PV flux keeps the resolved F); dq = on[m] sQ y1 (momentum
 // tendency).
 template <class R>
+__device__ __forceinline__ void apply_row(R* dF, R* dq, int64_t r, int M, const float* member_on, double sF,
+                                          double sQ, float y0, float y1) {
+  int e, m;
+  split<true>((int)r, M, e, m);
+  const double on = member_on[m];
+  dF[r] = (R)(on * sF * (double)y0);
+  dq[r] = (R)(on * sQ * (double)y1);
+}
+
+template <class R>
 __global__ void kg_closure_apply(R* dF, R* dq, const float* Y, const float* member_on, int64_t rows, int M,
                                  double sF, double sQ) {
   const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (r >= rows) return;
-  int e, m;
-  split<true>((int)r, M, e, m);
-  const double on = member_on[m];
-  dF[r] = (R)(on * sF * (double)Y[2 * r]);
-  dq[r] = (R)(on * sQ * (double)Y[2 * r + 1]);
+  apply_row<R>(dF, dq, r, M, member_on, sF, sQ, Y[2 * r], Y[2 * r + 1]);
+}
+
+// The closure of a slice's rows in one kernel, bit for bit kg_features, the network's inference
+// and kg_closure_apply in turn: per tile of 128 (edge, member) rows every thread builds its
+// row's features straight into the tile's shared-memory operand, the tile runs through the
+// network on the tensor cores, and every thread writes its row's two corrections. Features
+// and network outputs never go to HBM (48 + 8 bytes per row each way in the three-launch form).
+// A persistent grid; the bounded tensor-core waits report through the network's status word.
+template <class R>
+__global__ void __launch_bounds__(closure::TILE) kg_closure_fused(
+    DevTables T, DevWorkT<R> W, const R* y, int M, const float* geom, const FeatureNorm N,
+    const closure::ParamsBF16* wbf, const closure::Params* p, const float* member_on, double sF, double sQ, R* dF,
+    R* dq, int64_t rows, closure::Status* status) {
+  using namespace closure;
+  extern __shared__ __align__(1024) unsigned char smem[];
+  __shared__ __align__(16) InferStatic st;
+  const int t = threadIdx.x;
+  const int64_t ntiles = (rows + TILE - 1) / TILE;
+  if ((int64_t)blockIdx.x >= ntiles) return;
+  const InferSmem S(smem);
+  const uint32_t tmem = infer_setup(S, st, wbf, p);
+  MmaWaits waits(smem_u32(S.mbar), &st.abort);
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int64_t r = tile * TILE + t;
+    uint4 q[3] = {make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0)};
+    if (r < rows) feature_row<R>(T, W, y, M, geom, N, r, q);
+    infer_put_row(S, q);
+    float y0, y1;
+    if (!infer_tile(S, st, tmem, waits, true, y0, y1)) break;
+    if (r < rows) apply_row<R>(dF, dq, r, M, member_on, sF, sQ, y0, y1);
+  }
+  infer_finish(waits, tmem, status);
 }
 
 // Work-free momentum correction. With the cell kinetic energy K_i = sum_k kinetic[i,k] u_k^2,
@@ -347,6 +398,8 @@ struct ClosureSlot {
   trisk::FeatureNorm norm{};
   bool every_stage = false;    // false: the network runs at stage 1 and its output is reused
   bool work_free = false;      // project the momentum correction to do no work (per member)
+  bool fused = true;           // features, network and corrections in one kernel (else three)
+  int fused_per_sm = 1;        // resident CTAs per SM of the fused kernel
   double* sums = nullptr;      // 2 M: <g, dq>, <g, g> per member
   double* partials = nullptr;  // 2 M x WORK_SUM_BLOCKS per-block partial sums of them
 };
@@ -634,13 +687,27 @@ void enqueue_closure(TriskEnsemble& e, const std::vector<int>& set_slices, int s
       R* dF = reinterpret_cast<R*>(e.at(c.dF, r0));
       R* dq = reinterpret_cast<R*>(e.at(c.dq, r0));
       const R* ys = reinterpret_cast<const R*>(stage == 1 ? D.y : D.st);
-      kg_features<R><<<nb, 256, 0, e.stream>>>(D.T, work_as<R>(D.W), ys, D.M, c.geom, c.norm, X, nullptr, rows, G.M,
-                                               sl.m0);
-      CUDA_CHECK(cudaGetLastError());
-      closure_forward_on(c.net, X, rows, Y, e.stream);
-      kg_closure_apply<R><<<nb, 256, 0, e.stream>>>(dF, dq, Y, c.member_on + sl.m0, rows, D.M, c.norm.out_scale[0],
-                                                    c.norm.out_scale[1]);
-      CUDA_CHECK(cudaGetLastError());
+      if (c.fused) {
+        const closure::ParamsBF16* wbf;
+        const closure::Params* p;
+        closure::Status* status;
+        closure::closure_device_params(c.net, &wbf, &p, &status);
+        const int64_t tiles = cdiv(rows, closure::TILE);
+        const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)e.sms * c.fused_per_sm));
+        kg_closure_fused<R><<<grid, closure::TILE, closure::FWD_SMEM_BYTES, e.stream>>>(
+            D.T, work_as<R>(D.W), ys, D.M, c.geom, c.norm, wbf, p, c.member_on + sl.m0, c.norm.out_scale[0],
+            c.norm.out_scale[1], dF, dq, rows, status);
+        CUDA_CHECK(cudaGetLastError());
+        e.launches -= 2;  // one launch instead of three
+      } else {
+        kg_features<R><<<nb, 256, 0, e.stream>>>(D.T, work_as<R>(D.W), ys, D.M, c.geom, c.norm, X, nullptr, rows,
+                                                 G.M, sl.m0);
+        CUDA_CHECK(cudaGetLastError());
+        closure_forward_on(c.net, X, rows, Y, e.stream);
+        kg_closure_apply<R><<<nb, 256, 0, e.stream>>>(dF, dq, Y, c.member_on + sl.m0, rows, D.M,
+                                                      c.norm.out_scale[0], c.norm.out_scale[1]);
+        CUDA_CHECK(cudaGetLastError());
+      }
       if (c.work_free) {
         double* sums = c.sums + 2 * sl.m0;
         double* partials = c.partials + 2 * (int64_t)sl.m0 * WORK_SUM_BLOCKS;
@@ -1172,6 +1239,12 @@ int trisk_ensemble_set_closure(TriskEnsemble* ens, int32_t group, TriskClosure* 
   c.norm.out_scale[1] = norm[2 * NFEAT + 1];
   c.every_stage = (flags & 1) != 0;
   c.work_free = (flags & 2) != 0;
+  c.fused = (flags & 4) == 0;
+  if (c.fused)
+    with_real(e, [&](auto r) {
+      using R = decltype(r);
+      c.fused_per_sm = closure::infer_ctas_per_sm(reinterpret_cast<const void*>(kg_closure_fused<R>), e.device);
+    });
   if (c.work_free && !c.sums) {
     c.sums = e.alloc<double>(2 * (size_t)G.M);
     c.partials = e.alloc<double>(2 * (size_t)G.M * WORK_SUM_BLOCKS);

@@ -118,10 +118,12 @@ class Ensemble:
         return out
 
     def set_closure(self, group: int, net, geometry: np.ndarray, norm: np.ndarray, every_stage: bool = False,
-                    work_free: bool = False):
+                    work_free: bool = False, fused: bool = True):
         """Learned closure for a group (net: closure.ClosureMLP, or None to remove it).
         every_stage: run the network at every RK4 stage; work_free: remove from each member's
-        momentum correction its component along the energy gradient (no work on the flow)."""
+        momentum correction its component along the energy gradient (no work on the flow);
+        fused: features, network and corrections in one kernel (False: three launches with the
+        features and outputs in HBM; the same numbers)."""
         if net is None:
             check(lib.trisk_ensemble_set_closure(self._h, group, None, None, None, 0))
             self._net = None
@@ -129,7 +131,8 @@ class Ensemble:
         geometry = np.ascontiguousarray(geometry, dtype=np.float32)
         norm = np.ascontiguousarray(norm, dtype=np.float64)
         check(lib.trisk_ensemble_set_closure(self._h, group, net.handle, geometry.ctypes.data, norm.ctypes.data,
-                                             int(bool(every_stage)) | (2 if work_free else 0)))
+                                             int(bool(every_stage)) | (2 if work_free else 0) |
+                                             (0 if fused else 4)))
         self._net = net  # the ensemble launches it
 
     def closure_mask(self, group: int, member_on) -> None:

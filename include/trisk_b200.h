@@ -471,7 +471,9 @@ int trisk_ensemble_energy(TriskEnsemble* ensemble, int32_t group, double* energi
  * makes the momentum correction work-free per member: its component along the energy
  * gradient dE/du_e = u_e l_e (h_c0 d_c0 + h_c1 d_c1) (cell kinetic energy; l, d and the two
  * cell distances are geometry columns 0..3) is removed, so it does no work on the flow to
- * first order.
+ * first order; bit 2 (4) runs the features, the network and the corrections as three launches
+ * with the features and outputs in device memory, instead of one kernel that builds each tile's
+ * features in shared memory and applies its outputs there (the same numbers bit for bit).
  * net = NULL removes the group's closure. */
 int trisk_ensemble_set_closure(TriskEnsemble* ensemble, int32_t group, TriskClosure* net, const float* geometry,
                                const double* norm, int32_t flags);

@@ -278,3 +278,33 @@ def test_closure_energy_monitor_is_deterministic(require_gpu, work_free):
     assert 0 < m1[-1].sum() < M
     for a, b in zip(y1, y2):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("state_bits", [64, 32])
+def test_fused_closure_kernel_equals_three_launches(require_gpu, state_bits):
+    """The fused closure kernel (features built in shared memory, the network on the tensor
+    cores, the corrections written from registers) against features, network and corrections
+    as three launches through device memory: every member bit for bit after several steps, at
+    one network call per step and at every stage."""
+    from dmplex_b200.closure import ClosureMLP
+    from dmplex_b200.coarsen import edge_geometry
+    si = w.si_parameters()
+    g = trisk_grid(4, True)
+    m = d.TRiSKShallowWater(g, pv_flux="trisk", kinetic_energy="cell", **si)
+    M = 6
+    states = member_states(g, M, 41)
+    net = ClosureMLP(seed=8)
+    u = np.abs(states[0][:g.ne]).mean()
+    norm = np.concatenate([np.zeros(24), np.ones(24), [1e-3 * u, 1e-3 * u / 3600]])
+    for every_stage in (False, True):
+        out = []
+        for fused in (True, False):
+            ens = d.Ensemble([(m, M, 150.0, 5)], state_bits=state_bits)
+            for k, y in enumerate(states):
+                ens.set_member(0, k, y)
+            ens.set_closure(0, net, edge_geometry(g), norm, every_stage=every_stage, fused=fused)
+            ens.run(5)
+            ens.closure_check()
+            out.append([ens.get_member(0, k) for k in range(M)])
+        for a, b in zip(*out):
+            assert np.array_equal(a, b)
