@@ -214,6 +214,8 @@ def _load():
         "trisk_model_set_l2_residency": (C.c_int, [_p, _i64, _i32]),
         "trisk_model_get_l2_residency": (C.c_int, [_p, C.POINTER(_i64), C.POINTER(_i32)]),
         "trisk_l2_info": (C.c_int, [_i32, _p]),
+        "trisk_model_set_persistent": (C.c_int, [_p, _i32]),
+        "trisk_model_get_persistent": (C.c_int, [_p, C.POINTER(_i32)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -699,4 +699,86 @@ __global__ void __launch_bounds__(256) k_tend(DevTables T, DevWork W, DevStage S
   tend_body<PV, EPI, ENS, false, double, KEEP>(T, W, S, M, nbE, blockIdx.x);
 }
 
+// ------------------------------------------------------------------------------------
+// RK4 steps in one cooperative launch, for meshes whose tables and vectors stay in L2: the
+// twelve phases of a step follow one another inside the kernel, separated by a grid-wide
+// barrier, instead of as twelve launches (whose start-up latency dominates when each phase
+// moves a few MB). Every block loops over the phases' blocks of work (the bodies above), so
+// results are those of the launches bit for bit.
+
+// The grid barrier: arrivals counted in *count, released by incrementing *gen. A block's wait
+// gives up after a second, sets *err and leaves; a block that sees *err after a barrier
+// returns, so every wait ends.
+struct GridBarrier {
+  unsigned* count;
+  unsigned* gen;
+  int* err;
+};
+
+__device__ __forceinline__ long long barrier_ns() {
+  long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ bool grid_sync(const GridBarrier& B) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned* gen = B.gen;
+    const unsigned g = *gen;
+    __threadfence();
+    if (atomicAdd(B.count, 1u) == gridDim.x - 1) {
+      atomicExch(B.count, 0u);
+      __threadfence();
+      atomicAdd(B.gen, 1u);
+    } else {
+      const long long start = barrier_ns();
+      for (unsigned i = 1; *gen == g; ++i)
+        if ((i & 1023u) == 0 && barrier_ns() - start > 1000000000LL) {
+          atomicExch(B.err, 1);
+          break;
+        }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return *reinterpret_cast<volatile int*>(B.err) == 0;
+}
+
+template <int PV, int EPI>
+__device__ __forceinline__ void tend_phase(const DevTables& T, const DevWork& W, const DevStage& S, int nbE, int nbT) {
+  for (int vb = blockIdx.x; vb < nbT; vb += gridDim.x) tend_body<PV, EPI, false, false, double, false>(T, W, S, 1, nbE, vb);
+}
+
+template <int PV, int KE>
+__global__ void __launch_bounds__(256) k_rk4_persistent(DevTables T, DevWork W, DevStage S, double dt, int nsteps,
+                                                        GridBarrier B) {
+  const int nbV = (T.nv + (int)blockDim.x - 1) / (int)blockDim.x;
+  const int nbE = (T.ne + (int)blockDim.x - 1) / (int)blockDim.x;
+  const int nbC = (T.nc + (int)blockDim.x - 1) / (int)blockDim.x;
+  for (int step = 0; step < nsteps; ++step) {
+#pragma unroll 1
+    for (int stage = 1; stage <= 4; ++stage) {
+      const double* u = stage == 1 ? S.y : S.st;
+      for (int vb = blockIdx.x; vb < nbV; vb += gridDim.x)
+        vertex_body<PV, KE, false, double, false, 1>(T, W, u, u + T.ne, 1, 0, vb);
+      if (!grid_sync(B)) return;
+      for (int vb = blockIdx.x; vb < nbE + nbC; vb += gridDim.x)
+        flux_body<PV, KE, false, double, false, 1>(T, W, u, u + T.ne, 1, nbE, 0, vb);
+      if (!grid_sync(B)) return;
+      DevStage St = S;
+      St.u = u;
+      St.h = u + T.ne;
+      St.c = stage == 3 ? dt : dt / 2;
+      switch (stage) {
+        case 1: tend_phase<PV, EPI_STAGE1>(T, W, St, nbE, nbE + nbC); break;
+        case 2: tend_phase<PV, EPI_STAGE2>(T, W, St, nbE, nbE + nbC); break;
+        case 3: tend_phase<PV, EPI_STAGE3>(T, W, St, nbE, nbE + nbC); break;
+        default: tend_phase<PV, EPI_STAGE4>(T, W, St, nbE, nbE + nbC); break;
+      }
+      if (!grid_sync(B)) return;
+    }
+  }
+}
+
 }  // namespace trisk

@@ -250,8 +250,35 @@ void ensure_graph(TriskModel& m, double dt) {
   m.graph_dt = dt;
 }
 
+constexpr int PERSISTENT_BLOCK = 256;
+
+// All nsteps RK4 steps as one cooperative launch of k_rk4_persistent.
+void run_persistent(TriskModel& m, double dt, int64_t nsteps) {
+  DevStage S{};
+  S.y = m.y;
+  S.acc = m.acc;
+  S.st = m.st;
+  S.flag = m.flag;
+  S.sixth = dt / 6;
+  GridBarrier B{m.barrier, m.barrier + 1, m.barrier_err};
+  for (int64_t done = 0; done < nsteps;) {
+    const int n = (int)std::min<int64_t>(nsteps - done, 1 << 20);
+    with_modes(m.pv, m.ke, [&](auto pvc, auto kec) {
+      constexpr int PV = decltype(pvc)::value, KE = decltype(kec)::value;
+      void* args[] = {&m.T, &m.W, &S, &dt, const_cast<int*>(&n), &B};
+      CUDA_CHECK(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(k_rk4_persistent<PV, KE>),
+                                             dim3((unsigned)m.persistent_grid), dim3(PERSISTENT_BLOCK), args, 0,
+                                             m.stream));
+    });
+    m.launches++;
+    done += n;
+  }
+}
+
 void run_steps(TriskModel& m, double dt, int64_t nsteps) {
-  if (m.use_graph) {
+  if (m.persistent) {
+    run_persistent(m, dt, nsteps);
+  } else if (m.use_graph) {
     ensure_graph(m, dt);
     for (int64_t s = 0; s < nsteps; ++s) {
       CUDA_CHECK(cudaGraphLaunch(m.graph, m.stream));
@@ -306,9 +333,16 @@ void state_out(TriskModel& m, double* y_user, const double* src) {
 }
 
 void check_flag(TriskModel& m) {
-  int flag = 0;
+  int flag = 0, err = 0;
   CUDA_CHECK(cudaMemcpyAsync(&flag, m.flag, sizeof(int), cudaMemcpyDeviceToHost, m.stream));
+  if (m.barrier_err) CUDA_CHECK(cudaMemcpyAsync(&err, m.barrier_err, sizeof(int), cudaMemcpyDeviceToHost, m.stream));
   CUDA_CHECK(cudaStreamSynchronize(m.stream));
+  if (err) {
+    CUDA_CHECK(cudaMemsetAsync(m.barrier, 0, 2 * sizeof(unsigned), m.stream));
+    CUDA_CHECK(cudaMemsetAsync(m.barrier_err, 0, sizeof(int), m.stream));
+    CUDA_CHECK(cudaStreamSynchronize(m.stream));
+    throw Error(TRISK_ERR_TIMEOUT, "a grid-barrier wait of the one-launch RK4 step gave up");
+  }
   if (flag) {
     CUDA_CHECK(cudaMemsetAsync(m.flag, 0, sizeof(int), m.stream));
     throw Error(TRISK_ERR_NONFINITE, "the state became non-finite");
@@ -733,6 +767,33 @@ void finish_create(TriskModel& m, const Coefficients& C, const std::vector<V3>* 
   CUDA_CHECK(cudaDeviceSynchronize());
 }
 
+// Switches the one-launch RK4 step on or off: the barrier words, and the grid of as many
+// blocks as are co-resident (the cooperative launch refuses more).
+void set_persistent(TriskModel& m, bool on) {
+  if (!on) {
+    m.persistent = false;
+    return;
+  }
+  int coop = 0, sms = 0, occ = 0;
+  CUDA_CHECK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, m.device));
+  if (!coop) throw Error(TRISK_ERR_UNSUPPORTED, "the device has no cooperative launch");
+  CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m.device));
+  with_modes(m.pv, m.ke, [&](auto pvc, auto kec) {
+    constexpr int PV = decltype(pvc)::value, KE = decltype(kec)::value;
+    CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_rk4_persistent<PV, KE>, PERSISTENT_BLOCK, 0));
+  });
+  if (occ < 1) throw Error(TRISK_ERR_UNSUPPORTED, "the one-launch step does not fit an SM");
+  const int64_t work = cdiv(m.ne + m.nc, PERSISTENT_BLOCK);  // the widest phase
+  m.persistent_grid = (int)std::min<int64_t>((int64_t)sms * occ, work);
+  if (!m.barrier) {
+    m.barrier = m.alloc<unsigned>(2);
+    m.barrier_err = m.alloc<int>(1);
+  }
+  CUDA_CHECK(cudaMemset(m.barrier, 0, 2 * sizeof(unsigned)));
+  CUDA_CHECK(cudaMemset(m.barrier_err, 0, sizeof(int)));
+  m.persistent = true;
+}
+
 TriskModel* checked(TriskModel* m) {
   if (!m) throw Error(TRISK_ERR_ARGUMENT, "model is NULL");
   return m;
@@ -1039,9 +1100,11 @@ int trisk_autotune(TriskModel* model, double* y, double dt, int32_t steps, doubl
   if (!is_device_pointer(y)) throw Error(TRISK_ERR_ARGUMENT, "trisk_autotune needs a device state");
   // Times `steps` RK4 steps (graph + PDL as configured) for every combination of the three
   // phase block sizes, then for L2-resident table prefixes of several sizes with the best
-  // blocks, then the blocks again with the best prefix, and keeps the fastest. Every
-  // candidate computes the same numbers; the state is restored from the caller's copy
-  // before each trial. A persisting window, if one was set, is left off.
+  // blocks, then the blocks again with the best prefix, and for meshes that fit half the L2
+  // the one-launch step, and keeps the fastest. Every candidate computes the same numbers;
+  // the state is restored from the caller's copy before each trial. A persisting window, if
+  // one was set, is left off.
+  m.persistent = false;
   static const int choices[] = {64, 128, 256};
   static const int keep_mb[] = {0, 8, 16, 24, 32, 40, 48, 64};
   cudaEvent_t e0, e1;
@@ -1096,10 +1159,27 @@ int trisk_autotune(TriskModel* model, double* y, double dt, int32_t steps, doubl
   } catch (...) {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    m.persistent = false;
     throw;
+  }
+  // the one-launch step, for meshes whose tables and state vectors fit half the L2
+  bool use_persistent = false;
+  const double footprint = (double)m.table_block_bytes + 8.0 * sizeof(double) * (m.N + m.nv);
+  if (footprint <= l2 / 2) {
+    try {
+      const bool was = m.persistent;
+      set_persistent(m, true);
+      const double before = best_t;
+      trial(best[0], best[1], best[2], best_keep);  // the blocks do not apply to it; best_t moves if faster
+      use_persistent = best_t < before;
+      m.persistent = was;
+    } catch (const Error&) {
+      m.persistent = false;  // no cooperative launch: keep the launches
+    }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  m.persistent = use_persistent;
   for (int p = 0; p < 3; ++p) m.block[p] = best[p];
   m.l2_keep_bytes = best_keep;
   m.l2_window = false;
@@ -1473,5 +1553,22 @@ int trisk_dist_stream(TriskDist* dist, void** stream) {
 }
 
 int64_t trisk_dist_launch_count(TriskDist* dist) { return dist && dist->m ? dist->m->launches : -1; }
+
+int trisk_model_set_persistent(TriskModel* model, int32_t on) {
+  TRISK_API_BEGIN
+  TriskModel& m = *checked(model);
+  DeviceGuard guard(m.device);
+  CUDA_CHECK(cudaStreamSynchronize(m.stream));
+  set_persistent(m, on != 0);
+  TRISK_API_END
+}
+
+int trisk_model_get_persistent(TriskModel* model, int32_t* on) {
+  TRISK_API_BEGIN
+  TriskModel& m = *checked(model);
+  if (!on) throw Error(TRISK_ERR_ARGUMENT, "NULL argument");
+  *on = m.persistent ? 1 : 0;
+  TRISK_API_END
+}
 
 }  // extern "C"

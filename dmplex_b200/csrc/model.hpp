@@ -76,6 +76,11 @@ struct TriskModel {
   int64_t nc_own = -1, ne_own = -1;  // owned cells and edges come first (-1: all are owned)
   int block[3] = {128, 128, 128};  // threads per block of k_vertex, k_flux, k_tend
   bool use_graph = true, use_pdl = true, identity = true;
+  // RK4 steps in one cooperative launch (k_rk4_persistent): for meshes that stay in L2
+  bool persistent = false;
+  int persistent_grid = 0;               // co-resident blocks of 256 threads
+  unsigned* barrier = nullptr;           // arrivals, generation
+  int* barrier_err = nullptr;            // a grid-barrier wait gave up
   trisk::Coefficients C;  // file numbering, 0-based (kept for export)
   CoefficientExport exported;
   std::vector<int32_t> cell_n2o, edge_n2o, vert_n2o, cell_o2n, edge_o2n, vert_o2n;

@@ -149,6 +149,18 @@ class TRiSKShallowWater:
             raise ValueError("three block sizes")
         check(lib.trisk_model_set_block(self._h, b.ctypes.data))
 
+    @property
+    def persistent(self) -> bool:
+        """Whether the RK4 steps run as one cooperative launch (the autotuner may choose it)."""
+        on = C.c_int32()
+        check(lib.trisk_model_get_persistent(self._h, C.byref(on)))
+        return bool(on.value)
+
+    def set_persistent(self, on: bool) -> None:
+        """RK4 steps as one cooperative launch with grid barriers between the phases (meshes
+        that stay in L2), or as the CUDA graph of twelve launches per step."""
+        check(lib.trisk_model_set_persistent(self._h, int(bool(on))))
+
     def set_l2_residency(self, nbytes: int, window: bool = False) -> None:
         """Keeps the first nbytes of the packed tables in L2 (evict-last loads; with window
         also a persisting access-policy window). 0 streams every table."""

@@ -226,12 +226,21 @@ int trisk_model_info(TriskModel* model, int32_t* pv_mode, int32_t block[3], doub
 /* Autotuner (no reference counterpart): times `steps` RK4 steps of the device state y (left
  * unchanged) for every combination of the phase block sizes {64, 128, 256}, then L2-resident
  * table prefixes of 8..64 MB (trisk_model_set_l2_residency, no window) with the best blocks,
- * then the blocks again with the best prefix, and keeps the fastest in the model; best_ms
- * gets its time per step. */
+ * then the blocks again with the best prefix, then (for meshes whose tables and vectors fit
+ * half the L2) the one-launch step of trisk_model_set_persistent, and keeps the fastest in
+ * the model; best_ms gets its time per step. */
 int trisk_autotune(TriskModel* model, double* y_device, double dt, int32_t steps, double* best_ms);
 /* Sets the threads per block of the three phases (vertex, flux, tend), each a multiple of 32
  * in [64, 256], as an autotuner result found earlier (no reference counterpart). */
 int trisk_model_set_block(TriskModel* model, const int32_t block[3]);
+/* The one-launch RK4 step (no reference counterpart): on != 0 runs the RK4 steps of
+ * trisk_rk4_step(_async) as one cooperative launch whose blocks do the twelve phases of every
+ * step in turn, separated by a grid-wide barrier, instead of twelve launches per step (the
+ * same numbers bit for bit); for meshes that stay in L2, where launch latency dominates. A
+ * barrier wait that gives up (after a second) ends the launch; the next synchronizing call
+ * returns TRISK_ERR_TIMEOUT. TRISK_ERR_UNSUPPORTED without cooperative launch. */
+int trisk_model_set_persistent(TriskModel* model, int32_t on);
+int trisk_model_get_persistent(TriskModel* model, int32_t* on);
 /* L2 residency of the tables (no reference counterpart). The first `bytes` of the model's
  * packed table block (the tendency phase's tables first, then the flux phase's, then the
  * vertex phase's) are loaded with an L2 evict-last policy, so they stay in L2 from one

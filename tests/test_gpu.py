@@ -76,6 +76,47 @@ def test_multi_step_call_matches_single_steps(require_gpu):
     assert np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("pv,ke", [("trisk", "cell"), ("gassmann", "vertex"), ("gassmann_mean", "mixed")])
+def test_one_launch_rk4_step_bitwise(require_gpu, pv, ke):
+    """The one-launch RK4 step (one cooperative launch for all steps of a call, grid barriers
+    between the twelve phases of a step) against the oracle and against the twelve-launch
+    graph step: bit for bit, and one launch per call besides the state's renumbering."""
+    from oracle.oracle import Oracle
+    si = w.si_parameters()
+    g = trisk_grid(5, True)
+    o = Oracle(tables(5, pv, ke, True, None, **si), threads=8)
+    graph = d.TRiSKShallowWater(g, pv_flux=pv, kinetic_energy=ke, **si)
+    one = d.TRiSKShallowWater(g, pv_flux=pv, kinetic_energy=ke, **si)
+    one.set_persistent(True)
+    assert one.persistent and not graph.persistent
+    y = w.synthetic_state(g, seed=4)
+    a, b, ref = y.copy(), y.copy(), y.copy()
+    before = one.launch_count()
+    d.rk4_step(a, 300.0, d.tendency, d.RK4Cache(a), one, nsteps=7)
+    assert one.launch_count() - before == 1 + 2
+    d.rk4_step(b, 300.0, d.tendency, d.RK4Cache(b), graph, nsteps=7)
+    o.rk4_step(ref, 300.0, 7)
+    assert np.array_equal(a, b) and np.array_equal(a, ref)
+    one.set_persistent(False)  # back to the graph: still the same numbers
+    d.rk4_step(a, 300.0, d.tendency, d.RK4Cache(a), one, nsteps=2)
+    d.rk4_step(b, 300.0, d.tendency, d.RK4Cache(b), graph, nsteps=2)
+    assert np.array_equal(a, b)
+
+
+def test_one_launch_step_reports_nonfinite(require_gpu):
+    g = trisk_grid(3)
+    m = d.TRiSKShallowWater(g)
+    m.set_persistent(True)
+    y = tc2_state(g)
+    y[5] = np.nan
+    with pytest.raises(d.TriskError) as e:
+        d.rk4_step(y, 0.01, d.tendency, d.RK4Cache(y), m, nsteps=3)
+    assert e.value.status == 4
+    y = tc2_state(g)
+    d.rk4_step(y, 0.01, d.tendency, d.RK4Cache(y), m)
+    assert np.isfinite(y).all()
+
+
 @pytest.mark.parametrize("use_graph,use_pdl,block", [(False, False, 256), (True, False, 128), (False, True, 64)])
 def test_launch_modes_bitwise(require_gpu, use_graph, use_pdl, block):
     g = trisk_grid(4, True)
