@@ -406,10 +406,10 @@ struct ClosureSlot {
 
 // blocks of kg_work_sums along the edges (the row length of its partial sums)
 constexpr int WORK_SUM_BLOCKS = 1024;
-// A slice's gathered stage state and work vectors should stay in L2 beside the streaming
-// tables. The L2 is 126 MB, but each of the two dies' halves caches what its own SMs read, so
-// data every SM reads sees about half of it (the single-model path thrashes beyond a working
-// set of ~60 MB): the budget of the default slicing and of a launch set.
+// A launch set takes slices while their gathered stage state and work vectors stay within
+// this L2 budget. The L2 is 126 MB, but each of the two dies' halves caches what its own SMs
+// read, so data every SM reads sees about half of it (the single-model path thrashes beyond
+// a working set of ~60 MB).
 constexpr double SLICE_L2_BUDGET = 48.0 * (1 << 20);
 
 // A user group: its members' buffers (every slice's, one after the other) and its slicing.
@@ -520,25 +520,6 @@ void with_real(const TriskEnsemble& e, F&& f) {
     f(float{});
   else
     f(double{});
-}
-
-// The default members per slice of a group: the candidate M, M/2, M/4, ... that minimizes a
-// byte estimate per stage, (slices) T + M f max(0, 1 - B / (S f)): every slice streams the
-// tables T once, and the part of a slice's state and work vectors (f per member) beyond the
-// L2 budget B goes to DRAM and back.
-int default_slice(int M, double T, double f) {
-  int best = M;
-  double best_cost = INFINITY;
-  for (int S = M; S >= 1; S = S > 1 ? (S + 1) / 2 : 0) {
-    const double slices = std::ceil((double)M / S);
-    const double cost = slices * T + (double)M * f * std::max(0.0, 1.0 - SLICE_L2_BUDGET / (S * f));
-    if (cost < best_cost * 0.999) {
-      best_cost = cost;
-      best = S;
-    }
-    if (S == 1) break;
-  }
-  return best;
 }
 
 // The slices of every group for its current S: descriptors pointing into the group's buffers.
@@ -909,7 +890,7 @@ int trisk_ensemble_create_precision(TriskModel* const* models, const int32_t* me
     G.st = e->alloc_state(m->N * M);
     CUDA_CHECK(cudaMemset(G.y, 0, m->N * M * e->esize()));
     G.member_bytes = (double)e->esize() * (1.0 * m->N + 2.0 * m->nc + 2.0 * m->ne + 4.0 * m->nv);
-    G.S = default_slice(G.M, m->table_bytes_unique, G.member_bytes);
+    G.S = G.M;  // whole groups: measured faster than any slicing (the autotuner tries others)
     e->groups.push_back(G);
     e->models.push_back(m);
     e->max_state = std::max(e->max_state, m->N);

@@ -448,9 +448,10 @@ int64_t trisk_ensemble_launch_count(TriskEnsemble* ensemble);
 int trisk_ensemble_set_block(TriskEnsemble* ensemble, const int32_t block[3]);
 int trisk_ensemble_get_block(TriskEnsemble* ensemble, int32_t block[3]);
 /* Members per slice of every group (ngroups values; the last slice of a group may have
- * fewer). The default minimizes a byte estimate: tables streamed once per slice against the
- * part of a slice's gathered state and work vectors beyond a 48 MB L2 budget. Setting them keeps the
- * members' states; results are the same bit for bit for every slicing. */
+ * fewer). The default is the whole group: on a B200 every slicing of the configuration-3
+ * groups measured slower (tables streamed once per slice cost more than the L2 residency of
+ * a slice's work vectors saves). Setting them keeps the members' states; results are the same
+ * bit for bit for every slicing. */
 int trisk_ensemble_set_slices(TriskEnsemble* ensemble, const int32_t* members_per_slice);
 int trisk_ensemble_get_slices(TriskEnsemble* ensemble, int32_t* members_per_slice);
 /* Autotuner of the batched path (no reference counterpart): times `steps` RK4 steps of all
