@@ -189,3 +189,52 @@ def test_icon_galewsky_on_bisection_triangles():
         with np.errstate(all="ignore"):
             o.rk4_step(y, dt, n)
         assert bool(np.isfinite(y).all() and np.abs(y[:g.ne]).max() < 1.0) == survives, gradient
+
+
+# the same published ICON figures through the library's CUDA path: seconds on a B200, so they
+# are default GPU tests (the CPU forms above take minutes and need TRISK_LONG_TESTS)
+def _icon_tc2_l2_gpu(g):
+    from dmplex_b200 import icon
+    m = icon.ICONShallowWater(g)
+    u0 = 0.2
+    x = g.edge_points
+    u = u0 * np.einsum("ij,ij->i", np.stack([-x[:, 1], x[:, 0], np.zeros(len(x))], axis=1), g.edge_normals)
+    y = np.concatenate([u, 1 - (u0 + u0 ** 2 / 2) * g.centers[:, 2] ** 2])
+    y0 = y.copy()
+    dt = min(0.2 * np.sqrt(4 * np.pi / g.nc), 0.4 * float(g.dual_lengths.min()))
+    m.rk4_step(y, dt, int(np.ceil(1 / dt)))
+    dh = (y - y0)[g.ne:]
+    return np.sqrt(np.sum(g.cell_areas * dh ** 2) / (4 * np.pi))
+
+
+@pytest.mark.gpu
+def test_icon_level6_and_7_figures_on_the_gpu(require_gpu):
+    """TC2 L2 3.9e-6 (plain) and 1.4e-6 (spring) on triangle 6 through the ICON kernels; spring
+    asymmetry 0.10 / 0.089 on levels 6 / 7 (docs/STATUS.md:40-55)."""
+    assert close(_icon_tc2_l2_gpu(_triangles("plain", 6)), "3.9e-6")
+    g6 = _triangles("spring", 6)
+    assert close(_icon_tc2_l2_gpu(g6), "1.4e-6")
+    assert close(_asymmetry(g6), "0.10") and close(_asymmetry(_triangles("spring", 7)), "0.089")
+
+
+@pytest.mark.gpu
+def test_icon_galewsky_on_bisection_triangles_on_the_gpu(require_gpu):
+    """The published failure mode through the ICON kernels: the Galewsky jet on plain triangle 5
+    blows up before day 3 with ICON's kinetic-energy gradient (the library reports the
+    non-finite state) and stays stable with the centered one (:44-50)."""
+    from dmplex_b200 import icon, run
+    from dmplex_b200.cases import Galewsky
+    case = Galewsky(3.0)
+    g = _triangles("plain", 5)
+    dt, n = case.steps(g)
+    for gradient, survives in (("icon", False), ("centered", True)):
+        m = icon.ICONShallowWater(g, gravity=case.gravity, kinetic_gradient=gradient,
+                                  divergence_damping=case.icon_damping(g, dt))
+        y = run.edge_and_cell_state(g, case)
+        try:
+            m.rk4_step(y, dt, n)
+            stable = bool(np.isfinite(y).all() and np.abs(y[:g.ne]).max() < 1.0)
+        except d.TriskError as err:
+            assert err.status == 4
+            stable = False
+        assert stable == survives, gradient
