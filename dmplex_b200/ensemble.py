@@ -9,7 +9,7 @@ import ctypes as C
 
 import numpy as np
 
-from ._lib import check, lib, ptr
+from ._lib import check, lib
 from .model import TRiSKShallowWater, _state
 
 
