@@ -64,13 +64,6 @@ struct MpasTables {
   const double* coriolis;  // ldv
   const int32_t* ti;       // 3 x nt x lde
   const double* trisk;     // nt x lde
-  // The vn kernel's staging (blocks of MB edges): the distinct edges a block's TRiSK entries
-  // name, ascending (ub_edges[ub_offset[b] ..]), and each entry's slot among them (tl, 3 x nt x
-  // lde, as ti); ub_stride >= the largest count (0: no staging).
-  const int32_t* ub_edges;
-  const int32_t* ub_offset;
-  const uint16_t* tl;
-  int32_t ub_stride;
   const double* dz_c;      // nlev x nc
   const double* dzh_c;     // (nlev + 1) x nc
   const double* wlow;      // (nlev + 1) x nc
@@ -292,10 +285,6 @@ __device__ __forceinline__ double edge_w(const MpasTables& T, const MpasFieldsDe
   return M / (w0 * hl + w1 * hr);
 }
 
-template <int LPT, bool VI>
-__device__ __forceinline__ void vn_finish(const MpasTables& T, const MpasFieldsDev& F, int e, int k0, int k1,
-                                          double pressure, const double (&s)[LPT]);
-
 // 5: vn_tendency_kernel! (Tendencies.jl:38-75), flat ground (oro = 0). The TRiSK sums of
 // LPT levels are accumulated neighbour by neighbour so that each table entry is read once.
 template <int LPT, bool VI>
@@ -320,13 +309,6 @@ __device__ __forceinline__ void vn_rows(const MpasTables& T, const MpasFieldsDev
       }
     }
   }
-  vn_finish<LPT, VI>(T, F, e, k0, k1, pressure, s);
-}
-
-// The rest of vn_tendency_kernel! for LPT levels of edge e, given the TRiSK sums s.
-template <int LPT, bool VI>
-__device__ __forceinline__ void vn_finish(const MpasTables& T, const MpasFieldsDev& F, int e, int k0, int k1,
-                                          double pressure, const double (&s)[LPT]) {
   const int l = T.edge_cells[e], r = T.edge_cells[T.lde + e];
   const double w0 = T.edge_weight[e], w1 = T.edge_weight[T.lde + e], invd = T.inverse_dual[e];
   const bool mw = T.vertical == 2;
@@ -361,54 +343,6 @@ __device__ __forceinline__ void vn_finish(const MpasTables& T, const MpasFieldsD
       F.tvn[o] = t - we * (vup - vlow) / T.dz_e[o];
     }
   }
-}
-
-// 5, staged: the block's 128 edges name about 240 distinct edges in their 3 x nt TRiSK entries
-// (16 uses each on a Hilbert-ordered mesh), so F_s and q_e of those edges for the block's LPT
-// levels are loaded once into shared memory (ascending edge order, so neighbouring threads
-// read nearby addresses) and the sums read them there: one gather per distinct edge and level
-// instead of one per entry and level. The sums, their order and every value are those of
-// vn_rows, so the results are the same bit for bit.
-template <int LPT, bool VI>
-__global__ void __launch_bounds__(MB) k_mpas_vn_staged(MpasTables T, MpasFieldsDev F, double pressure) {
-  extern __shared__ double sh[];  // [2][LPT][ub_stride]: F_s, then q_e
-  const int blk = blockIdx.x;
-  const int e = blk * MB + threadIdx.x;
-  const int k0 = blockIdx.y * LPT;
-  const int k1 = min(k0 + LPT, T.nlev);
-  const int u0 = T.ub_offset[blk], nu = T.ub_offset[blk + 1] - u0;
-  double* sF = sh;
-  double* sQ = sh + (size_t)LPT * T.ub_stride;
-  for (int s = threadIdx.x; s < nu; s += MB) {
-    const int g = T.ub_edges[u0 + s];
-#pragma unroll
-    for (int q = 0; q < LPT; ++q)
-      if (k0 + q < k1) {
-        const size_t base = (size_t)(k0 + q) * T.ne;
-        sF[q * T.ub_stride + s] = F.Fs[base + g];
-        sQ[q * T.ub_stride + s] = F.qe[base + g];
-      }
-  }
-  __syncthreads();
-  if (e >= T.ne) return;
-  double s[LPT];
-#pragma unroll
-  for (int q = 0; q < LPT; ++q) s[q] = 0.0;
-  for (int j = 0; j < T.nt; ++j) {
-    const double wt = T.trisk[(size_t)j * T.lde + e];
-    const int a = T.tl[((size_t)0 * T.nt + j) * T.lde + e];
-    const int b = T.tl[((size_t)1 * T.nt + j) * T.lde + e];
-    const int c = T.tl[((size_t)2 * T.nt + j) * T.lde + e];
-#pragma unroll
-    for (int q = 0; q < LPT; ++q) {
-      if (k0 + q < k1) {
-        const double qb = sQ[q * T.ub_stride + b];
-        const double qc = c == b ? qb : sQ[q * T.ub_stride + c];  // the rhombus PV of one edge, twice
-        s[q] += wt * sF[q * T.ub_stride + a] * (qb + qc);
-      }
-    }
-  }
-  vn_finish<LPT, VI>(T, F, e, k0, k1, pressure, s);
 }
 
 template <bool VI>
@@ -510,28 +444,9 @@ void mlaunch(TriskMpas& m, cudaStream_t st, void (*kernel)(KArgs...), int64_t n,
   m.launches++;
 }
 
-// shared memory of the staged vn kernel with LPT levels per thread
-size_t vn_staged_smem(const MpasTables& T, int lpt) { return (size_t)2 * lpt * T.ub_stride * sizeof(double); }
-constexpr size_t VN_STAGED_SMEM_MAX = 200 * 1024;
-
-template <int LPT, bool VI>
-void launch_vn_staged(TriskMpas& m, const MpasFieldsDev& F, double pressure) {
-  const size_t smem = vn_staged_smem(m.T, LPT);
-  CUDA_CHECK(cudaFuncSetAttribute(k_mpas_vn_staged<LPT, VI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  dim3 grid((unsigned)cdiv(m.T.ne, MB), (unsigned)cdiv(m.T.nlev, LPT));
-  k_mpas_vn_staged<LPT, VI><<<grid, MB, smem, m.stream>>>(m.T, F, pressure);
-  CUDA_CHECK(cudaGetLastError());
-  m.launches++;
-}
-
 template <int LPT>
 void launch_vn(TriskMpas& m, const MpasFieldsDev& F, double pressure) {
-  const bool staged = m.T.ub_stride > 0 && vn_staged_smem(m.T, LPT) <= VN_STAGED_SMEM_MAX;
-  if (staged && m.T.vertical > 0)
-    launch_vn_staged<LPT, true>(m, F, pressure);
-  else if (staged)
-    launch_vn_staged<LPT, false>(m, F, pressure);
-  else if (m.T.vertical > 0)
+  if (m.T.vertical > 0)
     mlaunch(m, m.stream, k_mpas_vn<LPT, true>, m.T.ne, m.T.nlev, LPT, m.T, F, pressure);
   else
     mlaunch(m, m.stream, k_mpas_vn<LPT, false>, m.T.ne, m.T.nlev, LPT, m.T, F, pressure);
@@ -680,37 +595,6 @@ int trisk_mpas_create(const TriskMpasTables* t, int32_t device, int32_t levels_p
       }
     T.trisk = m->upload(tw);
     T.ti = m->upload(ti);
-    // staging of the vn kernel: per block of MB edges the distinct edges of its entries
-    const int64_t nblk = cdiv(ne, MB);
-    std::vector<int32_t> ub_offset((size_t)nblk + 1, 0), ub_edges, tl_slot;
-    std::vector<uint16_t> tl((size_t)3 * t->nt * lde, 0);
-    int32_t stride = 0;
-    bool fits = true;
-    for (int64_t b = 0; b < nblk && fits; ++b) {
-      const int64_t e0 = b * MB, e1 = std::min<int64_t>(e0 + MB, ne);
-      std::vector<int32_t> u;
-      for (int c = 0; c < 3; ++c)
-        for (int j = 0; j < t->nt; ++j)
-          for (int64_t e = e0; e < e1; ++e) u.push_back(ti[((size_t)c * t->nt + j) * lde + e]);
-      std::sort(u.begin(), u.end());
-      u.erase(std::unique(u.begin(), u.end()), u.end());
-      if (u.size() > 65535) fits = false;
-      for (int c = 0; c < 3 && fits; ++c)
-        for (int j = 0; j < t->nt; ++j)
-          for (int64_t e = e0; e < e1; ++e) {
-            const size_t at_ = ((size_t)c * t->nt + j) * lde + e;
-            tl[at_] = (uint16_t)(std::lower_bound(u.begin(), u.end(), ti[at_]) - u.begin());
-          }
-      ub_edges.insert(ub_edges.end(), u.begin(), u.end());
-      ub_offset[b + 1] = (int32_t)ub_edges.size();
-      stride = std::max<int32_t>(stride, (int32_t)u.size());
-    }
-    if (fits && !ub_edges.empty()) {
-      T.ub_edges = m->upload(ub_edges);
-      T.ub_offset = m->upload(ub_offset);
-      T.tl = m->upload(tl);
-      T.ub_stride = stride;
-    }
   }
   T.dz_c = m->upload(t->dz_cells, (size_t)nl * nc, "dz_cells");
   T.dzh_c = m->upload(t->dzh_cells, (size_t)(nl + 1) * nc, "dzh_cells");
