@@ -57,6 +57,8 @@ def parse():
     p.add_argument("--no-closure", action="store_true", help="skip the learned-closure leg")
     p.add_argument("--no-hexagon5", action="store_true", help="skip the hexagon-5 CPU/GPU leg")
     p.add_argument("--ensemble-days", type=float, default=1.0, help="simulated days of the ensemble leg")
+    p.add_argument("--ensemble-groups", default=None,
+                   help="groups of the ensemble leg as level x members, e.g. 7x8,6x32 (default: configuration 3)")
     p.add_argument("--no-icon", action="store_true", help="skip the ICON triangle-model leg")
     p.add_argument("--icon-level", type=int, default=8, help="triangle level of the ICON leg (8: 1.31 M cells)")
     p.add_argument("--icon-steps", type=int, default=100, help="timed RK4 steps of the ICON leg")
@@ -469,17 +471,18 @@ def ncu_traffic(kernel):
 ENSEMBLE_GROUPS = ((5, 64), (6, 32), (7, 8))  # (mesh level, members), one simulated day, FP64
 
 
-def run_ensemble_leg(local_rank, seed, days=1.0, state_bits=64):
+def run_ensemble_leg(local_rank, seed, days=1.0, state_bits=64, groups_spec=ENSEMBLE_GROUPS):
     """Batched ensemble of three mesh levels in one persistent CUDA-graph launch per phase:
     every member has its own seed, harmonic degree <= 12 and height rms in 50-300 m; each
     level has its own dt (Courant 0.5) and runs `days` simulated days (state_bits 32: the
-    states and work vectors are stored as float, the arithmetic stays FP64)."""
+    states and work vectors are stored as float, the arithmetic stays FP64). groups_spec:
+    (level, members) of each group, configuration 3's by default."""
     import torch
     import dmplex_b200 as d
     from dmplex_b200 import workloads as w
     si = w.si_parameters()
     groups, info = [], []
-    for level, members in ENSEMBLE_GROUPS:
+    for level, members in groups_spec:
         g = d.TRiSKGrid(d.create_hexagon_mesh(level, centroidal=True))
         m = d.TRiSKShallowWater(g, pv_flux=PV, kinetic_energy=KE, device=local_rank, **si)
         nsteps, dt = w.day_steps(g)
@@ -511,7 +514,7 @@ def run_ensemble_leg(local_rank, seed, days=1.0, state_bits=64):
         n_b *= state_bits / 64  # the state in its storage precision
         nbytes += s * (4 * (T + 2 * members * n_b) + 15 * members * n_b)
     peak, _ = measured_peak()
-    return {"workload": "ensemble " + " + ".join(f"{k}x hexagon{l}" for l, k in ENSEMBLE_GROUPS) +
+    return {"workload": "ensemble " + " + ".join(f"{k}x hexagon{l}" for l, k in groups_spec) +
                         f", {PV}/{KE}, {'FP64' if state_bits == 64 else 'FP32 state, FP64 arithmetic'}, "
                         f"{days:g} simulated day each",
             "value": cell_steps / (ms * 1e-3), "unit": "cell-steps/s",
@@ -829,9 +832,12 @@ def run_b200(args, rank, world, local_rank):
 
     ensemble = None
     if not args.no_ensemble:
-        ensemble = optional_leg(run_ensemble_leg, local_rank, seed=1000 * (rank + 1), days=args.ensemble_days)
+        spec = ENSEMBLE_GROUPS if not args.ensemble_groups else \
+            tuple(tuple(int(v) for v in gr.split("x")) for gr in args.ensemble_groups.split(","))
+        ensemble = optional_leg(run_ensemble_leg, local_rank, seed=1000 * (rank + 1), days=args.ensemble_days,
+                                groups_spec=spec)
         f32 = optional_leg(run_ensemble_leg, local_rank, seed=1000 * (rank + 1), days=args.ensemble_days,
-                           state_bits=32)
+                           state_bits=32, groups_spec=spec)
         if "error" not in ensemble and "error" not in f32:
             ensemble["fp32_state"] = {k: f32[k] for k in ("value", "gpu_seconds_per_simulated_day", "gbs", "frac")}
         if world > 1 and "error" not in ensemble:
