@@ -58,7 +58,7 @@ def parse():
     p.add_argument("--no-hexagon5", action="store_true", help="skip the hexagon-5 CPU/GPU leg")
     p.add_argument("--ensemble-days", type=float, default=1.0, help="simulated days of the ensemble leg")
     p.add_argument("--ensemble-groups", default=None,
-                   help="groups of the ensemble leg as level x members, e.g. 7x8,6x32 (default: configuration 3)")
+                   help="groups of the ensemble leg as level x members, e.g. 7x8,6x32 (default: 5x64,6x32,7x8)")
     p.add_argument("--no-icon", action="store_true", help="skip the ICON triangle-model leg")
     p.add_argument("--icon-level", type=int, default=8, help="triangle level of the ICON leg (8: 1.31 M cells)")
     p.add_argument("--icon-steps", type=int, default=100, help="timed RK4 steps of the ICON leg")
@@ -476,7 +476,7 @@ def run_ensemble_leg(local_rank, seed, days=1.0, state_bits=64, groups_spec=ENSE
     every member has its own seed, harmonic degree <= 12 and height rms in 50-300 m; each
     level has its own dt (Courant 0.5) and runs `days` simulated days (state_bits 32: the
     states and work vectors are stored as float, the arithmetic stays FP64). groups_spec:
-    (level, members) of each group, configuration 3's by default."""
+    (level, members) of each group, 64 x hexagon 5, 32 x hexagon 6 and 8 x hexagon 7 by default."""
     import torch
     import dmplex_b200 as d
     from dmplex_b200 import workloads as w
@@ -643,7 +643,7 @@ def run_closure_leg(local_rank, members=128, seed=7):
 
 
 def closure_errors(local_rank, g6, g7, g8, net, norm, costs, seeds=(2001, 2002), days=2):
-    """The north-star comparison measured here: fine hexagon-8 runs (dt 20 s) from held-out
+    """The closure's comparison measured here: fine hexagon-8 runs (dt 20 s) from held-out
     seeds, coarse-grained to hexagon 6 every day, judge plain FP64 hexagon 6 (dt 150 s) and 7
     (dt 75 s, coarse-grained to hexagon 6 for the comparison) and the closure on hexagon 6 (FP32
     state, energy-drift fallback); then the GPU seconds per member-day the plain method needs

@@ -2,7 +2,7 @@
 
 An edge-local MLP 24 -> 64 -> 64 -> 2 with GELU: BF16 weights and activations, FP32
 accumulation, FP32 master weights updated by Adam. There is no closure in the reference;
-the plain FP64 method stays the judge of its error and its fallback (workloads, bench).
+the plain FP64 method stays the measure of its error and its fallback (workloads, bench).
 Device arrays are CUDA torch tensors: features (n, 24) bfloat16, targets and outputs
 (n, 2) float32.
 """

@@ -538,7 +538,7 @@ def evaluate(gf, gc, mlp, norm, eval_seeds=4, eval_days=10, coarse_dt=150.0, fin
 
 
 def equal_error_table(gf, gc, mlp, norm, seeds, days, coarse_dt, daily, runs, device=0, log=print):
-    """The north star's comparison at equal h L2 error: plain FP64 runs one level finer than
+    """The comparison at equal h L2 error: plain FP64 runs one level finer than
     the coarse mesh (dt halved) judged on the coarse mesh like the others, the GPU seconds per
     member-day of large ensembles (128 coarse members, 32 finer ones; the closure with FP32
     state), and per day the plain cost at the closure's error (log-linear between the two plain

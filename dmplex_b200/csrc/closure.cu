@@ -2,7 +2,7 @@
 // layers run on the 5th-generation tensor cores (tcgen05.mma, BF16 operands in shared
 // memory, FP32 accumulators in tensor memory), for inference and for training.
 //
-// There is no closure in the reference; this is the north star's addition. The MLP reads
+// There is no closure in the reference; the closure is this library's addition. The MLP reads
 // 24 normalized features of an edge and returns two corrections (to the edge mass flux and
 // to the edge momentum tendency).
 //

@@ -549,7 +549,7 @@ void build_numbering(TriskModel& m, const Coefficients& C, const std::vector<V3>
 // [k][ld] int32 table in internal numbering from a [k + w*entity] file-numbered table.
 size_t pack_index(Packer& P, const std::vector<int64_t>& tab, int w, int wpad, int64_t n, int64_t ld,
                   const std::vector<int32_t>& n2o, const std::vector<int32_t>& target_o2n) {
-  if (w > wpad) throw Error(TRISK_ERR_UNSUPPORTED, "neighbour table wider than this build supports");
+  if (w > wpad) throw Error(TRISK_ERR_UNSUPPORTED, "neighbour table wider than the kernels support");
   const size_t off = P.add((size_t)wpad * ld * sizeof(int32_t));
   int32_t* out = P.at<int32_t>(off);
   for (int64_t j = 0; j < n; ++j) {
@@ -561,7 +561,7 @@ size_t pack_index(Packer& P, const std::vector<int64_t>& tab, int w, int wpad, i
 
 size_t pack_weight(Packer& P, const std::vector<double>& tab, int w, int wpad, int64_t n, int64_t ld,
                    const std::vector<int32_t>& n2o) {
-  if (w > wpad) throw Error(TRISK_ERR_UNSUPPORTED, "neighbour table wider than this build supports");
+  if (w > wpad) throw Error(TRISK_ERR_UNSUPPORTED, "neighbour table wider than the kernels support");
   const size_t off = P.add((size_t)wpad * ld * sizeof(double));
   double* out = P.at<double>(off);
   for (int64_t j = 0; j < n; ++j) {

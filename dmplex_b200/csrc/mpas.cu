@@ -522,7 +522,7 @@ int trisk_mpas_create(const TriskMpasTables* t, int32_t device, int32_t levels_p
   if (t->nc < 1 || t->ne < 1 || t->nv < 1 || t->nlev < 2)
     throw Error(TRISK_ERR_ARGUMENT, "need cells, edges, vertices and at least two layers");
   if (t->cw < 3 || t->cw > MCW || t->vw < 1 || t->vw > MVW || t->nt < 1 || t->nt > MNT)
-    throw Error(TRISK_ERR_UNSUPPORTED, "tables wider than this build handles (10 edges per cell, 4 per vertex, "
+    throw Error(TRISK_ERR_UNSUPPORTED, "tables wider than the kernels handle (10 edges per cell, 4 per vertex, "
                                        "18 TRiSK neighbours)");
   if (t->vertical < 0 || t->vertical > 2) throw Error(TRISK_ERR_ARGUMENT, "vertical must be 0, 1 or 2");
   if (t->five_band && t->vertical == 0)

@@ -33,7 +33,7 @@ enum {
   TRISK_ERR_CUDA = 3,        /* a CUDA call failed, or no GPU */
   TRISK_ERR_NONFINITE = 4,   /* the state became non-finite during the call */
   TRISK_ERR_TIMEOUT = 5,     /* a bounded device wait gave up */
-  TRISK_ERR_UNSUPPORTED = 6, /* valid input this build does not handle */
+  TRISK_ERR_UNSUPPORTED = 6, /* valid input the library does not handle */
   TRISK_ERR_MESH = 7         /* mesh generation or grid construction failed */
 };
 enum { TRISK_PV_TRISK = 0, TRISK_PV_GASSMANN = 1, TRISK_PV_GASSMANN_MEAN = 2 };
@@ -257,7 +257,7 @@ int trisk_l2_info(int32_t device, int64_t info[4]);
  * kernel launch and returns the mean duration in ms of each phase kernel in ms[3]. */
 int trisk_profile_phases(TriskModel* model, double* y_device, double dt, int64_t nsteps, double ms[3]);
 
-/* ---- ICON triangle shallow water (ICONShallowWater.jl) ----------------
+/* ---- ICON triangle shallow water (ICONShallowWater.jl) -----------------------------
  * Replaces ICONShallowWater(grid; gravity, coriolis, rbf_scale, divergence_damping,
  * kinetic_gradient) (src/FiniteVolumes/ICONShallowWater.jl:96-147): the premultiplied
  * coefficients of that constructor, 1-based Int64 and (entity, k) ordered as Julia holds
