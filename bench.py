@@ -548,10 +548,11 @@ def run_closure_leg(local_rank, members=128, seed=7):
     m6 = d.TRiSKShallowWater(g6, pv_flux="trisk", kinetic_energy="cell", device=local_rank, **si)
     states = w.ensemble_members(g6, members, seed=seed, degree=8, rms_range=(100.0, 100.0))
     steps = 576
-    net, norm = None, None
+    net, norm, every = None, None, 1
     if os.path.exists(CLOSURE_WEIGHTS):
         z = np.load(CLOSURE_WEIGHTS)
         net, norm = ClosureMLP(z["params"], device=local_rank), z["norm"]
+        every = int(z["closure_every"]) if "closure_every" in z.files else 1
         out["weights"] = "trained (dmplex_b200/data/closure_hexagon6.npz)"
     else:
         net = ClosureMLP(device=local_rank, seed=0)
@@ -563,7 +564,7 @@ def run_closure_leg(local_rank, members=128, seed=7):
         for k, y in enumerate(states):
             ens.set_member(0, k, y)
         if with_closure:
-            ens.set_closure(0, net, edge_geometry(g6), norm)
+            ens.set_closure(0, net, edge_geometry(g6), norm, every=every)
         e0 = ens.energy(0)
         ens.run(2)
         ens.reset()
@@ -625,7 +626,8 @@ def run_closure_leg(local_rank, members=128, seed=7):
     e7.synchronize()
     out["plain_hexagon7_fp64_gpu_seconds_per_member_day"] = a.elapsed_time(b) / 1e3 / 96 * 1152 / 32
     del e7
-    out["measured_errors"] = optional_leg(closure_errors, local_rank, g6, g7, g8, net, norm, out)
+    out["network_every_steps"] = every
+    out["measured_errors"] = optional_leg(closure_errors, local_rank, g6, g7, g8, net, norm, out, every=every)
     if os.path.exists(CLOSURE_SUMMARY):
         with open(CLOSURE_SUMMARY) as f:
             s = json.load(f)
@@ -642,7 +644,7 @@ def run_closure_leg(local_rank, members=128, seed=7):
     return out
 
 
-def closure_errors(local_rank, g6, g7, g8, net, norm, costs, seeds=(2001, 2002), days=2):
+def closure_errors(local_rank, g6, g7, g8, net, norm, costs, seeds=(2001, 2002), days=2, every=1):
     """The closure's comparison measured here: fine hexagon-8 runs (dt 20 s) from held-out
     seeds, coarse-grained to hexagon 6 every day, judge plain FP64 hexagon 6 (dt 150 s) and 7
     (dt 75 s, coarse-grained to hexagon 6 for the comparison) and the closure on hexagon 6 (FP32
@@ -655,7 +657,7 @@ def closure_errors(local_rank, g6, g7, g8, net, norm, costs, seeds=(2001, 2002),
     init = daily[0]
     runs = {"plain_hexagon6_fp64": cp.run_coarse(g6, init, days, 150.0, daily, device=local_rank),
             "closure_hexagon6": cp.run_coarse(g6, init, days, 150.0, daily, net, norm, device=local_rank,
-                                              state_bits=32),
+                                              state_bits=32, every=every),
             "plain_hexagon7_fp64": cp.plain_level_errors(g8, g6, g7, list(seeds), days, 75.0, daily,
                                                          device=local_rank)}
     err = {k: [float(np.mean(x)) for x in r["h_l2"]] for k, r in runs.items()}

@@ -278,12 +278,13 @@ def l2_errors(gc, Vc, Y, Yt):
 
 
 def run_coarse(gc, Y_init, days, dt, daily_truth, mlp=None, norm=None, drift_per_day=1e-6, device=0,
-               every_stage=False, momentum_scale=1.0, state_bits=64, checks_per_day=8, work_free=False):
+               every_stage=False, momentum_scale=1.0, state_bits=64, checks_per_day=8, work_free=False, every=1):
     """Coarse ensemble (members = columns of Y_init) for `days` days; h and vorticity errors
     against the daily truth, GPU seconds, and the members that fell back to the plain step
     (energy drift per elapsed day above drift_per_day, checked checks_per_day times a day).
     momentum_scale multiplies the closure's momentum correction (0 keeps only the mass-flux
-    correction); state_bits 32 stores the members' states as float."""
+    correction); state_bits 32 stores the members' states as float; every: the network runs
+    on every `every`-th step, its corrections kept in between."""
     if norm is not None:
         norm = np.array(norm, dtype=np.float64)
         norm[2 * NFEAT + 1] *= momentum_scale
@@ -298,7 +299,7 @@ def run_coarse(gc, Y_init, days, dt, daily_truth, mlp=None, norm=None, drift_per
         col.copy_(Y_init[:, k])
         ens.set_member(0, k, col)
     if mlp is not None:
-        ens.set_closure(0, mlp, edge_geometry(gc), norm, every_stage, work_free)
+        ens.set_closure(0, mlp, edge_geometry(gc), norm, every_stage, work_free, every=every)
     on = np.ones(S, dtype=np.float32)
     e0 = ens.energy(0)
     Vc = relative_vorticity_matrix(model_tables(gc, pv_flux=PV, kinetic_energy=KE, **si))
@@ -377,9 +378,11 @@ def plain_level_errors(gf, gc, gm, seeds, days, dt, daily_truth, device=0, state
             "cells": int(gm.nc), "dt": 86400 / steps_day, "members": S, "state_bits": state_bits}
 
 
-def member_day_cost(g, members, dt, state_bits=64, mlp=None, norm=None, steps=96, device=0, seed=3) -> float:
+def member_day_cost(g, members, dt, state_bits=64, mlp=None, norm=None, steps=96, device=0, seed=3,
+                    every=1) -> float:
     """GPU seconds per member and simulated day of a `members`-member ensemble on grid g at
-    time step dt (with the closure if mlp is given), from `steps` timed steps after a warm-up."""
+    time step dt (with the closure if mlp is given, its network every `every` steps), from
+    `steps` timed steps after a warm-up."""
     import torch
     si = w.si_parameters()
     m = TRiSKShallowWater(g, pv_flux=PV, kinetic_energy=KE, device=device, **si)
@@ -387,7 +390,7 @@ def member_day_cost(g, members, dt, state_bits=64, mlp=None, norm=None, steps=96
     for k, y in enumerate(w.ensemble_members(g, members, seed=seed, degree=8, rms_range=(100.0, 100.0))):
         ens.set_member(0, k, y)
     if mlp is not None:
-        ens.set_closure(0, mlp, edge_geometry(g), norm)
+        ens.set_closure(0, mlp, edge_geometry(g), norm, every=every)
     ens.run(2)
     stream = torch.cuda.ExternalStream(ens.stream(), device=device)
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -410,7 +413,7 @@ def equal_error_cost(errors: dict, costs: dict, target: float) -> float:
 
 
 def calibrate(gf, gc, mlp, norm, seeds=(501, 502), days=2, coarse_dt=150.0, fine_dt=20.0,
-              scales=(0.0, 0.05, 0.1, 0.2, 0.4, 1.0), device=0, log=print, work_free=False, daily=None):
+              scales=(0.0, 0.05, 0.1, 0.2, 0.4, 1.0), device=0, log=print, work_free=False, daily=None, every=1):
     """A-posteriori choice of the momentum correction's scale: coarse runs with the closure
     (no fallback, mass-flux part unscaled) from validation seeds, none of them a training or
     evaluation seed, against their coarse-grained fine runs (daily: those, if already made);
@@ -422,7 +425,7 @@ def calibrate(gf, gc, mlp, norm, seeds=(501, 502), days=2, coarse_dt=150.0, fine
     table = {}
     for sc in scales:
         r = run_coarse(gc, daily[0], days, coarse_dt, daily, mlp, norm, drift_per_day=np.inf, device=device,
-                       momentum_scale=sc, state_bits=32, work_free=work_free)
+                       momentum_scale=sc, state_bits=32, work_free=work_free, every=every)
         err = float(np.mean(r["h_l2"])) if r["diverged_on_day"] is None else float("inf")
         table[str(sc)] = err
         log(f"calibration: momentum scale {sc}: mean h L2 over {days} days {err:.3f} m")
@@ -433,7 +436,7 @@ def calibrate(gf, gc, mlp, norm, seeds=(501, 502), days=2, coarse_dt=150.0, fine
 def pipeline(fine_level=8, coarse_level=6, train_seeds=32, train_days=10, snapshots=2000, eval_seeds=4,
              eval_days=10, coarse_dt=150.0, window=1800.0, fine_dt=20.0, epochs=3, device=0, out_params=None,
              target="tendency", log=print, input_noise=(0.0,), calibrate_days=4,
-             scales=(0.0, 0.05, 0.1, 0.15, 0.2, 0.25, 0.3)):
+             scales=(0.0, 0.05, 0.1, 0.15, 0.2, 0.25, 0.3), every=1):
     """The whole closure experiment; returns a JSON-able summary. target "tendency": the
     residual is the coarse model's missing tendency at the coarse-grained state; "window":
     the mean missing tendency over `window` seconds (window / fine_dt fine steps, window /
@@ -471,18 +474,18 @@ def pipeline(fine_level=8, coarse_level=6, train_seeds=32, train_days=10, snapsh
         log(f"input noise {noise}: training loss per epoch {history}, held-out {held:.4f} (without the closure "
             f"{zero:.4f}), skill (mass flux, momentum) {skill}")
         scale, table = calibrate(gf, gc, mlp, norm, days=calibrate_days, coarse_dt=coarse_dt, fine_dt=fine_dt,
-                                 scales=scales, device=device, log=log, daily=cal_daily)
+                                 scales=scales, device=device, log=log, daily=cal_daily, every=every)
         vnorm = np.array(norm, dtype=np.float64)
         vnorm[2 * NFEAT + 1] *= scale  # the calibrated momentum scale is part of the saved closure
         if out_params and not results:
             np.savez(out_params, params=mlp.params(), norm=vnorm, fine_level=fine_level, coarse_level=coarse_level,
                      window=window if target == "window" else 0.0, target=target, momentum_scale=scale,
-                     input_noise=noise)
+                     input_noise=noise, closure_every=every)
         r = {"input_noise": noise, "train_loss": history, "heldout_loss": held, "heldout_loss_without_closure": zero,
              "output_skill": skill, "calibrated_momentum_scale": scale, "calibration_mean_h_l2": table,
              "calibration_days": calibrate_days}
         r.update(evaluate(gf, gc, mlp, vnorm, eval_seeds, eval_days, coarse_dt, fine_dt, device, log,
-                          daily=eval_daily, fine_eval_seconds=fine_eval_s))
+                          daily=eval_daily, fine_eval_seconds=fine_eval_s, every=every))
         results.append(r)
     del X, T
     torch.cuda.empty_cache()
@@ -501,12 +504,13 @@ def pipeline(fine_level=8, coarse_level=6, train_seeds=32, train_days=10, snapsh
 
 
 def evaluate(gf, gc, mlp, norm, eval_seeds=4, eval_days=10, coarse_dt=150.0, fine_dt=20.0, device=0, log=print,
-             work_free=False, daily=None, fine_eval_seconds=None):
+             work_free=False, daily=None, fine_eval_seconds=None, every=1):
     """Coarse runs from the coarse-grained state of held-out seeds against the coarse-grained
     fine run (daily: that run's daily coarse-grained states, if already made): plain (FP64 and
     FP32 state), and with FP32 state the closure with the energy-drift fallback, without it,
     evaluated at every RK4 stage, and the mass-flux correction alone; then the equal-error
-    table."""
+    table. every: the closure runs its network every `every` steps (not in the every-stage
+    variant)."""
     eval_list = list(range(1001, 1001 + eval_seeds))
     fine_eval_s = fine_eval_seconds
     if daily is None:
@@ -517,6 +521,7 @@ def evaluate(gf, gc, mlp, norm, eval_seeds=4, eval_days=10, coarse_dt=150.0, fin
     init = daily[0]
     f32 = {"state_bits": 32}
     out["work_free_momentum_correction"] = bool(work_free)
+    out["closure_every"] = int(every)
     variants = {"plain_coarse": {},
                 "plain_coarse_fp32": dict(f32),
                 "closure_coarse": {"mlp": mlp, "norm": norm, **f32},
@@ -528,16 +533,19 @@ def evaluate(gf, gc, mlp, norm, eval_seeds=4, eval_days=10, coarse_dt=150.0, fin
     for name, kw in variants.items():
         if "mlp" in kw:
             kw["work_free"] = work_free
+            if not kw.get("every_stage"):
+                kw["every"] = every
         r = run_coarse(gc, init, eval_days, coarse_dt, daily, device=device, **kw)
         out[name] = r
         log(f"{name}: h L2 per day {[round(float(np.mean(x)), 2) for x in r['h_l2']]}, vorticity "
             f"{[float('%.3g' % np.mean(x)) for x in r['zeta_l2']]}, fallback {r['fallback_members']}, "
             f"diverged on day {r['diverged_on_day']}")
-    out.update(equal_error_table(gf, gc, mlp, norm, eval_list, eval_days, coarse_dt, daily, out, device, log))
+    out.update(equal_error_table(gf, gc, mlp, norm, eval_list, eval_days, coarse_dt, daily, out, device, log,
+                                 every=every))
     return out
 
 
-def equal_error_table(gf, gc, mlp, norm, seeds, days, coarse_dt, daily, runs, device=0, log=print):
+def equal_error_table(gf, gc, mlp, norm, seeds, days, coarse_dt, daily, runs, device=0, log=print, every=1):
     """The comparison at equal h L2 error: plain FP64 runs one level finer than
     the coarse mesh (dt halved) judged on the coarse mesh like the others, the GPU seconds per
     member-day of large ensembles (128 coarse members, 32 finer ones; the closure with FP32
@@ -548,7 +556,7 @@ def equal_error_table(gf, gc, mlp, norm, seeds, days, coarse_dt, daily, runs, de
     inter = plain_level_errors(gf, gc, gm, seeds, days, coarse_dt / 2, daily, device=device)
     costs = {"plain_coarse_fp64": member_day_cost(gc, 128, coarse_dt, 64, device=device),
              "plain_finer_fp64": member_day_cost(gm, 32, coarse_dt / 2, 64, device=device),
-             "closure_coarse_fp32": member_day_cost(gc, 128, coarse_dt, 32, mlp, norm, device=device)}
+             "closure_coarse_fp32": member_day_cost(gc, 128, coarse_dt, 32, mlp, norm, device=device, every=every)}
     table = []
     closure = runs.get("closure_coarse", {}).get("h_l2", [])
     for d in range(min(days, len(closure))):
@@ -596,6 +604,8 @@ def main():
                    help="with --evaluate: the momentum correction does no work on each member's flow")
     p.add_argument("--scales", default="0,0.05,0.1,0.15,0.2,0.25,0.3", help="momentum scales the calibration tries")
     p.add_argument("--input-noise", default="0", help="comma-separated: one network per training-input noise level")
+    p.add_argument("--closure-every", type=int, default=1,
+                   help="run the network every N steps and keep its corrections in between")
     a = p.parse_args()
     scales = tuple(float(x) for x in a.scales.split(","))
     if a.evaluate:
@@ -612,21 +622,22 @@ def main():
                 raise SystemExit("the saved closure's momentum output is off; nothing to re-calibrate")
             norm[2 * NFEAT + 1] /= old
             scale, table = calibrate(gf, gc, mlp, norm, days=a.calibrate_days, coarse_dt=a.coarse_dt,
-                                     fine_dt=a.fine_dt, scales=scales, work_free=a.work_free)
+                                     fine_dt=a.fine_dt, scales=scales, work_free=a.work_free, every=a.closure_every)
             norm[2 * NFEAT + 1] *= scale
             s.update({"calibrated_momentum_scale": scale, "calibration_mean_h_l2": table,
                       "calibration_days": a.calibrate_days})
             if a.params:
-                np.savez(a.params, **{k: z[k] for k in z.files if k not in ("norm", "momentum_scale", "work_free")},
-                         norm=norm, momentum_scale=scale, work_free=a.work_free)
+                np.savez(a.params, **{k: z[k] for k in z.files
+                                      if k not in ("norm", "momentum_scale", "work_free", "closure_every")},
+                         norm=norm, momentum_scale=scale, work_free=a.work_free, closure_every=a.closure_every)
         s.update(evaluate(gf, gc, mlp, norm, a.eval_seeds, a.eval_days, a.coarse_dt, a.fine_dt,
-                          work_free=a.work_free))
+                          work_free=a.work_free, every=a.closure_every))
     else:
         s = pipeline(a.fine, a.coarse, a.train_seeds, a.train_days, a.snapshots, a.eval_seeds, a.eval_days,
                      a.coarse_dt, a.window, a.fine_dt, a.epochs, out_params=a.params, target=a.target,
                      input_noise=tuple(float(x) for x in a.input_noise.split(",")),
-                     calibrate_days=a.calibrate_days, scales=scales)
-        s["command"] = "python -m dmplex_b200.closure_pipeline " + " ".join(__import__("sys").argv[1:])
+                     calibrate_days=a.calibrate_days, scales=scales, every=a.closure_every)
+    s["command"] = "python -m dmplex_b200.closure_pipeline " + " ".join(__import__("sys").argv[1:])
     with open(a.out, "w") as f:
         json.dump(s, f, indent=1)
     print(json.dumps({k: v for k, v in s.items() if not isinstance(v, dict)}))

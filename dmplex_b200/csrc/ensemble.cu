@@ -220,6 +220,20 @@ __global__ void kg_closure_apply(R* dF, R* dq, const float* Y, const float* memb
   apply_row<R>(dF, dq, r, M, member_on, sF, sQ, Y[2 * r], Y[2 * r + 1]);
 }
 
+// The corrections of the members whose closure is off set to zero (kept corrections of a member
+// that falls back must not outlive the fallback).
+template <class R>
+__global__ void kg_zero_off_members(R* dF, R* dq, const float* member_on, int64_t rows, int M) {
+  const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (r >= rows) return;
+  int e, m;
+  split<true>((int)r, M, e, m);
+  if (member_on[m] == 0.0f) {
+    dF[r] = (R)0.0;
+    dq[r] = (R)0.0;
+  }
+}
+
 // The closure of a slice's rows in one kernel, bit for bit kg_features, the network's inference
 // and kg_closure_apply in turn: per tile of 128 (edge, member) rows every thread builds its
 // row's features straight into the tile's shared-memory operand, the tile runs through the
@@ -230,13 +244,14 @@ template <class R>
 __global__ void __launch_bounds__(closure::TILE) kg_closure_fused(
     DevTables T, DevWorkT<R> W, const R* y, int M, const float* geom, const FeatureNorm N,
     const closure::ParamsBF16* wbf, const closure::Params* p, const float* member_on, double sF, double sQ, R* dF,
-    R* dq, int64_t rows, closure::Status* status) {
+    R* dq, int64_t rows, closure::Status* status, const int* counter, int every) {
   using namespace closure;
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ __align__(16) InferStatic st;
   const int t = threadIdx.x;
   const int64_t ntiles = (rows + TILE - 1) / TILE;
   if ((int64_t)blockIdx.x >= ntiles) return;
+  if (every > 1 && *counter % every != 0) return;  // not a network step: the corrections are kept
   const InferSmem S(smem);
   const uint32_t tmem = infer_setup(S, st, wbf, p);
   MmaWaits waits(smem_u32(S.mbar), &st.abort);
@@ -399,6 +414,7 @@ struct ClosureSlot {
   bool every_stage = false;    // false: the network runs at stage 1 and its output is reused
   bool work_free = false;      // project the momentum correction to do no work (per member)
   bool fused = true;           // features, network and corrections in one kernel (else three)
+  int every = 1;               // the network runs every `every` steps; its corrections are kept between
   int fused_per_sm = 1;        // resident CTAs per SM of the fused kernel
   double* sums = nullptr;      // 2 M: <g, dq>, <g, g> per member
   double* partials = nullptr;  // 2 M x WORK_SUM_BLOCKS per-block partial sums of them
@@ -677,7 +693,7 @@ void enqueue_closure(TriskEnsemble& e, const std::vector<int>& set_slices, int s
         const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)e.sms * c.fused_per_sm));
         kg_closure_fused<R><<<grid, closure::TILE, closure::FWD_SMEM_BYTES, e.stream>>>(
             D.T, work_as<R>(D.W), ys, D.M, c.geom, c.norm, wbf, p, c.member_on + sl.m0, c.norm.out_scale[0],
-            c.norm.out_scale[1], dF, dq, rows, status);
+            c.norm.out_scale[1], dF, dq, rows, status, D.counter, c.every);
         CUDA_CHECK(cudaGetLastError());
         e.launches -= 2;  // one launch instead of three
       } else {
@@ -1221,6 +1237,9 @@ int trisk_ensemble_set_closure(TriskEnsemble* ens, int32_t group, TriskClosure* 
   c.every_stage = (flags & 1) != 0;
   c.work_free = (flags & 2) != 0;
   c.fused = (flags & 4) == 0;
+  c.every = std::max(1, (flags >> 8) & 0xFF);
+  if (c.every > 1 && (c.every_stage || !c.fused))
+    throw Error(TRISK_ERR_UNSUPPORTED, "a network interval of several steps needs the fused kernel, at stage 1 only");
   if (c.fused)
     with_real(e, [&](auto r) {
       using R = decltype(r);
@@ -1245,6 +1264,18 @@ int trisk_ensemble_closure_mask(TriskEnsemble* ens, int32_t group, const float* 
   if (!c.net) throw Error(TRISK_ERR_ARGUMENT, "the group has no closure");
   DeviceGuard guard(e.device);
   CUDA_CHECK(cudaMemcpyAsync(c.member_on, member_on, G.M * sizeof(float), cudaMemcpyHostToDevice, e.stream));
+  for (const Slice& sl : e.slices) {  // kept corrections of the members turned off
+    if (&e.groups[sl.group] != &G) continue;
+    const int64_t ne = sl.D.T.ne, rows = ne * sl.D.M, r0 = ne * sl.m0;
+    with_real(e, [&](auto r) {
+      using R = decltype(r);
+      kg_zero_off_members<R><<<(unsigned)cdiv(rows, 256), 256, 0, e.stream>>>(
+          reinterpret_cast<R*>(e.at(c.dF, r0)), reinterpret_cast<R*>(e.at(c.dq, r0)), c.member_on + sl.m0, rows,
+          sl.D.M);
+    });
+    CUDA_CHECK(cudaGetLastError());
+    e.launches++;
+  }
   CUDA_CHECK(cudaStreamSynchronize(e.stream));
   TRISK_API_END
 }

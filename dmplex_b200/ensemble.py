@@ -118,12 +118,15 @@ class Ensemble:
         return out
 
     def set_closure(self, group: int, net, geometry: np.ndarray, norm: np.ndarray, every_stage: bool = False,
-                    work_free: bool = False, fused: bool = True):
+                    work_free: bool = False, fused: bool = True, every: int = 1):
         """Learned closure for a group (net: closure.ClosureMLP, or None to remove it).
         every_stage: run the network at every RK4 stage; work_free: remove from each member's
         momentum correction its component along the energy gradient (no work on the flow);
         fused: features, network and corrections in one kernel (False: three launches with the
-        features and outputs in HBM; the same numbers)."""
+        features and outputs in HBM; the same numbers); every: run the network on every
+        `every`-th step and keep its corrections on the steps between."""
+        if not 1 <= int(every) <= 255:
+            raise ValueError("every must be in 1..255")
         if net is None:
             check(lib.trisk_ensemble_set_closure(self._h, group, None, None, None, 0))
             self._net = None
@@ -132,7 +135,7 @@ class Ensemble:
         norm = np.ascontiguousarray(norm, dtype=np.float64)
         check(lib.trisk_ensemble_set_closure(self._h, group, net.handle, geometry.ctypes.data, norm.ctypes.data,
                                              int(bool(every_stage)) | (2 if work_free else 0) |
-                                             (0 if fused else 4)))
+                                             (0 if fused else 4) | (int(every) << 8)))
         self._net = net  # the ensemble launches it
 
     def closure_mask(self, group: int, member_on) -> None:

@@ -483,7 +483,11 @@ int trisk_ensemble_energy(TriskEnsemble* ensemble, int32_t group, double* energi
  * cell distances are geometry columns 0..3) is removed, so it does no work on the flow to
  * first order; bit 2 (4) runs the features, the network and the corrections as three launches
  * with the features and outputs in device memory, instead of one kernel that builds each tile's
- * features in shared memory and applies its outputs there (the same numbers bit for bit).
+ * features in shared memory and applies its outputs there (the same numbers bit for bit);
+ * bits 8-15: the network interval n (0 or 1: every step): the network runs on the steps whose
+ * group step count is a multiple of n and its corrections are kept and applied on the steps
+ * between (needs the one-kernel form at stage 1 only, else TRISK_ERR_UNSUPPORTED). Turning
+ * a member off (trisk_ensemble_closure_mask) clears its kept corrections at once.
  * net = NULL removes the group's closure. */
 int trisk_ensemble_set_closure(TriskEnsemble* ensemble, int32_t group, TriskClosure* net, const float* geometry,
                                const double* norm, int32_t flags);

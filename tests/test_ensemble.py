@@ -308,3 +308,68 @@ def test_fused_closure_kernel_equals_three_launches(require_gpu, state_bits):
             out.append([ens.get_member(0, k) for k in range(M)])
         for a, b in zip(*out):
             assert np.array_equal(a, b)
+
+
+def test_closure_network_interval(require_gpu):
+    """The network every n steps with its corrections kept between: a network of constant
+    output gives the every-step run bit for bit; a real network gives the every-step run on the
+    first step and a different one after; a member turned off loses its kept corrections at
+    once and then follows the plain step bit for bit; the interval needs the one-kernel form at
+    stage 1."""
+    from oracle import closure_oracle as co
+    from dmplex_b200.closure import ClosureMLP
+    from dmplex_b200.coarsen import edge_geometry
+    si = w.si_parameters()
+    g = trisk_grid(4, True)
+    m = d.TRiSKShallowWater(g, pv_flux="trisk", kinetic_energy="cell", **si)
+    M = 4
+    states = member_states(g, M, 51)
+    u = np.abs(states[0][:g.ne]).mean()
+    norm = np.concatenate([np.zeros(24), np.ones(24), [1e-3 * u, 1e-3 * u / 3600]])
+
+    def run(net, every, steps, off_after=None):
+        ens = d.Ensemble([(m, M, 150.0, 50)], state_bits=64)
+        for k, y in enumerate(states):
+            ens.set_member(0, k, y)
+        ens.set_closure(0, net, edge_geometry(g), norm, every=every)
+        if off_after is None:
+            ens.run(steps)
+        else:
+            ens.run(off_after)
+            ens.closure_mask(0, np.array([0, 1, 1, 1], dtype=np.float32))
+            mid = ens.get_member(0, 0)
+            ens.run(steps - off_after)
+            return [ens.get_member(0, k) for k in range(M)], mid
+        ens.closure_check()
+        return [ens.get_member(0, k) for k in range(M)]
+
+    p = co.init_params(3)
+    blocks = {}
+    k = 0
+    for name, shape in co.SHAPES:
+        n = int(np.prod(shape))
+        blocks[name] = slice(k, k + n)
+        k += n
+    const = p.copy()
+    const[blocks["W3"]] = 0.0
+    const[blocks["b3"]] = [0.7, -0.4]
+    const_net = ClosureMLP(const.astype(np.float32))
+    for a, b in zip(run(const_net, 1, 5), run(const_net, 3, 5)):
+        assert np.array_equal(a, b)
+    net = ClosureMLP(seed=9)
+    one, three = run(net, 1, 1), run(net, 3, 1)
+    for a, b in zip(one, three):
+        assert np.array_equal(a, b)
+    one, three = run(net, 1, 4), run(net, 3, 4)
+    assert not all(np.array_equal(a, b) for a, b in zip(one, three))
+    after, mid = run(net, 4, 3, off_after=1)  # member 0 off after the first (network) step
+    ref = mid.copy()
+    d.rk4_step(ref, 150.0, d.tendency, d.RK4Cache(ref), m, nsteps=2)
+    assert np.array_equal(after[0], ref)
+    ens = d.Ensemble([(m, M, 150.0, 5)])
+    with pytest.raises(d.TriskError) as e:
+        ens.set_closure(0, net, edge_geometry(g), norm, every=2, fused=False)
+    assert e.value.status == 6
+    with pytest.raises(d.TriskError) as e:
+        ens.set_closure(0, net, edge_geometry(g), norm, every=2, every_stage=True)
+    assert e.value.status == 6
