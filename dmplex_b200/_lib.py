@@ -206,6 +206,8 @@ def _load():
         "trisk_dist_launch_count": (_i64, [_p]),
         "trisk_ensemble_set_slices": (C.c_int, [_p, _p]),
         "trisk_ensemble_get_slices": (C.c_int, [_p, _p]),
+        "trisk_ensemble_set_members_per_thread": (C.c_int, [_p, _i32]),
+        "trisk_ensemble_get_members_per_thread": (C.c_int, [_p, C.POINTER(_i32)]),
         "trisk_ensemble_closure_mask": (C.c_int, [_p, _i32, _p]),
         "trisk_ensemble_features": (C.c_int, [_p, _i32, _p, _p, _p]),
         "trisk_ensemble_closure_check": (C.c_int, [_p]),

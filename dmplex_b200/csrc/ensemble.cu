@@ -11,6 +11,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <type_traits>
 
 #include <cuda_bf16.h>
 
@@ -66,7 +67,9 @@ __device__ __forceinline__ R* as_r(double* p) {
   return reinterpret_cast<R*>(p);
 }
 
-template <int PV, int KE, class R>
+// PW: 4 for an ensemble whose every slice takes four members per thread (one instantiation
+// with room for the wider registers), 0 for one or two members per thread as each slice has.
+template <int PV, int KE, class R, int PW>
 __global__ void __launch_bounds__(256) kg_vertex(const GroupSet G, int first_stage) {
   pdl_trigger();
   for (int vb = blockIdx.x; vb < G.totalV; vb += gridDim.x) {
@@ -74,15 +77,17 @@ __global__ void __launch_bounds__(256) kg_vertex(const GroupSet G, int first_sta
     const GroupDesc& D = G.g[gi];
     if (*D.counter >= D.nsteps) continue;
     const R* u = as_r<R>(first_stage ? D.y : D.st);
-    if (D.P == 2)
-      vertex_body<PV, KE, true, R, false, 2>(D.T, work_as<R>(D.W), u, u + (size_t)D.T.ne * D.M, D.M, 0,
-                                             vb - D.startV);
+    const R* h = u + (size_t)D.T.ne * D.M;
+    if constexpr (PW == 4)
+      vertex_body<PV, KE, true, R, false, 4>(D.T, work_as<R>(D.W), u, h, D.M, 0, vb - D.startV);
+    else if (D.P == 2)
+      vertex_body<PV, KE, true, R, false, 2>(D.T, work_as<R>(D.W), u, h, D.M, 0, vb - D.startV);
     else
-      vertex_body<PV, KE, true, R>(D.T, work_as<R>(D.W), u, u + (size_t)D.T.ne * D.M, D.M, 0, vb - D.startV);
+      vertex_body<PV, KE, true, R>(D.T, work_as<R>(D.W), u, h, D.M, 0, vb - D.startV);
   }
 }
 
-template <int PV, int KE, class R>
+template <int PV, int KE, class R, int PW>
 __global__ void __launch_bounds__(256) kg_flux(const GroupSet G, int first_stage, int want_K) {
   pdl_trigger();
   for (int vb = blockIdx.x; vb < G.totalF; vb += gridDim.x) {
@@ -90,17 +95,19 @@ __global__ void __launch_bounds__(256) kg_flux(const GroupSet G, int first_stage
     const GroupDesc& D = G.g[gi];
     if (*D.counter >= D.nsteps) continue;
     const R* u = as_r<R>(first_stage ? D.y : D.st);
-    if (D.P == 2)
-      flux_body<PV, KE, true, R, false, 2>(D.T, work_as<R>(D.W), u, u + (size_t)D.T.ne * D.M, D.M, D.nEF, want_K,
-                                           vb - D.startF);
+    const R* h = u + (size_t)D.T.ne * D.M;
+    if constexpr (PW == 4)
+      flux_body<PV, KE, true, R, false, 4>(D.T, work_as<R>(D.W), u, h, D.M, D.nEF, want_K, vb - D.startF);
+    else if (D.P == 2)
+      flux_body<PV, KE, true, R, false, 2>(D.T, work_as<R>(D.W), u, h, D.M, D.nEF, want_K, vb - D.startF);
     else
-      flux_body<PV, KE, true, R>(D.T, work_as<R>(D.W), u, u + (size_t)D.T.ne * D.M, D.M, D.nEF, want_K,
-                                 vb - D.startF);
+      flux_body<PV, KE, true, R>(D.T, work_as<R>(D.W), u, h, D.M, D.nEF, want_K, vb - D.startF);
   }
 }
 
-template <int PV, int EPI, class R>
-__global__ void __launch_bounds__(256, 4) kg_tend(const GroupSet G) {  // <= 64 registers: 8 blocks of 128
+// <= 64 registers (8 blocks of 128) for one or two members per thread; <= 128 for four
+template <int PV, int EPI, class R, int PW>
+__global__ void __launch_bounds__(256, PW == 4 ? 2 : 4) kg_tend(const GroupSet G) {
   pdl_trigger();
   for (int vb = blockIdx.x; vb < G.totalT; vb += gridDim.x) {
     const int gi = group_of(G, vb, 2);
@@ -113,7 +120,12 @@ __global__ void __launch_bounds__(256, 4) kg_tend(const GroupSet G) {  // <= 64 
     S.flag = G.flag;
     S.c = EPI == EPI_STAGE3 ? D.dt : D.dt / 2;
     S.sixth = D.dt / 6;
-    if (D.P == 2) {
+    if constexpr (PW == 4) {
+      if (D.W.dq)
+        tend_body_p<PV, EPI, true, R, 4>(D.T, work_as<R>(D.W), S, D.M, D.nET, vb - D.startT);
+      else
+        tend_body_p<PV, EPI, false, R, 4>(D.T, work_as<R>(D.W), S, D.M, D.nET, vb - D.startT);
+    } else if (D.P == 2) {
       if (D.W.dq)
         tend_body_p<PV, EPI, true, R, 2>(D.T, work_as<R>(D.W), S, D.M, D.nET, vb - D.startT);
       else
@@ -460,6 +472,9 @@ struct TriskEnsemble {
   int pv = 0, ke = 0;
   int block[3] = {128, 128, 128};  // threads per block of the vertex, flux and tendency phases
   int occ[3] = {1, 1, 1};          // resident blocks per SM of the three phases
+  // members per thread: 2 (two for an even slice, else one) or 4 (every slice's member count
+  // a multiple of four; set with trisk_ensemble_set_members_per_thread)
+  int mpt = 2;
   int sms = 1;
   std::vector<EnsembleGroup> groups;
   std::vector<Slice> slices;                 // every group's slices, group after group
@@ -570,10 +585,18 @@ void build_slices(TriskEnsemble& e) {
         D.W.dq = e.at(G.cl.dq, m.ne * m0);
         D.W.dF = e.at(G.cl.dF, m.ne * m0);
       }
-      D.P = Ms % 2 == 0 ? 2 : 1;
+      D.P = e.mpt == 4 ? 4 : (Ms % 2 == 0 ? 2 : 1);
       e.slices.push_back(sl);
     }
   }
+}
+
+// every slice's member count a multiple of four (the slices of a group: S members each, the
+// last one the rest of M)
+bool four_per_thread_fits(const TriskEnsemble& e) {
+  for (const EnsembleGroup& G : e.groups)
+    if (G.M % 4 || G.S % 4) return false;
+  return true;
 }
 
 void drop_graphs(TriskEnsemble& e) {
@@ -640,9 +663,17 @@ void layout(TriskEnsemble& e) {
     constexpr int PV = decltype(pvc)::value, KE = decltype(kec)::value;
     with_real(e, [&](auto r) {
       using R = decltype(r);
-      CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&e.occ[0], kg_vertex<PV, KE, R>, e.block[0], 0));
-      CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&e.occ[1], kg_flux<PV, KE, R>, e.block[1], 0));
-      CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&e.occ[2], kg_tend<PV, EPI_STAGE2, R>, e.block[2], 0));
+      auto occ = [&](auto pwc) {
+        constexpr int PW = decltype(pwc)::value;
+        CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&e.occ[0], kg_vertex<PV, KE, R, PW>, e.block[0], 0));
+        CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&e.occ[1], kg_flux<PV, KE, R, PW>, e.block[1], 0));
+        CUDA_CHECK(
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&e.occ[2], kg_tend<PV, EPI_STAGE2, R, PW>, e.block[2], 0));
+      };
+      if (e.mpt == 4)
+        occ(std::integral_constant<int, 4>{});
+      else
+        occ(std::integral_constant<int, 0>{});
     });
   });
   drop_graphs(e);
@@ -734,15 +765,22 @@ void enqueue_ensemble_step(TriskEnsemble& e, unsigned mask) {
         const GroupSet& G = sets[k];
         with_real(e, [&](auto r) {
           using R = decltype(r);
-          elaunch(e, kg_vertex<PV, KE, R>, 0, G.totalV, !(stage == 1 && k == 0), G, stage == 1 ? 1 : 0);
-          elaunch(e, kg_flux<PV, KE, R>, 1, G.totalF, true, G, stage == 1 ? 1 : 0, 0);
-          enqueue_closure(e, members[k], stage);
-          switch (stage) {
-            case 1: elaunch(e, kg_tend<PV, EPI_STAGE1, R>, 2, G.totalT, true, G); break;
-            case 2: elaunch(e, kg_tend<PV, EPI_STAGE2, R>, 2, G.totalT, true, G); break;
-            case 3: elaunch(e, kg_tend<PV, EPI_STAGE3, R>, 2, G.totalT, true, G); break;
-            default: elaunch(e, kg_tend<PV, EPI_STAGE4, R>, 2, G.totalT, true, G); break;
-          }
+          auto phases = [&](auto pwc) {
+            constexpr int PW = decltype(pwc)::value;
+            elaunch(e, kg_vertex<PV, KE, R, PW>, 0, G.totalV, !(stage == 1 && k == 0), G, stage == 1 ? 1 : 0);
+            elaunch(e, kg_flux<PV, KE, R, PW>, 1, G.totalF, true, G, stage == 1 ? 1 : 0, 0);
+            enqueue_closure(e, members[k], stage);
+            switch (stage) {
+              case 1: elaunch(e, kg_tend<PV, EPI_STAGE1, R, PW>, 2, G.totalT, true, G); break;
+              case 2: elaunch(e, kg_tend<PV, EPI_STAGE2, R, PW>, 2, G.totalT, true, G); break;
+              case 3: elaunch(e, kg_tend<PV, EPI_STAGE3, R, PW>, 2, G.totalT, true, G); break;
+              default: elaunch(e, kg_tend<PV, EPI_STAGE4, R, PW>, 2, G.totalT, true, G); break;
+            }
+          };
+          if (e.mpt == 4)
+            phases(std::integral_constant<int, 4>{});
+          else
+            phases(std::integral_constant<int, 0>{});
         });
       }
     }
@@ -917,6 +955,10 @@ int trisk_ensemble_create_precision(TriskModel* const* models, const int32_t* me
   e->staging = e->alloc<double>(e->max_state);
   CUDA_CHECK(cudaMemset(e->counters, 0, MAX_GROUPS * sizeof(int)));
   CUDA_CHECK(cudaMemset(e->flag, 0, sizeof(int)));
+  // FP32 state: four members per thread where every group allows it (one 16-byte load per
+  // gathered value, as two FP64 members take; measured faster on every FP32 group, slower on
+  // every FP64 one)
+  e->mpt = e->fp32 && four_per_thread_fits(*e) ? 4 : 2;
   build_slices(*e);
   layout(*e);
   CUDA_CHECK(cudaDeviceSynchronize());
@@ -1058,6 +1100,33 @@ int trisk_ensemble_set_slices(TriskEnsemble* ens, const int32_t* members_per_sli
   DeviceGuard guard(e.device);
   CUDA_CHECK(cudaStreamSynchronize(e.stream));
   for (int g = 0; g < (int)e.groups.size(); ++g) reslice(e, g, members_per_slice[g]);
+  if (e.mpt == 4 && !four_per_thread_fits(e)) {  // back to two members per thread
+    e.mpt = 2;
+    build_slices(e);
+    layout(e);
+  }
+  TRISK_API_END
+}
+
+int trisk_ensemble_set_members_per_thread(TriskEnsemble* ens, int32_t members) {
+  TRISK_API_BEGIN
+  TriskEnsemble& e = *checked_e(ens);
+  if (members != 2 && members != 4) throw Error(TRISK_ERR_ARGUMENT, "members per thread must be 2 or 4");
+  if (members == 4 && !four_per_thread_fits(e))
+    throw Error(TRISK_ERR_UNSUPPORTED, "four members per thread need every slice's member count a multiple of four");
+  DeviceGuard guard(e.device);
+  CUDA_CHECK(cudaStreamSynchronize(e.stream));
+  e.mpt = members;
+  build_slices(e);
+  layout(e);
+  TRISK_API_END
+}
+
+int trisk_ensemble_get_members_per_thread(TriskEnsemble* ens, int32_t* members) {
+  TRISK_API_BEGIN
+  TriskEnsemble& e = *checked_e(ens);
+  if (!members) throw Error(TRISK_ERR_ARGUMENT, "NULL argument");
+  *members = e.mpt;
   TRISK_API_END
 }
 
@@ -1076,7 +1145,8 @@ int trisk_ensemble_autotune(TriskEnsemble* ens, int32_t steps, double* best_ms) 
   DeviceGuard guard(e.device);
   CUDA_CHECK(cudaStreamSynchronize(e.stream));
   // Times `steps` RK4 steps of all groups for every combination of the three phases' block
-  // sizes, then for the members per slice of each group in turn (S, S/2, S/4 ... and 2 S ..
+  // sizes, then four members per thread (where every slice allows it) at each tendency block
+  // size, then for the members per slice of each group in turn (S, S/2, S/4 ... and 2 S ..
   // up to the group), and keeps the fastest. The members' states (in the slicing they had),
   // the step counters and each group's step count are saved first and restored after every
   // trial and at the end, so the ensemble continues as if nothing had run (every candidate
@@ -1126,6 +1196,8 @@ int trisk_ensemble_autotune(TriskEnsemble* ens, int32_t steps, double* best_ms) 
   };
   int best[3] = {e.block[0], e.block[1], e.block[2]};
   double best_t = INFINITY;
+  e.mpt = 2;  // the blocks first with one or two members per thread
+  build_slices(e);
   try {
     for (int a : choices)
       for (int b : choices)
@@ -1144,6 +1216,28 @@ int trisk_ensemble_autotune(TriskEnsemble* ens, int32_t steps, double* best_ms) 
         }
     for (int p = 0; p < 3; ++p) e.block[p] = best[p];
     layout(e);
+    // four members per thread, at each tendency block size, where every slice allows it
+    int best_mpt = 2;
+    if (four_per_thread_fits(e)) {
+      const int b2 = best[2];
+      e.mpt = 4;
+      build_slices(e);
+      for (int c : choices) {
+        e.block[2] = c;
+        layout(e);
+        const double ms = trial();
+        if (ms < best_t) {
+          best_t = ms;
+          best[2] = c;
+          best_mpt = 4;
+        }
+      }
+      if (best_mpt != 4) best[2] = b2;
+      e.mpt = best_mpt;
+      build_slices(e);
+      for (int p = 0; p < 3; ++p) e.block[p] = best[p];
+      layout(e);
+    }
     for (int g = 0; g < ng; ++g) {
       const int M = e.groups[g].M, start = e.groups[g].S;
       int best_S = start;
@@ -1154,7 +1248,7 @@ int trisk_ensemble_autotune(TriskEnsemble* ens, int32_t steps, double* best_ms) 
         if (S >= M) break;
       }
       for (int S : candidates) {
-        if (S == start) continue;
+        if (S == start || (e.mpt == 4 && S % 4)) continue;
         set_slicing(g, S);
         const double ms = trial();
         if (ms < best_t) {

@@ -184,9 +184,9 @@ __device__ __forceinline__ void split(int t, int M, int& ent, int& mem) {
   }
 }
 
-// P members per thread (P = 1 or 2, M a multiple of P): the thread's members are mm ..
-// mm + P - 1, read and written as one P-wide vector; the arithmetic per member is that of
-// P = 1, so results are the same bit for bit.
+// P members per thread (P = 1, 2 or 4, M a multiple of P): the thread's members are mm ..
+// mm + P - 1, read and written as one P-wide vector (two 16-byte halves for four FP64
+// members); the arithmetic per member is that of P = 1, so results are the same bit for bit.
 template <bool ENS, int P>
 __device__ __forceinline__ void split_p(int t, int M, int& ent, int& mm) {
   if (P == 1) {
@@ -202,6 +202,18 @@ template <class R, int P>
 __device__ __forceinline__ void ld_members(const R* p, double (&x)[P]) {
   if constexpr (P == 1) {
     x[0] = p[0];
+  } else if constexpr (P == 4 && sizeof(R) == 8) {
+    const double2 a = *reinterpret_cast<const double2*>(p), b = *reinterpret_cast<const double2*>(p + 2);
+    x[0] = a.x;
+    x[1] = a.y;
+    x[2] = b.x;
+    x[3] = b.y;
+  } else if constexpr (P == 4) {
+    const float4 v = *reinterpret_cast<const float4*>(p);
+    x[0] = v.x;
+    x[1] = v.y;
+    x[2] = v.z;
+    x[3] = v.w;
   } else if constexpr (sizeof(R) == 8) {
     const double2 v = *reinterpret_cast<const double2*>(p);
     x[0] = v.x;
@@ -217,6 +229,11 @@ template <class R, int P>
 __device__ __forceinline__ void st_members(R* p, const double (&x)[P]) {
   if constexpr (P == 1) {
     p[0] = (R)x[0];
+  } else if constexpr (P == 4 && sizeof(R) == 8) {
+    *reinterpret_cast<double2*>(p) = make_double2(x[0], x[1]);
+    *reinterpret_cast<double2*>(p + 2) = make_double2(x[2], x[3]);
+  } else if constexpr (P == 4) {
+    *reinterpret_cast<float4*>(p) = make_float4((float)x[0], (float)x[1], (float)x[2], (float)x[3]);
   } else if constexpr (sizeof(R) == 8) {
     *reinterpret_cast<double2*>(p) = make_double2(x[0], x[1]);
   } else {

@@ -80,6 +80,16 @@ class Ensemble:
             raise ValueError("one slice size per group")
         check(lib.trisk_ensemble_set_slices(self._h, b.ctypes.data))
 
+    @property
+    def members_per_thread(self) -> int:
+        """2 (two members per thread where a slice's member count is even) or 4."""
+        v = C.c_int32()
+        check(lib.trisk_ensemble_get_members_per_thread(self._h, C.byref(v)))
+        return v.value
+
+    def set_members_per_thread(self, members: int) -> None:
+        check(lib.trisk_ensemble_set_members_per_thread(self._h, int(members)))
+
     def run_async(self, steps: int) -> None:
         check(lib.trisk_ensemble_run_async(self._h, int(steps)))
 

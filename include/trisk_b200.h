@@ -454,9 +454,18 @@ int trisk_ensemble_get_block(TriskEnsemble* ensemble, int32_t block[3]);
  * bit for bit for every slicing. */
 int trisk_ensemble_set_slices(TriskEnsemble* ensemble, const int32_t* members_per_slice);
 int trisk_ensemble_get_slices(TriskEnsemble* ensemble, int32_t* members_per_slice);
+/* Members per thread of the three phases: 2 (two members per thread for a slice with an even
+ * member count, else one) or 4 (four, as one 16-byte FP32 or two 16-byte FP64 vectors per
+ * gathered value, so each table entry a thread loads serves four members; every slice's
+ * member count must be a multiple of four, else TRISK_ERR_UNSUPPORTED, and a later slicing
+ * that breaks this returns to 2). The default is 4 for an FP32-state ensemble whose groups
+ * allow it, else 2. Results are the same bit for bit. */
+int trisk_ensemble_set_members_per_thread(TriskEnsemble* ensemble, int32_t members);
+int trisk_ensemble_get_members_per_thread(TriskEnsemble* ensemble, int32_t* members);
 /* Autotuner of the batched path (no reference counterpart): times `steps` RK4 steps of all
- * groups for every combination of the phase block sizes {64, 128, 256}, then for each group
- * a few members-per-slice values around the current one, keeps the fastest and restores the
+ * groups for every combination of the phase block sizes {64, 128, 256}, then four members per
+ * thread at each tendency block size (where the slices allow it), then for each group a few
+ * members-per-slice values around the current one, keeps the fastest and restores the
  * members' states, step counters and step counts, so results are unchanged; best_ms gets the
  * time per step. Each call keeps one copy of the states until the ensemble is destroyed. */
 int trisk_ensemble_autotune(TriskEnsemble* ensemble, int32_t steps, double* best_ms);

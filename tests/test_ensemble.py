@@ -163,8 +163,9 @@ def test_fp32_state_ensemble(require_gpu, pv, ke):
 
 @pytest.mark.parametrize("state_bits", [64, 32])
 def test_closure_two_members_per_thread(require_gpu, state_bits):
-    """The closure path with two members per thread (an even member count) against one member
-    per thread (an odd count): the network is row-wise, so every member is bit-identical."""
+    """The closure path with two and four members per thread (an even member count) against one
+    member per thread (an odd count): the network is row-wise, so every member is
+    bit-identical."""
     from dmplex_b200.closure import ClosureMLP
     from dmplex_b200.coarsen import edge_geometry
     si = w.si_parameters()
@@ -175,21 +176,23 @@ def test_closure_two_members_per_thread(require_gpu, state_bits):
     u = np.abs(states[0][:g.ne]).mean()
     norm = np.concatenate([np.zeros(24), np.ones(24), [1e-3 * u, 1e-3 * u / 3600]])
     out = {}
-    for M in (4, 5):
+    for M, mpt in ((4, 2), (4, 4), (5, 2)):
         ens = d.Ensemble([(m, M, 150.0, 6)], state_bits=state_bits)
+        ens.set_members_per_thread(mpt)
         for k in range(M):
             ens.set_member(0, k, states[k])
         ens.set_closure(0, net, edge_geometry(g), norm)
         ens.run(6)
         ens.closure_check()
-        out[M] = [ens.get_member(0, k) for k in range(4)]
+        out[M, mpt] = [ens.get_member(0, k) for k in range(4)]
     plain = d.Ensemble([(m, 4, 150.0, 6)], state_bits=state_bits)
     for k in range(4):
         plain.set_member(0, k, states[k])
     plain.run(6)
     for k in range(4):
-        assert np.array_equal(out[4][k], out[5][k]), k
-        assert not np.array_equal(out[4][k], plain.get_member(0, k))
+        assert np.array_equal(out[4, 2][k], out[5, 2][k]), k
+        assert np.array_equal(out[4, 4][k], out[5, 2][k]), k
+        assert not np.array_equal(out[4, 2][k], plain.get_member(0, k))
 
 
 def test_ensemble_autotune_keeps_results(require_gpu):
@@ -373,3 +376,47 @@ def test_closure_network_interval(require_gpu):
     with pytest.raises(d.TriskError) as e:
         ens.set_closure(0, net, edge_geometry(g), norm, every=2, every_stage=True)
     assert e.value.status == 6
+
+
+@pytest.mark.parametrize("pv,ke,state_bits", [("trisk", "cell", 32), ("gassmann", "vertex", 64),
+                                              ("gassmann_mean", "mixed", 32), ("trisk", "vertex", 64)])
+def test_four_members_per_thread_bitwise(require_gpu, pv, ke, state_bits):
+    """Four members per thread (16-byte FP32 or two 16-byte FP64 vectors per gathered value)
+    against the default two: every member bit for bit, with a closure-free group of 8 and one of
+    12 members in sliced and whole form; refused while a slice's member count is not a multiple
+    of four, and dropped back to two by a slicing that breaks it."""
+    si = w.si_parameters()
+    levels, members, nsteps = (3, 4), (8, 12), (6, 4)
+    grids = [trisk_grid(n, True) for n in levels]
+    models = [d.TRiSKShallowWater(g, pv_flux=pv, kinetic_energy=ke, **si) for g in grids]
+    dts = [w.courant_dt(g) for g in grids]
+    states = [member_states(g, k, seed) for g, k, seed in zip(grids, members, (7, 8))]
+    out = []
+    for mpt, slices in ((2, None), (4, None), (4, [4, 8])):
+        ens = d.Ensemble([(m, k, dt, s) for m, k, dt, s in zip(models, members, dts, nsteps)],
+                         state_bits=state_bits)
+        if slices:
+            ens.set_slices(slices)
+        ens.set_members_per_thread(mpt)
+        assert ens.members_per_thread == mpt
+        for gi, group in enumerate(states):
+            for k, y in enumerate(group):
+                ens.set_member(gi, k, y)
+        ens.run(max(nsteps))
+        assert ens.steps_taken() == list(nsteps)
+        out.append([[ens.get_member(gi, k) for k in range(len(group))] for gi, group in enumerate(states)])
+        if slices:
+            ens.set_slices([2, 6])  # 2 is not a multiple of four: back to two per thread
+            assert ens.members_per_thread == 2
+    for other in out[1:]:
+        for ga, gb in zip(out[0], other):
+            for a, b in zip(ga, gb):
+                assert np.array_equal(a, b)
+    odd = d.Ensemble([(models[0], 6, dts[0], 2)])
+    with pytest.raises(d.TriskError) as e:
+        odd.set_members_per_thread(4)
+    assert e.value.status == 6
+    # the default: four per thread for FP32 state where the groups allow it, else two
+    assert d.Ensemble([(models[0], 8, dts[0], 2)], state_bits=32).members_per_thread == 4
+    assert d.Ensemble([(models[0], 8, dts[0], 2)], state_bits=64).members_per_thread == 2
+    assert d.Ensemble([(models[0], 6, dts[0], 2)], state_bits=32).members_per_thread == 2
