@@ -257,14 +257,14 @@ template <class R>
 __global__ void __launch_bounds__(closure::TILE) kg_closure_fused(
     DevTables T, DevWorkT<R> W, const R* y, int M, const float* geom, const FeatureNorm N,
     const closure::ParamsBF16* wbf, const closure::Params* p, const float* member_on, double sF, double sQ, R* dF,
-    R* dq, int64_t rows, closure::Status* status, const int* counter, int every) {
+    R* dq, int64_t rows, closure::Status* status, const int* counter, int every, int phase) {
   using namespace closure;
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ __align__(16) InferStatic st;
   const int t = threadIdx.x;
   const int64_t ntiles = (rows + TILE - 1) / TILE;
   if ((int64_t)blockIdx.x >= ntiles) return;
-  if (every > 1 && *counter % every != 0) return;  // not a network step: the corrections are kept
+  if (every > 1 && (*counter - phase) % every != 0) return;  // not a network step: the corrections are kept
   const InferSmem S(smem);
   const uint32_t tmem = infer_setup(S, st, wbf, p);
   MmaWaits waits(smem_u32(S.mbar), &st.abort);
@@ -428,6 +428,7 @@ struct ClosureSlot {
   bool work_free = false;      // project the momentum correction to do no work (per member)
   bool fused = true;           // features, network and corrections in one kernel (else three)
   int every = 1;               // the network runs every `every` steps; its corrections are kept between
+  int phase = 0;               // on the steps whose count is phase modulo every
   int fused_per_sm = 1;        // resident CTAs per SM of the fused kernel
   double* sums = nullptr;      // 2 M: <g, dq>, <g, g> per member
   double* partials = nullptr;  // 2 M x WORK_SUM_BLOCKS per-block partial sums of them
@@ -600,6 +601,20 @@ bool four_per_thread_fits(const TriskEnsemble& e) {
   return true;
 }
 
+void drop_graphs(TriskEnsemble& e);
+
+// The next step of group G runs its closure's network, whatever its interval (its kept
+// corrections belong to states or a layout that the host has just changed).
+void restart_network(TriskEnsemble& e, EnsembleGroup& G) {
+  ClosureSlot& c = G.cl;
+  if (!c.net || c.every <= 1) return;
+  const int phase = (int)(G.taken % c.every);
+  if (phase != c.phase) {
+    c.phase = phase;
+    drop_graphs(e);  // the phase is an argument of the captured launches
+  }
+}
+
 void drop_graphs(TriskEnsemble& e) {
   for (auto& kv : e.graphs)
     if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
@@ -725,7 +740,7 @@ void enqueue_closure(TriskEnsemble& e, const std::vector<int>& set_slices, int s
         const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)e.sms * c.fused_per_sm));
         kg_closure_fused<R><<<grid, closure::TILE, closure::FWD_SMEM_BYTES, e.stream>>>(
             D.T, work_as<R>(D.W), ys, D.M, c.geom, c.norm, wbf, p, c.member_on + sl.m0, c.norm.out_scale[0],
-            c.norm.out_scale[1], dF, dq, rows, status, D.counter, c.every);
+            c.norm.out_scale[1], dF, dq, rows, status, D.counter, c.every, c.phase);
         CUDA_CHECK(cudaGetLastError());
         e.launches -= 2;  // one launch instead of three
       } else {
@@ -885,6 +900,7 @@ void reslice(TriskEnsemble& e, int g, int S) {
   G.S = S;
   build_slices(e);
   drop_graphs(e);
+  restart_network(e, G);
 }
 
 }  // namespace
@@ -990,6 +1006,7 @@ int trisk_ensemble_set_member(TriskEnsemble* ens, int32_t group, int32_t member,
   });
   CUDA_CHECK(cudaGetLastError());
   CUDA_CHECK(cudaStreamSynchronize(e.stream));
+  restart_network(e, e.groups[group]);  // a new state: its corrections are formed afresh
   TRISK_API_END
 }
 
@@ -1055,7 +1072,10 @@ int trisk_ensemble_reset(TriskEnsemble* ens) {
   DeviceGuard guard(e.device);
   CUDA_CHECK(cudaMemsetAsync(e.counters, 0, MAX_GROUPS * sizeof(int), e.stream));
   CUDA_CHECK(cudaStreamSynchronize(e.stream));
-  for (EnsembleGroup& G : e.groups) G.taken = 0;
+  for (EnsembleGroup& G : e.groups) {
+    G.taken = 0;
+    restart_network(e, G);
+  }
   TRISK_API_END
 }
 
@@ -1273,6 +1293,10 @@ int trisk_ensemble_autotune(TriskEnsemble* ens, int32_t steps, double* best_ms) 
   for (int g = 0; g < ng; ++g) e.groups[g].taken = taken[g];
   CUDA_CHECK(cudaMemcpyAsync(e.counters, counters.data(), MAX_GROUPS * sizeof(int), cudaMemcpyHostToDevice,
                              e.stream));
+  for (EnsembleGroup& G : e.groups) {  // the trials overwrote the kept corrections
+    G.cl.phase = -1;
+    restart_network(e, G);
+  }
   CUDA_CHECK(cudaMemsetAsync(e.flag, 0, sizeof(int), e.stream));
   CUDA_CHECK(cudaStreamSynchronize(e.stream));
   if (best_ms) *best_ms = best_t / steps;
@@ -1345,6 +1369,7 @@ int trisk_ensemble_set_closure(TriskEnsemble* ens, int32_t group, TriskClosure* 
     c.partials = e.alloc<double>(2 * (size_t)G.M * WORK_SUM_BLOCKS);
   }
   c.net = net;
+  c.phase = (int)(G.taken % c.every);  // the network runs at the next step
   build_slices(e);
   drop_graphs(e);
   TRISK_API_END

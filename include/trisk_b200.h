@@ -496,7 +496,10 @@ int trisk_ensemble_energy(TriskEnsemble* ensemble, int32_t group, double* energi
  * bits 8-15: the network interval n (0 or 1: every step): the network runs on the steps whose
  * group step count is a multiple of n and its corrections are kept and applied on the steps
  * between (needs the one-kernel form at stage 1 only, else TRISK_ERR_UNSUPPORTED). Turning
- * a member off (trisk_ensemble_closure_mask) clears its kept corrections at once.
+ * a member off (trisk_ensemble_closure_mask) clears its kept corrections at once, and the
+ * network runs on the next step after the closure is set and after every call that changes
+ * the members' states or layout (set_member, reset, set_slices, autotune), whatever the
+ * interval.
  * net = NULL removes the group's closure. */
 int trisk_ensemble_set_closure(TriskEnsemble* ensemble, int32_t group, TriskClosure* net, const float* geometry,
                                const double* norm, int32_t flags);

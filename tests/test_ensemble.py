@@ -369,6 +369,23 @@ def test_closure_network_interval(require_gpu):
     ref = mid.copy()
     d.rk4_step(ref, 150.0, d.tendency, d.RK4Cache(ref), m, nsteps=2)
     assert np.array_equal(after[0], ref)
+    # new states mid-interval: the network runs on the next step (as on a fresh ensemble's first)
+    fresh = member_states(g, M, 52)
+    ens = d.Ensemble([(m, M, 150.0, 50)], state_bits=64)
+    for k, y in enumerate(states):
+        ens.set_member(0, k, y)
+    ens.set_closure(0, net, edge_geometry(g), norm, every=4)
+    ens.run(2)
+    for k, y in enumerate(fresh):
+        ens.set_member(0, k, y)
+    ens.run(1)
+    ref = d.Ensemble([(m, M, 150.0, 50)], state_bits=64)
+    for k, y in enumerate(fresh):
+        ref.set_member(0, k, y)
+    ref.set_closure(0, net, edge_geometry(g), norm, every=4)
+    ref.run(1)
+    for k in range(M):
+        assert np.array_equal(ens.get_member(0, k), ref.get_member(0, k)), k
     ens = d.Ensemble([(m, M, 150.0, 5)])
     with pytest.raises(d.TriskError) as e:
         ens.set_closure(0, net, edge_geometry(g), norm, every=2, fused=False)
