@@ -587,7 +587,12 @@ void build_slices(TriskEnsemble& e) {
         D.W.dq = e.at(G.cl.dq, m.ne * m0);
         D.W.dF = e.at(G.cl.dF, m.ne * m0);
       }
-      D.P = e.mpt == 4 ? 4 : (Ms % 2 == 0 ? 2 : 1);
+      // Two members per thread load and store them as one 8- or 16-byte vector, which needs
+      // the slice's buffers to start at an even element: every n * m0 even (n = the entity
+      // counts; always so on the generated meshes, whose counts are even). Four members per
+      // thread need every m0 to be a multiple of four, which four_per_thread_fits checks.
+      const bool even_base = m0 % 2 == 0 || (m.ne % 2 == 0 && m.nc % 2 == 0 && m.nv % 2 == 0);
+      D.P = e.mpt == 4 ? 4 : (Ms % 2 == 0 && even_base ? 2 : 1);
       e.slices.push_back(sl);
     }
   }

@@ -455,7 +455,7 @@ int trisk_ensemble_get_block(TriskEnsemble* ensemble, int32_t block[3]);
 int trisk_ensemble_set_slices(TriskEnsemble* ensemble, const int32_t* members_per_slice);
 int trisk_ensemble_get_slices(TriskEnsemble* ensemble, int32_t* members_per_slice);
 /* Members per thread of the three phases: 2 (two members per thread for a slice with an even
- * member count, else one) or 4 (four, as one 16-byte FP32 or two 16-byte FP64 vectors per
+ * member count whose buffers start at an even element, else one) or 4 (four, as one 16-byte FP32 or two 16-byte FP64 vectors per
  * gathered value, so each table entry a thread loads serves four members; every slice's
  * member count must be a multiple of four, else TRISK_ERR_UNSUPPORTED, and a later slicing
  * that breaks this returns to 2). The default is 4 for an FP32-state ensemble whose groups
