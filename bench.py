@@ -59,6 +59,12 @@ def parse():
     p.add_argument("--ensemble-days", type=float, default=1.0, help="simulated days of the ensemble leg")
     p.add_argument("--ensemble-groups", default=None,
                    help="groups of the ensemble leg as level x members, e.g. 7x8,6x32 (default: 5x64,6x32,7x8)")
+    p.add_argument("--ensemble-scheme", default=f"{PV}/{KE}",
+                   help="PV flux / kinetic energy of the ensemble leg, e.g. trisk/cell (default: gassmann/vertex)")
+    p.add_argument("--ensemble-state", default="both", choices=["both", "64", "32"],
+                   help="state precision of the ensemble leg: FP64 and FP32 (both), or one of them")
+    p.add_argument("--ensemble-no-autotune", action="store_true",
+                   help="ensemble leg at the default block sizes and slices, without the autotuner")
     p.add_argument("--no-icon", action="store_true", help="skip the ICON triangle-model leg")
     p.add_argument("--icon-level", type=int, default=8, help="triangle level of the ICON leg (8: 1.31 M cells)")
     p.add_argument("--icon-steps", type=int, default=100, help="timed RK4 steps of the ICON leg")
@@ -471,12 +477,15 @@ def ncu_traffic(kernel):
 ENSEMBLE_GROUPS = ((5, 64), (6, 32), (7, 8))  # (mesh level, members), one simulated day, FP64
 
 
-def run_ensemble_leg(local_rank, seed, days=1.0, state_bits=64, groups_spec=ENSEMBLE_GROUPS):
+def run_ensemble_leg(local_rank, seed, days=1.0, state_bits=64, groups_spec=ENSEMBLE_GROUPS, pv=PV, ke=KE,
+                     autotune=True):
     """Batched ensemble of three mesh levels in one persistent CUDA-graph launch per phase:
     every member has its own seed, harmonic degree <= 12 and height rms in 50-300 m; each
     level has its own dt (Courant 0.5) and runs `days` simulated days (state_bits 32: the
     states and work vectors are stored as float, the arithmetic stays FP64). groups_spec:
-    (level, members) of each group, 64 x hexagon 5, 32 x hexagon 6 and 8 x hexagon 7 by default."""
+    (level, members) of each group, 64 x hexagon 5, 32 x hexagon 6 and 8 x hexagon 7 by default;
+    pv/ke: the scheme (Gassmann PV flux and vertex kinetic energy by default); autotune: let
+    the autotuner pick block sizes and slices first."""
     import torch
     import dmplex_b200 as d
     from dmplex_b200 import workloads as w
@@ -484,7 +493,7 @@ def run_ensemble_leg(local_rank, seed, days=1.0, state_bits=64, groups_spec=ENSE
     groups, info = [], []
     for level, members in groups_spec:
         g = d.TRiSKGrid(d.create_hexagon_mesh(level, centroidal=True))
-        m = d.TRiSKShallowWater(g, pv_flux=PV, kinetic_energy=KE, device=local_rank, **si)
+        m = d.TRiSKShallowWater(g, pv_flux=pv, kinetic_energy=ke, device=local_rank, **si)
         nsteps, dt = w.day_steps(g)
         nsteps = max(1, int(round(nsteps * days)))
         groups.append((m, members, dt, nsteps))
@@ -493,7 +502,7 @@ def run_ensemble_leg(local_rank, seed, days=1.0, state_bits=64, groups_spec=ENSE
     for gi, (g, m, members, nsteps, dt) in enumerate(info):
         for k, y in enumerate(w.ensemble_members(g, members, seed=seed + gi)):
             ens.set_member(gi, k, y)
-    tuned_ms = ens.autotune(5)  # phase block sizes and slices; the states are left as they were
+    tuned_ms = ens.autotune(5) if autotune else None  # block sizes and slices; the states are kept
     stream = torch.cuda.ExternalStream(ens.stream(), device=local_rank)
     longest = max(x[3] for x in info)
     ens.run(3)  # warm-up (graph capture)
@@ -515,7 +524,7 @@ def run_ensemble_leg(local_rank, seed, days=1.0, state_bits=64, groups_spec=ENSE
         nbytes += s * (4 * (T + 2 * members * n_b) + 15 * members * n_b)
     peak, _ = measured_peak()
     return {"workload": "ensemble " + " + ".join(f"{k}x hexagon{l}" for l, k in groups_spec) +
-                        f", {PV}/{KE}, {'FP64' if state_bits == 64 else 'FP32 state, FP64 arithmetic'}, "
+                        f", {pv}/{ke}, {'FP64' if state_bits == 64 else 'FP32 state, FP64 arithmetic'}, "
                         f"{days:g} simulated day each",
             "value": cell_steps / (ms * 1e-3), "unit": "cell-steps/s",
             "gpu_seconds_per_simulated_day": ms * 1e-3 / days,
@@ -836,11 +845,17 @@ def run_b200(args, rank, world, local_rank):
     if not args.no_ensemble:
         spec = ENSEMBLE_GROUPS if not args.ensemble_groups else \
             tuple(tuple(int(v) for v in gr.split("x")) for gr in args.ensemble_groups.split(","))
-        ensemble = optional_leg(run_ensemble_leg, local_rank, seed=1000 * (rank + 1), days=args.ensemble_days,
-                                groups_spec=spec)
-        f32 = optional_leg(run_ensemble_leg, local_rank, seed=1000 * (rank + 1), days=args.ensemble_days,
-                           state_bits=32, groups_spec=spec)
-        if "error" not in ensemble and "error" not in f32:
+        pv, ke = args.ensemble_scheme.split("/")
+        leg = dict(seed=1000 * (rank + 1), days=args.ensemble_days, groups_spec=spec, pv=pv, ke=ke,
+                   autotune=not args.ensemble_no_autotune)
+        ensemble = f32 = None
+        if args.ensemble_state in ("both", "64"):
+            ensemble = optional_leg(run_ensemble_leg, local_rank, **leg)
+        if args.ensemble_state in ("both", "32"):
+            f32 = optional_leg(run_ensemble_leg, local_rank, state_bits=32, **leg)
+        if ensemble is None:
+            ensemble = f32
+        elif f32 is not None and "error" not in ensemble and "error" not in f32:
             ensemble["fp32_state"] = {k: f32[k] for k in ("value", "gpu_seconds_per_simulated_day", "gbs", "frac")}
         if world > 1 and "error" not in ensemble:
             ensemble["value_all_ranks"] = world * ensemble["value"]
