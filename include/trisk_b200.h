@@ -5,8 +5,9 @@
  * In dmplex.jl the path sits behind Julia generic functions, not an FFI:
  *   tendency!(dy, y, m::TRiSKShallowWater)          src/FiniteVolumes/TRiSKShallowWater.jl:379
  *   rk4_step!(y, dt, tendency!, cache, model)       src/TimeSteppers/RungeKutta.jl:18
- * The entry points below are what a `ccall` shim binds in their place (the shim is in
- * INTEGRATION.md). Conventions shared by every entry point:
+ * The entry points below are what a Julia `ccall` shim binds in their place: a model type
+ * whose tendency! and rk4_step! methods call trisk_tendency and trisk_rk4_step. Conventions
+ * shared by every entry point:
  *   - State y = [u_1..u_ne; h_1..h_nc] in file (Plex) numbering, FP64, exactly the
  *     reference's layout (TRiSKShallowWater.jl:172-174).
  *   - Tables are passed as Julia holds them: column-major [k, entity] (k fastest),
