@@ -105,10 +105,12 @@ __global__ void __launch_bounds__(256) kg_flux(const GroupSet G, int first_stage
   }
 }
 
-// <= 64 registers (8 blocks of 128) for one or two members per thread; <= 85 for four (three
-// blocks of 256: measured 2-5 % faster than 128 registers at two blocks)
+// <= 64 registers (8 blocks of 128) for one or two members per thread, and for four with a
+// Gassmann PV flux (measured 5-6 % faster than 85 on the FP32 hexagon-6 and -7 groups); <= 85
+// for four with the TRiSK PV flux (three blocks of 256: 2-5 % faster than 128 registers at two
+// blocks, and 12 % faster than 64 on 128 hexagon-6 members)
 template <int PV, int EPI, class R, int PW>
-__global__ void __launch_bounds__(256, PW == 4 ? 3 : 4) kg_tend(const GroupSet G) {
+__global__ void __launch_bounds__(256, PW == 4 && PV == PVM_TRISK ? 3 : 4) kg_tend(const GroupSet G) {
   pdl_trigger();
   for (int vb = blockIdx.x; vb < G.totalT; vb += gridDim.x) {
     const int gi = group_of(G, vb, 2);
