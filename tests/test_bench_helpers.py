@@ -46,3 +46,20 @@ def test_leg_summary_is_compact_and_keeps_errors():
     assert s["ensemble"]["fp32_state_gpu_seconds_per_simulated_day"] == 0.98 and "steps" not in s["ensemble"]
     assert s["closure"] == {"error": "RuntimeError: boom"} and s["icon"] is None
     assert len(json.dumps(s)) < 1500
+
+
+def test_ensemble_leg_flags(monkeypatch):
+    """The ensemble leg runs the configured groups, scheme, precision and autotuner choice;
+    the defaults are the batched benchmark's (Gassmann PV flux, vertex kinetic energy, FP64
+    and FP32 state, autotuned)."""
+    import sys
+
+    import bench
+    monkeypatch.setattr(sys, "argv", ["bench.py"])
+    a = bench.parse()
+    assert (a.ensemble_scheme, a.ensemble_state, a.ensemble_no_autotune) == ("gassmann/vertex", "both", False)
+    monkeypatch.setattr(sys, "argv", ["bench.py", "--ensemble-groups", "6x128", "--ensemble-scheme", "trisk/cell",
+                                      "--ensemble-state", "32", "--ensemble-no-autotune"])
+    a = bench.parse()
+    assert (a.ensemble_groups, a.ensemble_scheme, a.ensemble_state, a.ensemble_no_autotune) == \
+        ("6x128", "trisk/cell", "32", True)
