@@ -87,11 +87,13 @@ __device__ __forceinline__ long long global_ns() {
   return t;
 }
 
-// Waits for the completion of the mbarrier phase of parity `phase`, for at most MBAR_WAIT_NS;
-// false if it gave up.
+// Waits for the completion of the mbarrier phase of parity `phase`, for at most MBAR_WAIT_NS
+// and at most MBAR_WAIT_TRIES polls (a backstop that the clock always beats: a poll takes more
+// than a nanosecond); false if it gave up.
+constexpr uint32_t MBAR_WAIT_TRIES = 1u << 31;
 __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase) {
   long long start = 0;
-  for (uint32_t i = 0;; ++i) {
+  for (uint32_t i = 0; i < MBAR_WAIT_TRIES; ++i) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
@@ -106,6 +108,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase) {
       else if (now - start > MBAR_WAIT_NS) return false;
     }
   }
+  return false;
 }
 
 // 16 consecutive FP32 columns of this thread's TMEM lane

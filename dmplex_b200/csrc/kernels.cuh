@@ -724,8 +724,8 @@ __global__ void __launch_bounds__(256) k_tend(DevTables T, DevWork W, DevStage S
 // results are those of the launches bit for bit.
 
 // The grid barrier: arrivals counted in *count, released by incrementing *gen. A block's wait
-// gives up after a second, sets *err and leaves; a block that sees *err after a barrier
-// returns, so every wait ends.
+// gives up after a second (or 2^31 polls, a backstop that the clock always beats), sets *err
+// and leaves; a block that sees *err after a barrier returns, so every wait ends.
 struct GridBarrier {
   unsigned* count;
   unsigned* gen;
@@ -751,7 +751,7 @@ __device__ __forceinline__ bool grid_sync(const GridBarrier& B) {
     } else {
       const long long start = barrier_ns();
       for (unsigned i = 1; *gen == g; ++i)
-        if ((i & 1023u) == 0 && barrier_ns() - start > 1000000000LL) {
+        if (((i & 1023u) == 0 && barrier_ns() - start > 1000000000LL) || i == (1u << 31)) {
           atomicExch(B.err, 1);
           break;
         }
